@@ -1,0 +1,114 @@
+// Device-side data layout and kernel entry points for the locally corrected
+// combined-field matvec (Laplace and Helmholtz), sm_100a.
+//
+// HBM layout of one operator plan (all arrays SoA, 0-based):
+//   targets       : tx,ty,tz            f64[ntarg] each
+//   oversampled   : sx,sy,sz,nx,ny,nz,w f64[nptso] each (srcover, whtsover)
+//   patches       : pstart[npatches+1], ostart[npatches+1] (node offsets),
+//                   pclass[npatches] -> interpolation matrix of the class
+//                   (iptype, norder, nfar): imat[nf x np] f64 (row-major)
+//   near matrix   : row_ptr[ntarg+1] (into col/wofs), col[nnz] patch index,
+//                   wofs[nnz+1] entry offsets (iquad-1),
+//                   W_eff[nquad] = wnear - smooth oversampled part, stored
+//                   f64 (and f32 for the mixed-precision path);
+//                   complex values are interleaved (re, im).
+// Densities are stored point-major with nd densities per point
+// (sigma[(pt*nd + m)], the reference's sigma(ndim, npts)), complex
+// interleaved.  Per matvec the strength kernel writes per-source
+// charge/dipole strengths (scaled by alpha, beta, w and 1/(4 pi)), the far
+// kernel writes per-chunk partial potentials (scratch), and the combine
+// kernel sums the partials and the near correction into pot.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bie {
+namespace dev {
+
+struct Geometry {
+  int64_t ntarg = 0, nptso = 0, npatches = 0, npts = 0;
+  const double* tx = nullptr;
+  const double* ty = nullptr;
+  const double* tz = nullptr;
+  const double* sx = nullptr;
+  const double* sy = nullptr;
+  const double* sz = nullptr;
+  const double* snx = nullptr;
+  const double* sny = nullptr;
+  const double* snz = nullptr;
+  const double* sw = nullptr;
+  const int32_t* pstart = nullptr;   // npatches+1
+  const int32_t* ostart = nullptr;   // npatches+1
+  const int32_t* pclass = nullptr;   // npatches
+  const int64_t* cmoff = nullptr;    // per class offset into imat
+  const double* imat = nullptr;
+  int max_np = 0, max_nf = 0;
+};
+
+struct Near {
+  int64_t nnz = 0, nquad = 0;
+  const int64_t* row_ptr = nullptr;  // ntarg+1
+  const int32_t* col = nullptr;      // nnz
+  const int64_t* wofs = nullptr;     // nnz+1
+};
+
+// Kernel constants. kind 0: Laplace (real alpha, beta), 1: Helmholtz.
+struct KParams {
+  int kind = 0;
+  double ar = 0, ai = 0, br = 0, bi = 0, kr = 0, ki = 0;
+  double thresh = 0;
+};
+
+// precision: 0 = f64 far field, 1 = f32 far field (f64 accumulation across
+// source tiles).
+struct MatvecArgs {
+  int precision = 0;
+  int nd = 1;
+  int nchunks = 1;
+  const double* sigma = nullptr;  // npts*nd (x2 if complex)
+  double* pot = nullptr;          // ntarg*nd (x2 if complex)
+  void* strengths = nullptr;      // nptso*nd*(2 or 4) reals of the far precision
+  double* partial = nullptr;      // nchunks*ntarg*nd*(1 or 2)
+  const void* weff = nullptr;     // W_eff in f64 or f32
+  int weff_f32 = 0;
+};
+
+cudaError_t launch_strengths(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                             cudaStream_t st);
+cudaError_t launch_far(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                       cudaStream_t st);
+cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
+                           const MatvecArgs& a, cudaStream_t st);
+// W_eff = wnear - [K(t_i, y_l) w_l]_l * imat  for every near pair, in f64.
+cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp,
+                        const double* wnear, double* weff, cudaStream_t st);
+cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t st);
+
+// Number of source chunks the far kernel splits the sources into (the
+// partial-potential scratch holds nchunks*ntarg*nd values).
+int far_nchunks(int64_t ntarg, int64_t nptso, int kind, int precision, int nd, int num_sms);
+
+// ---- GMRES helpers --------------------------------------------------------
+// Vectors hold npts points x nd densities (point-major), n = npts*nd values
+// (2n doubles when complex); density d is independent system d, so inner
+// products are per density.  wts are per point.
+// out[2*(k*nd+d)] + i out[2*(k*nd+d)+1] = sum_pt wts * conj(V_k[pt,d]) w[pt,d]
+// for k < m, V_k = V + k*ldv; partial needs 2*m*nd*nblk doubles.
+cudaError_t launch_mdot(const double* V, int64_t ldv, int m, const double* w,
+                        const double* wts, int64_t npts, int nd, int cplx, double* partial,
+                        int nblk, double* out, cudaStream_t st);
+// w[pt,d] -= sum_k h[k,d] V_k[pt,d]   (h complex on device, layout as out)
+cudaError_t launch_maxpy(const double* V, int64_t ldv, int m, const double* h, double* w,
+                         int64_t n, int nd, int cplx, cudaStream_t st);
+// y[pt,d] = s[d] x[pt,d], s complex on device (y may alias x)
+cudaError_t launch_dscale(const double* x, double* y, const double* s, int64_t n, int nd,
+                          int cplx, cudaStream_t st);
+// y = a x + b y with scalar complex a = (ar, ai), b = (br, bi)
+cudaError_t launch_axpby(const double* x, double* y, double ar, double ai, double br, double bi,
+                         int64_t n, int cplx, cudaStream_t st);
+// y[pt,d] = sum_k c[k,d] V_k[pt,d]
+cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
+                         int64_t n, int nd, int cplx, cudaStream_t st);
+
+}  // namespace dev
+}  // namespace bie

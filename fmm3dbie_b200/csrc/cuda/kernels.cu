@@ -1,0 +1,773 @@
+// Matvec and GMRES kernels for the combined-field layer potentials (sm_100a).
+//
+// Stages of one matvec (lap_comb_dir_eval_addsub, lap_comb_dir.f90:806-1178;
+// helm_comb_dir_eval_addsub, helm_comb_dir.f:856-1210):
+//   (a) strengths : per patch, sigma_over = imat * sigma_patch
+//                   (oversample_fun_guru, surf_routs.f90:511-591), scaled to
+//                   charge alpha*w/(4pi) and dipole beta*w/(4pi) strengths;
+//   (b) far       : direct sum over all oversampled sources for every
+//                   target, skipping r^2 < thresh^2 (stands in for
+//                   lfmm3d / hfmm3d, including their self-interaction rule);
+//   (c) combine   : pot_i = sum of far partials + sum_k W_eff(k) . sigma,
+//                   W_eff = wnear - smooth near part (folded once per plan,
+//                   replacing the per-call l3ddirectcdp/h3ddirectcdp subtraction).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "device.cuh"
+
+namespace bie {
+namespace dev {
+
+namespace {
+
+constexpr double kOver4Pi = 0.07957747154594767;
+
+template <typename R>
+struct Vec;
+template <>
+struct Vec<float> {
+  using T2 = float2;
+  using T4 = float4;
+};
+template <>
+struct Vec<double> {
+  using T2 = double2;
+  using T4 = double4;
+};
+
+// ---------------------------------------------------------------------------
+// (a) strengths
+// ---------------------------------------------------------------------------
+template <typename R, int CPLX>
+__global__ void strengths_kernel(Geometry g, KParams kp, const double* __restrict__ sigma,
+                                 R* __restrict__ str, int nd) {
+  extern __shared__ double sh[];
+  const int p = blockIdx.x;
+  const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
+  const int os = g.ostart[p], nf = g.ostart[p + 1] - os;
+  const double* M = g.imat + g.cmoff[g.pclass[p]];
+  const int vals = np * nd * (CPLX ? 2 : 1);
+  for (int q = threadIdx.x; q < vals; q += blockDim.x) sh[q] = sigma[size_t(ps) * nd * (CPLX ? 2 : 1) + q];
+  __syncthreads();
+  for (int q = threadIdx.x; q < nf * nd; q += blockDim.x) {
+    const int l = q / nd, m = q - l * nd;
+    const double* row = M + size_t(l) * np;
+    double sr = 0, si = 0;
+    if (CPLX) {
+      for (int j = 0; j < np; ++j) {
+        const double mv = row[j];
+        sr = fma(mv, sh[2 * (j * nd + m)], sr);
+        si = fma(mv, sh[2 * (j * nd + m) + 1], si);
+      }
+    } else {
+      for (int j = 0; j < np; ++j) sr = fma(row[j], sh[j * nd + m], sr);
+    }
+    const double f = g.sw[os + l] * kOver4Pi;
+    const size_t o = size_t(os + l) * nd + m;
+    if (CPLX) {
+      // c = alpha * sigma_over * f, d = beta * sigma_over * f
+      str[4 * o + 0] = R((kp.ar * sr - kp.ai * si) * f);
+      str[4 * o + 1] = R((kp.ar * si + kp.ai * sr) * f);
+      str[4 * o + 2] = R((kp.br * sr - kp.bi * si) * f);
+      str[4 * o + 3] = R((kp.br * si + kp.bi * sr) * f);
+    } else {
+      str[2 * o + 0] = R(kp.ar * sr * f);
+      str[2 * o + 1] = R(kp.br * sr * f);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// (b) far field: tiled direct N-body
+// ---------------------------------------------------------------------------
+// 2*pi split for Cody-Waite reduction: kHi has 8 significant bits so n*kHi
+// is exact for |n| < 2^16; kLo = 2*pi - kHi rounded to float.
+constexpr float kTwoPiHi = 6.28125f;
+constexpr float kTwoPiLo = 1.9353071795864769253e-3f;
+constexpr float kInvTwoPi = 0.15915494309189533577f;
+
+__device__ __forceinline__ void pair_helm(float tx, float ty, float tz, const float4 g0,
+                                          const float2 g1, const float4 s, float k, float kim,
+                                          float thr2, bool ck, float& pr, float& pi) {
+  const float dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float rinv = (r2 >= thr2) ? rsqrtf(r2) : 0.0f;
+  const float r = r2 * rinv;
+  const float kr = k * r;
+  const float nrev = rintf(kr * kInvTwoPi);
+  float xr = fmaf(-nrev, kTwoPiHi, kr);
+  xr = fmaf(-nrev, kTwoPiLo, xr);
+  float sn, cs;
+  __sincosf(xr, &sn, &cs);
+  float rs = rinv;
+  if (ck) rs *= __expf(-kim * r);
+  const float dn = fmaf(dx, g0.w, fmaf(dy, g1.x, dz * g1.y));
+  // dipole factor d * (n.(t-s)) (1 - i k r) / r^2 with complex k
+  const float q = dn * rinv * rinv;
+  const float wr = ck ? q * (1.0f + kim * r) : q;
+  const float wi = -q * kr;
+  const float er = fmaf(s.z, wr, fmaf(-s.w, wi, s.x)) * rs;
+  const float ei = fmaf(s.z, wi, fmaf(s.w, wr, s.y)) * rs;
+  pr = fmaf(cs, er, fmaf(-sn, ei, pr));
+  pi = fmaf(cs, ei, fmaf(sn, er, pi));
+}
+
+__device__ __forceinline__ void pair_helm(double tx, double ty, double tz, const double4 g0,
+                                          const double2 g1, const double4 s, double k, double kim,
+                                          double thr2, bool ck, double& pr, double& pi) {
+  const double dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  const bool ok = r2 >= thr2;
+  const double rinv = ok ? rsqrt(r2) : 0.0;
+  const double r = r2 * rinv;
+  const double kr = k * r;
+  double sn, cs;
+  sincos(kr, &sn, &cs);
+  double rs = rinv;
+  if (ck) rs *= exp(-kim * r);
+  const double dn = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y));
+  const double q = dn * rinv * rinv;
+  const double wr = ck ? q * (1.0 + kim * r) : q;
+  const double wi = -q * kr;
+  const double er = fma(s.z, wr, fma(-s.w, wi, s.x)) * rs;
+  const double ei = fma(s.z, wi, fma(s.w, wr, s.y)) * rs;
+  pr = fma(cs, er, fma(-sn, ei, pr));
+  pi = fma(cs, ei, fma(sn, er, pi));
+}
+
+template <typename R>
+__device__ __forceinline__ void pair_lap(R tx, R ty, R tz, const typename Vec<R>::T4 g0,
+                                         const typename Vec<R>::T2 g1,
+                                         const typename Vec<R>::T2 s, R thr2, R& p) {
+  const R dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const R r2 = dx * dx + dy * dy + dz * dz;
+  R rinv;
+  if constexpr (sizeof(R) == 4)
+    rinv = (r2 >= thr2) ? rsqrtf(r2) : R(0);
+  else
+    rinv = (r2 >= thr2) ? rsqrt(r2) : R(0);
+  const R dn = dx * g0.w + dy * g1.x + dz * g1.y;
+  const R e = s.x + s.y * dn * (rinv * rinv);
+  p += e * rinv;
+}
+
+template <int KIND, typename R, int NT, int TPT, int TILE, bool CK>
+__global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R* __restrict__ str,
+                                                 double* __restrict__ partial, int64_t chunk_len,
+                                                 int nd) {
+  using R2 = typename Vec<R>::T2;
+  using R4 = typename Vec<R>::T4;
+  constexpr int SW = (KIND == 1) ? 4 : 2;  // strength reals per source
+  __shared__ R4 sg0[TILE];
+  __shared__ R2 sg1[TILE];
+  __shared__ R sst[TILE * SW];
+  const int64_t ntarg = g.ntarg, nptso = g.nptso;
+  const int64_t tbase = int64_t(blockIdx.x) * NT * TPT;
+  const int m = blockIdx.z;  // density index
+  // Coordinates are shifted by the block's first target so that nearby
+  // pairs keep their relative accuracy in single precision.
+  const int64_t tc = tbase < ntarg ? tbase : ntarg - 1;
+  const double cx = g.tx[tc], cy = g.ty[tc], cz = g.tz[tc];
+  R tx[TPT], ty[TPT], tz[TPT];
+  double accr[TPT], acci[TPT];
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    const int64_t it = tbase + threadIdx.x + int64_t(t) * NT;
+    const int64_t ic = it < ntarg ? it : ntarg - 1;
+    tx[t] = R(g.tx[ic] - cx);
+    ty[t] = R(g.ty[ic] - cy);
+    tz[t] = R(g.tz[ic] - cz);
+    accr[t] = 0.0;
+    acci[t] = 0.0;
+  }
+  const R thr2 = R(kp.thresh * kp.thresh);
+  const R k = R(kp.kr), kim = R(kp.ki);
+  const int64_t s0 = int64_t(blockIdx.y) * chunk_len;
+  const int64_t s1 = min(s0 + chunk_len, nptso);
+  for (int64_t sb = s0; sb < s1; sb += TILE) {
+    const int ns = int((s1 - sb) < TILE ? (s1 - sb) : TILE);
+    __syncthreads();
+    for (int q = threadIdx.x; q < TILE; q += NT) {
+      if (q < ns) {
+        const int64_t s = sb + q;
+        sg0[q] = R4{R(g.sx[s] - cx), R(g.sy[s] - cy), R(g.sz[s] - cz), R(g.snx[s])};
+        sg1[q] = R2{R(g.sny[s]), R(g.snz[s])};
+#pragma unroll
+        for (int c = 0; c < SW; ++c) sst[q * SW + c] = str[(size_t(s) * nd + m) * SW + c];
+      } else {
+        sg0[q] = R4{R(0), R(0), R(0), R(0)};
+        sg1[q] = R2{R(0), R(0)};
+#pragma unroll
+        for (int c = 0; c < SW; ++c) sst[q * SW + c] = R(0);
+      }
+    }
+    __syncthreads();
+    R pr[TPT], pi[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) pr[t] = pi[t] = R(0);
+#pragma unroll 2
+    for (int j = 0; j < TILE; ++j) {
+      const R4 a = sg0[j];
+      const R2 b = sg1[j];
+      if constexpr (KIND == 1) {
+        const R4 s = reinterpret_cast<const R4*>(sst)[j];
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) pair_helm(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, pr[t], pi[t]);
+      } else {
+        const R2 s = reinterpret_cast<const R2*>(sst)[j];
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) pair_lap<R>(tx[t], ty[t], tz[t], a, b, s, thr2, pr[t]);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+      accr[t] += double(pr[t]);
+      acci[t] += double(pi[t]);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    const int64_t it = tbase + threadIdx.x + int64_t(t) * NT;
+    if (it >= ntarg) continue;
+    const size_t o = (size_t(blockIdx.y) * ntarg + it) * nd + m;
+    if (KIND == 1) {
+      partial[2 * o] = accr[t];
+      partial[2 * o + 1] = acci[t];
+    } else {
+      partial[o] = accr[t];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// (c) combine: far partials + near-correction SpMM, one warp per target row
+// ---------------------------------------------------------------------------
+template <int CPLX, typename W>
+__global__ void combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
+                               const double* __restrict__ sigma, const double* __restrict__ partial,
+                               int nchunks, double* __restrict__ pot, int nd) {
+  const int lane = threadIdx.x & 31;
+  const int64_t i = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (i >= g.ntarg) return;
+  const int64_t ntarg = g.ntarg;
+  const int64_t k0 = nr.row_ptr[i], k1 = nr.row_ptr[i + 1];
+  if (nd == 1) {
+    double ar = 0, ai = 0;
+    for (int c = lane; c < nchunks; c += 32) {
+      const size_t o = size_t(c) * ntarg + i;
+      if (CPLX) {
+        ar += partial[2 * o];
+        ai += partial[2 * o + 1];
+      } else {
+        ar += partial[o];
+      }
+    }
+    // lanes are grouped per near patch: G lanes per patch, 32/G patches at once
+    for (int64_t kb = k0; kb < k1;) {
+      const int p0 = nr.col[kb];
+      const int npv = g.pstart[p0 + 1] - g.pstart[p0];
+      const int G = npv > 16 ? 32 : (npv > 8 ? 16 : 8);
+      const int per = 32 / G;
+      const int64_t k = kb + lane / G;
+      if (k < k1) {
+        const int p = nr.col[k];
+        const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
+        const int64_t wb = nr.wofs[k];
+        for (int mm = lane % G; mm < np; mm += G) {
+          if (CPLX) {
+            const double wr = double(weff[2 * (wb + mm)]), wi = double(weff[2 * (wb + mm) + 1]);
+            const double sr = sigma[2 * (ps + mm)], si = sigma[2 * (ps + mm) + 1];
+            ar = fma(wr, sr, fma(-wi, si, ar));
+            ai = fma(wr, si, fma(wi, sr, ai));
+          } else {
+            ar = fma(double(weff[wb + mm]), sigma[ps + mm], ar);
+          }
+        }
+      }
+      kb += per;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      ar += __shfl_xor_sync(0xffffffffu, ar, off);
+      if (CPLX) ai += __shfl_xor_sync(0xffffffffu, ai, off);
+    }
+    if (lane == 0) {
+      if (CPLX) {
+        pot[2 * i] = ar;
+        pot[2 * i + 1] = ai;
+      } else {
+        pot[i] = ar;
+      }
+    }
+    return;
+  }
+  // several densities per point: lanes run over densities
+  for (int m = lane; m < nd; m += 32) {
+    double ar = 0, ai = 0;
+    for (int c = 0; c < nchunks; ++c) {
+      const size_t o = (size_t(c) * ntarg + i) * nd + m;
+      if (CPLX) {
+        ar += partial[2 * o];
+        ai += partial[2 * o + 1];
+      } else {
+        ar += partial[o];
+      }
+    }
+    for (int64_t k = k0; k < k1; ++k) {
+      const int p = nr.col[k];
+      const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
+      const int64_t wb = nr.wofs[k];
+      for (int mm = 0; mm < np; ++mm) {
+        const size_t so = size_t(ps + mm) * nd + m;
+        if (CPLX) {
+          const double wr = double(weff[2 * (wb + mm)]), wi = double(weff[2 * (wb + mm) + 1]);
+          const double sr = sigma[2 * so], si = sigma[2 * so + 1];
+          ar = fma(wr, sr, fma(-wi, si, ar));
+          ai = fma(wr, si, fma(wi, sr, ai));
+        } else {
+          ar = fma(double(weff[wb + mm]), sigma[so], ar);
+        }
+      }
+    }
+    const size_t o = size_t(i) * nd + m;
+    if (CPLX) {
+      pot[2 * o] = ar;
+      pot[2 * o + 1] = ai;
+    } else {
+      pot[o] = ar;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fold: W_eff = wnear - (smooth oversampled contribution) for each near pair
+// ---------------------------------------------------------------------------
+template <int CPLX>
+__global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __restrict__ wnear,
+                            double* __restrict__ weff) {
+  extern __shared__ double sh[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* a = sh + size_t(warp) * g.max_nf * 2;
+  // find the row of pair k by binary search over row_ptr
+  const int64_t k = int64_t(blockIdx.x) * (blockDim.x >> 5) + warp;
+  if (k >= nr.nnz) return;
+  int64_t lo = 0, hi = g.ntarg;  // row_ptr[lo] <= k < row_ptr[hi]
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (nr.row_ptr[mid] <= k)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const int64_t i = lo;
+  const double tx = g.tx[i], ty = g.ty[i], tz = g.tz[i];
+  const int p = nr.col[k];
+  const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
+  const int os = g.ostart[p], nf = g.ostart[p + 1] - os;
+  const double* M = g.imat + g.cmoff[g.pclass[p]];
+  const double thr2 = kp.thresh * kp.thresh;
+  for (int l = lane; l < nf; l += 32) {
+    const int s = os + l;
+    const double dx = tx - g.sx[s], dy = ty - g.sy[s], dz = tz - g.sz[s];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    double vr = 0, vi = 0;
+    if (r2 >= thr2) {
+      const double r = sqrt(r2), rinv = 1.0 / r;
+      const double dn = dx * g.snx[s] + dy * g.sny[s] + dz * g.snz[s];
+      const double f = g.sw[s] * kOver4Pi;
+      if (CPLX) {
+        double sn, cs;
+        sincos(kp.kr * r, &sn, &cs);
+        const double damp = exp(-kp.ki * r);
+        const double er = cs * damp * rinv, ei = sn * damp * rinv;  // e^{ikr}/r
+        // (1 - i k r) with complex k: 1 + ki r - i kr r
+        const double qr = dn * rinv * rinv * (1.0 + kp.ki * r), qi = -dn * rinv * rinv * kp.kr * r;
+        // alpha + beta*q
+        const double cr = kp.ar + kp.br * qr - kp.bi * qi;
+        const double ci = kp.ai + kp.br * qi + kp.bi * qr;
+        vr = (cr * er - ci * ei) * f;
+        vi = (cr * ei + ci * er) * f;
+      } else {
+        vr = (kp.ar + kp.br * dn * rinv * rinv) * rinv * f;
+      }
+    }
+    a[2 * l] = vr;
+    a[2 * l + 1] = vi;
+  }
+  __syncwarp();
+  const int64_t wb = nr.wofs[k];
+  for (int mm = lane; mm < np; mm += 32) {
+    double sr = 0, si = 0;
+    for (int l = 0; l < nf; ++l) {
+      const double mv = M[size_t(l) * np + mm];
+      sr = fma(a[2 * l], mv, sr);
+      si = fma(a[2 * l + 1], mv, si);
+    }
+    if (CPLX) {
+      weff[2 * (wb + mm)] = wnear[2 * (wb + mm)] - sr;
+      weff[2 * (wb + mm) + 1] = wnear[2 * (wb + mm) + 1] - si;
+    } else {
+      weff[wb + mm] = wnear[wb + mm] - sr;
+    }
+  }
+}
+
+__global__ void to_f32_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = float(in[i]);
+}
+
+// ---------------------------------------------------------------------------
+// GMRES vector kernels.  Vectors hold npts points x nd densities
+// (point-major); the nd densities are nd independent systems, so every
+// inner product is segmented by density index.
+// ---------------------------------------------------------------------------
+template <int CPLX>
+__global__ void mdot_partial_kernel(const double* __restrict__ V, int64_t ldv, int m,
+                                    const double* __restrict__ w, const double* __restrict__ wts,
+                                    int64_t npts, int nd, double* __restrict__ partial) {
+  __shared__ double2 red[256];
+  const int tid = threadIdx.x;
+  const int rows = blockDim.x / nd;  // blockDim.x is a multiple of nd
+  const int dd = tid % nd, r = tid / nd;
+  for (int k = 0; k < m; ++k) {
+    const double* v = V + size_t(k) * ldv;
+    double sr = 0, si = 0;
+    for (int64_t pt = int64_t(blockIdx.x) * rows + r; pt < npts; pt += int64_t(gridDim.x) * rows) {
+      const int64_t e = pt * nd + dd;
+      const double wt = wts[pt];
+      if (CPLX) {
+        const double vr = v[2 * e], vi = v[2 * e + 1], xr = w[2 * e], xi = w[2 * e + 1];
+        sr += wt * (vr * xr + vi * xi);
+        si += wt * (vr * xi - vi * xr);
+      } else {
+        sr += wt * v[e] * w[e];
+      }
+    }
+    red[tid] = make_double2(sr, si);
+    __syncthreads();
+    if (tid < nd) {
+      double ar = 0, ai = 0;
+      for (int q = 0; q < rows; ++q) {
+        ar += red[q * nd + tid].x;
+        ai += red[q * nd + tid].y;
+      }
+      const size_t o = (size_t(k) * nd + tid) * gridDim.x + blockIdx.x;
+      partial[2 * o] = ar;
+      partial[2 * o + 1] = ai;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void mdot_final_kernel(const double* __restrict__ partial, int nblk,
+                                  double* __restrict__ out) {
+  __shared__ double red[2][32];
+  const int k = blockIdx.x;  // flattened (k, density)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double sr = 0, si = 0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    sr += partial[2 * (size_t(k) * nblk + b)];
+    si += partial[2 * (size_t(k) * nblk + b) + 1];
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    sr += __shfl_xor_sync(0xffffffffu, sr, off);
+    si += __shfl_xor_sync(0xffffffffu, si, off);
+  }
+  if (lane == 0) {
+    red[0][warp] = sr;
+    red[1][warp] = si;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    sr = lane < nw ? red[0][lane] : 0.0;
+    si = lane < nw ? red[1][lane] : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, off);
+      si += __shfl_xor_sync(0xffffffffu, si, off);
+    }
+    if (lane == 0) {
+      out[2 * k] = sr;
+      out[2 * k + 1] = si;
+    }
+  }
+}
+
+// w[pt,d] -= sum_k h[k,d] V_k[pt,d]
+template <int CPLX>
+__global__ void maxpy_kernel(const double* __restrict__ V, int64_t ldv, int m,
+                             const double* __restrict__ h, double* __restrict__ w, int64_t n,
+                             int nd) {
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int dd = int(e % nd);
+    if (CPLX) {
+      double xr = w[2 * e], xi = w[2 * e + 1];
+      for (int k = 0; k < m; ++k) {
+        const double hr = h[2 * (k * nd + dd)], hi = h[2 * (k * nd + dd) + 1];
+        const double vr = V[size_t(k) * ldv + 2 * e], vi = V[size_t(k) * ldv + 2 * e + 1];
+        xr -= hr * vr - hi * vi;
+        xi -= hr * vi + hi * vr;
+      }
+      w[2 * e] = xr;
+      w[2 * e + 1] = xi;
+    } else {
+      double x = w[e];
+      for (int k = 0; k < m; ++k) x -= h[2 * (k * nd + dd)] * V[size_t(k) * ldv + e];
+      w[e] = x;
+    }
+  }
+}
+
+// y[pt,d] = sum_k c[k,d] V_k[pt,d]
+template <int CPLX>
+__global__ void combo_kernel(const double* __restrict__ V, int64_t ldv, int m,
+                             const double* __restrict__ c, double* __restrict__ y, int64_t n,
+                             int nd) {
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int dd = int(e % nd);
+    double xr = 0, xi = 0;
+    for (int k = 0; k < m; ++k) {
+      const double cr = c[2 * (k * nd + dd)], ci = c[2 * (k * nd + dd) + 1];
+      if (CPLX) {
+        const double vr = V[size_t(k) * ldv + 2 * e], vi = V[size_t(k) * ldv + 2 * e + 1];
+        xr += cr * vr - ci * vi;
+        xi += cr * vi + ci * vr;
+      } else {
+        xr += cr * V[size_t(k) * ldv + e];
+      }
+    }
+    if (CPLX) {
+      y[2 * e] = xr;
+      y[2 * e + 1] = xi;
+    } else {
+      y[e] = xr;
+    }
+  }
+}
+
+// y = a*x + b*y, scalar complex a, b
+template <int CPLX>
+__global__ void axpby_kernel(const double* __restrict__ x, double* __restrict__ y, double ar,
+                             double ai, double br, double bi, int64_t n) {
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    if (CPLX) {
+      const double xr = x[2 * e], xi = x[2 * e + 1], yr = y[2 * e], yi = y[2 * e + 1];
+      y[2 * e] = ar * xr - ai * xi + br * yr - bi * yi;
+      y[2 * e + 1] = ar * xi + ai * xr + br * yi + bi * yr;
+    } else {
+      y[e] = ar * x[e] + br * y[e];
+    }
+  }
+}
+
+// y[pt,d] = s[d] * x[pt,d] with s complex, on device
+template <int CPLX>
+__global__ void dscale_kernel(const double* __restrict__ x, double* __restrict__ y,
+                              const double* __restrict__ s, int64_t n, int nd) {
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int dd = int(e % nd);
+    const double sr = s[2 * dd], si = s[2 * dd + 1];
+    if (CPLX) {
+      const double xr = x[2 * e], xi = x[2 * e + 1];
+      y[2 * e] = sr * xr - si * xi;
+      y[2 * e + 1] = sr * xi + si * xr;
+    } else {
+      y[e] = sr * x[e];
+    }
+  }
+}
+
+inline int grid_for(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > 148 * 16) b = 148 * 16;
+  return int(b);
+}
+
+// Far-kernel launch shapes.
+constexpr int kFarThreads = 128;
+constexpr int kFarTile = 128;
+constexpr int kTptF32 = 4;
+constexpr int kTptF64 = 2;
+
+}  // namespace
+
+int far_nchunks(int64_t ntarg, int64_t nptso, int kind, int precision, int nd, int num_sms) {
+  (void)kind;
+  const int tpt = precision == 1 ? kTptF32 : kTptF64;
+  const int64_t tblocks = (ntarg + int64_t(kFarThreads) * tpt - 1) / (int64_t(kFarThreads) * tpt);
+  const int64_t want = int64_t(num_sms) * 6;  // blocks in flight over the chip
+  int64_t s = (want + tblocks * nd - 1) / (tblocks * nd);
+  const int64_t maxs = std::max<int64_t>(1, nptso / (2 * kFarTile));
+  s = std::max<int64_t>(1, std::min<int64_t>(s, maxs));
+  return int(s);
+}
+
+cudaError_t launch_strengths(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                             cudaStream_t st) {
+  const int cplx = kp.kind == 1;
+  const size_t sh = size_t(g.max_np) * a.nd * (cplx ? 2 : 1) * sizeof(double);
+  if (sh > 200 * 1024) return cudaErrorInvalidValue;
+  const dim3 grid(static_cast<unsigned>(g.npatches)), block(128);
+  if (a.precision == 1) {
+    if (sh > 48 * 1024) {
+      cudaFuncSetAttribute(strengths_kernel<float, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
+      cudaFuncSetAttribute(strengths_kernel<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
+    }
+    if (cplx)
+      strengths_kernel<float, 1><<<grid, block, sh, st>>>(g, kp, a.sigma, (float*)a.strengths, a.nd);
+    else
+      strengths_kernel<float, 0><<<grid, block, sh, st>>>(g, kp, a.sigma, (float*)a.strengths, a.nd);
+  } else {
+    if (sh > 48 * 1024) {
+      cudaFuncSetAttribute(strengths_kernel<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
+      cudaFuncSetAttribute(strengths_kernel<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
+    }
+    if (cplx)
+      strengths_kernel<double, 1><<<grid, block, sh, st>>>(g, kp, a.sigma, (double*)a.strengths, a.nd);
+    else
+      strengths_kernel<double, 0><<<grid, block, sh, st>>>(g, kp, a.sigma, (double*)a.strengths, a.nd);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_far(const Geometry& g, const KParams& kp, const MatvecArgs& a, cudaStream_t st) {
+  if (g.ntarg == 0) return cudaSuccess;
+  const int tpt = a.precision == 1 ? kTptF32 : kTptF64;
+  const int64_t per_block = int64_t(kFarThreads) * tpt;
+  const int64_t tblocks = (g.ntarg + per_block - 1) / per_block;
+  int64_t chunk = (g.nptso + a.nchunks - 1) / a.nchunks;
+  chunk = ((chunk + kFarTile - 1) / kFarTile) * kFarTile;
+  const dim3 grid(static_cast<unsigned>(tblocks), static_cast<unsigned>(a.nchunks), static_cast<unsigned>(a.nd));
+  const dim3 block(kFarThreads);
+  const bool ck = kp.kind == 1 && kp.ki != 0.0;
+  if (a.precision == 1) {
+    const float* s = (const float*)a.strengths;
+    if (kp.kind == 1) {
+      if (ck)
+        far_kernel<1, float, kFarThreads, kTptF32, kFarTile, true><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
+      else
+        far_kernel<1, float, kFarThreads, kTptF32, kFarTile, false><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
+    } else {
+      far_kernel<0, float, kFarThreads, kTptF32, kFarTile, false><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
+    }
+  } else {
+    const double* s = (const double*)a.strengths;
+    if (kp.kind == 1) {
+      if (ck)
+        far_kernel<1, double, kFarThreads, kTptF64, kFarTile, true><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
+      else
+        far_kernel<1, double, kFarThreads, kTptF64, kFarTile, false><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
+    } else {
+      far_kernel<0, double, kFarThreads, kTptF64, kFarTile, false><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
+                           const MatvecArgs& a, cudaStream_t st) {
+  if (g.ntarg == 0) return cudaSuccess;
+  const int threads = 256;
+  const int64_t blocks = (g.ntarg * 32 + threads - 1) / threads;
+  const dim3 grid(static_cast<unsigned>(blocks)), block(threads);
+  if (kp.kind == 1) {
+    if (a.weff_f32)
+      combine_kernel<1, float><<<grid, block, 0, st>>>(g, nr, (const float*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+    else
+      combine_kernel<1, double><<<grid, block, 0, st>>>(g, nr, (const double*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+  } else {
+    if (a.weff_f32)
+      combine_kernel<0, float><<<grid, block, 0, st>>>(g, nr, (const float*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+    else
+      combine_kernel<0, double><<<grid, block, 0, st>>>(g, nr, (const double*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp, const double* wnear,
+                        double* weff, cudaStream_t st) {
+  if (nr.nnz == 0) return cudaSuccess;
+  const int warps = 4;
+  const size_t sh = size_t(warps) * g.max_nf * 2 * sizeof(double);
+  if (sh > 200 * 1024) return cudaErrorInvalidValue;
+  const dim3 grid(static_cast<unsigned>((nr.nnz + warps - 1) / warps)), block(32 * warps);
+  if (kp.kind == 1) {
+    if (sh > 48 * 1024) cudaFuncSetAttribute(fold_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
+    fold_kernel<1><<<grid, block, sh, st>>>(g, nr, kp, wnear, weff);
+  } else {
+    if (sh > 48 * 1024) cudaFuncSetAttribute(fold_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
+    fold_kernel<0><<<grid, block, sh, st>>>(g, nr, kp, wnear, weff);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  to_f32_kernel<<<grid_for(n, 256), 256, 0, st>>>(in, out, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mdot(const double* V, int64_t ldv, int m, const double* w, const double* wts,
+                        int64_t npts, int nd, int cplx, double* partial, int nblk, double* out,
+                        cudaStream_t st) {
+  if (m <= 0) return cudaSuccess;
+  if (nd < 1 || nd > 256) return cudaErrorInvalidValue;
+  const int threads = (256 / nd) * nd;
+  if (cplx)
+    mdot_partial_kernel<1><<<nblk, threads, 0, st>>>(V, ldv, m, w, wts, npts, nd, partial);
+  else
+    mdot_partial_kernel<0><<<nblk, threads, 0, st>>>(V, ldv, m, w, wts, npts, nd, partial);
+  mdot_final_kernel<<<m * nd, 256, 0, st>>>(partial, nblk, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_maxpy(const double* V, int64_t ldv, int m, const double* h, double* w,
+                         int64_t n, int nd, int cplx, cudaStream_t st) {
+  if (m <= 0) return cudaSuccess;
+  if (cplx)
+    maxpy_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, h, w, n, nd);
+  else
+    maxpy_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, h, w, n, nd);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dscale(const double* x, double* y, const double* s, int64_t n, int nd, int cplx,
+                          cudaStream_t st) {
+  if (cplx)
+    dscale_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(x, y, s, n, nd);
+  else
+    dscale_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(x, y, s, n, nd);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpby(const double* x, double* y, double ar, double ai, double br, double bi,
+                         int64_t n, int cplx, cudaStream_t st) {
+  if (cplx)
+    axpby_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(x, y, ar, ai, br, bi, n);
+  else
+    axpby_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(x, y, ar, ai, br, bi, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
+                         int64_t n, int nd, int cplx, cudaStream_t st) {
+  if (cplx)
+    combo_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, c, y, n, nd);
+  else
+    combo_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, c, y, n, nd);
+  return cudaGetLastError();
+}
+
+}  // namespace dev
+}  // namespace bie

@@ -1,0 +1,545 @@
+// Operator plan, batched GMRES and the mixed-precision refinement solver.
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "../host/basis.h"
+#include "../host/setup.h"
+
+namespace bie {
+
+namespace {
+thread_local std::string g_last_error;
+
+#define BIE_CUDA(call)                                                             \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));          \
+      return e_ == cudaErrorMemoryAllocation ? kErrNoMem : kErrCuda;               \
+    }                                                                              \
+  } while (0)
+
+template <class T>
+cudaError_t upload(DBuf<T>& b, const std::vector<T>& h, cudaStream_t st) {
+  cudaError_t e = b.alloc(std::max<size_t>(h.size(), 1));
+  if (e != cudaSuccess) return e;
+  if (h.empty()) return cudaSuccess;
+  return cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+}  // namespace
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+int Plan::build(const PlanSpec& s, cudaStream_t st) {
+  BIE_CUDA(cudaGetDevice(&device));
+  BIE_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+  kind = s.kind;
+  cplx = s.kind == 1;
+  npts = s.npts;
+  ntarg = s.ntarg;
+  nptso = s.nptso;
+  npatches = s.npatches;
+  nnz = s.nnz;
+  nquad = s.nquad;
+  // ---- validate the reference-style inputs --------------------------------
+  if (npatches <= 0 || npts <= 0 || ntarg < 0 || nptso <= 0 || nnz < 0) {
+    set_last_error("non-positive sizes");
+    return kErrArg;
+  }
+  if (s.ixyzs[0] != 1 || s.ixyzs[npatches] != npts + 1 || s.ixyzso[0] != 1 ||
+      s.ixyzso[npatches] != nptso + 1) {
+    set_last_error("ixyzs/ixyzso inconsistent with npts/nptso");
+    return kErrArg;
+  }
+  int max_np = 0, max_nf = 0;
+  for (int64_t p = 0; p < npatches; ++p) {
+    const int ip = int(s.iptype[p]), no = int(s.norders[p]), nf = int(s.novers[p]);
+    const int64_t np = s.ixyzs[p + 1] - s.ixyzs[p];
+    const int64_t nfp = s.ixyzso[p + 1] - s.ixyzso[p];
+    if (!valid_patch(ip, no) || !valid_patch(ip, nf) || np != npols_of(ip, no) ||
+        nfp != npols_of(ip, nf)) {
+      set_last_error("patch " + std::to_string(p + 1) + ": order/type/size mismatch");
+      return kErrArg;
+    }
+    max_np = std::max<int>(max_np, int(np));
+    max_nf = std::max<int>(max_nf, int(nfp));
+  }
+  if (s.row_ptr[0] != 1 || s.row_ptr[ntarg] != nnz + 1) {
+    set_last_error("row_ptr inconsistent with nnz");
+    return kErrArg;
+  }
+  for (int64_t i = 0; i < ntarg; ++i)
+    if (s.row_ptr[i + 1] < s.row_ptr[i]) {
+      set_last_error("row_ptr not monotone");
+      return kErrArg;
+    }
+  if (nnz > 0 && s.iquad[0] != 1) {
+    set_last_error("iquad(1) must be 1");
+    return kErrArg;
+  }
+  for (int64_t k = 0; k < nnz; ++k) {
+    const int64_t c = s.col_ind[k];
+    if (c < 1 || c > npatches || s.iquad[k + 1] - s.iquad[k] != s.ixyzs[c] - s.ixyzs[c - 1]) {
+      set_last_error("col_ind/iquad entry " + std::to_string(k + 1) + " invalid");
+      return kErrArg;
+    }
+  }
+  if (nnz > 0 && s.iquad[nnz] - 1 != nquad) {
+    set_last_error("nquad != iquad(nnz+1)-1");
+    return kErrArg;
+  }
+  // ---- host-side arrays ------------------------------------------------------
+  std::vector<double> htx(ntarg), hty(ntarg), htz(ntarg);
+  for (int64_t i = 0; i < ntarg; ++i) {
+    htx[i] = s.targs[size_t(s.ndtarg) * i];
+    hty[i] = s.targs[size_t(s.ndtarg) * i + 1];
+    htz[i] = s.targs[size_t(s.ndtarg) * i + 2];
+  }
+  std::vector<double> hsx(nptso), hsy(nptso), hsz(nptso), hnx(nptso), hny(nptso), hnz(nptso),
+      hw(nptso);
+  for (int64_t j = 0; j < nptso; ++j) {
+    const double* o = s.srcover + 12 * j;
+    hsx[j] = o[0];
+    hsy[j] = o[1];
+    hsz[j] = o[2];
+    hnx[j] = o[9];
+    hny[j] = o[10];
+    hnz[j] = o[11];
+    hw[j] = s.whtsover[j];
+  }
+  std::vector<int32_t> hps(npatches + 1), hos(npatches + 1), hpc(npatches);
+  std::map<std::tuple<int, int, int>, int> cls;
+  std::vector<int64_t> hcm;
+  std::vector<double> him;
+  for (int64_t p = 0; p <= npatches; ++p) {
+    hps[p] = int32_t(s.ixyzs[p] - 1);
+    hos[p] = int32_t(s.ixyzso[p] - 1);
+  }
+  for (int64_t p = 0; p < npatches; ++p) {
+    auto key = std::make_tuple(int(s.iptype[p]), int(s.norders[p]), int(s.novers[p]));
+    auto it = cls.find(key);
+    if (it == cls.end()) {
+      std::vector<double> m;
+      const int ier = interp_matrix(std::get<0>(key), std::get<1>(key), std::get<2>(key), m);
+      if (ier) {
+        set_last_error("interpolation matrix: basis tables unavailable or singular");
+        return ier == 6 ? kErrTables : kErrSingular;
+      }
+      const int id = int(hcm.size());
+      hcm.push_back(int64_t(him.size()));
+      him.insert(him.end(), m.begin(), m.end());
+      it = cls.emplace(key, id).first;
+    }
+    hpc[p] = it->second;
+  }
+  std::vector<int64_t> hrp(ntarg + 1), hwo(nnz + 1);
+  std::vector<int32_t> hcol(nnz);
+  for (int64_t i = 0; i <= ntarg; ++i) hrp[i] = s.row_ptr[i] - 1;
+  for (int64_t k = 0; k < nnz; ++k) {
+    hcol[k] = int32_t(s.col_ind[k] - 1);
+    hwo[k] = s.iquad[k] - 1;
+  }
+  hwo[nnz] = nquad;
+  // smooth quadrature weights at the nodes (needed by the GMRES inner product)
+  std::vector<double> hqw(npts);
+  {
+    Surf sf;
+    sf.npatches = npatches;
+    sf.npts = npts;
+    sf.norders = s.norders;
+    sf.ixyzs = s.ixyzs;
+    sf.iptype = s.iptype;
+    sf.srccoefs = s.srccoefs;
+    sf.srcvals = s.srcvals;
+    qwts(sf, hqw.data());
+  }
+  kp.kind = kind;
+  kp.ar = s.alpha.real();
+  kp.ai = s.alpha.imag();
+  kp.br = s.beta.real();
+  kp.bi = s.beta.imag();
+  kp.kr = s.zk.real();
+  kp.ki = s.zk.imag();
+  if (kind == 0) kp.ai = kp.bi = kp.kr = kp.ki = 0.0;
+  kp.thresh = fmm_thresh(nptso, s.srcover, 12, ntarg, s.targs, s.ndtarg);
+  // ---- upload ----------------------------------------------------------------
+  BIE_CUDA(upload(tx_, htx, st));
+  BIE_CUDA(upload(ty_, hty, st));
+  BIE_CUDA(upload(tz_, htz, st));
+  BIE_CUDA(upload(sx_, hsx, st));
+  BIE_CUDA(upload(sy_, hsy, st));
+  BIE_CUDA(upload(sz_, hsz, st));
+  BIE_CUDA(upload(snx_, hnx, st));
+  BIE_CUDA(upload(sny_, hny, st));
+  BIE_CUDA(upload(snz_, hnz, st));
+  BIE_CUDA(upload(sw_, hw, st));
+  BIE_CUDA(upload(pstart_, hps, st));
+  BIE_CUDA(upload(ostart_, hos, st));
+  BIE_CUDA(upload(pclass_, hpc, st));
+  BIE_CUDA(upload(cmoff_, hcm, st));
+  BIE_CUDA(upload(imat_, him, st));
+  BIE_CUDA(upload(row_ptr_, hrp, st));
+  BIE_CUDA(upload(col_, hcol, st));
+  BIE_CUDA(upload(wofs_, hwo, st));
+  BIE_CUDA(upload(wts_, hqw, st));
+  g.ntarg = ntarg;
+  g.nptso = nptso;
+  g.npatches = npatches;
+  g.npts = npts;
+  g.tx = tx_.p;
+  g.ty = ty_.p;
+  g.tz = tz_.p;
+  g.sx = sx_.p;
+  g.sy = sy_.p;
+  g.sz = sz_.p;
+  g.snx = snx_.p;
+  g.sny = sny_.p;
+  g.snz = snz_.p;
+  g.sw = sw_.p;
+  g.pstart = pstart_.p;
+  g.ostart = ostart_.p;
+  g.pclass = pclass_.p;
+  g.cmoff = cmoff_.p;
+  g.imat = imat_.p;
+  g.max_np = max_np;
+  g.max_nf = max_nf;
+  nr.nnz = nnz;
+  nr.nquad = nquad;
+  nr.row_ptr = row_ptr_.p;
+  nr.col = col_.p;
+  nr.wofs = wofs_.p;
+  // ---- fold the smooth near part into W_eff (in place over wnear) -----------
+  const size_t wlen = size_t(nquad) * (cplx ? 2 : 1);
+  BIE_CUDA(weff64_.alloc(std::max<size_t>(wlen, 1)));
+  if (wlen) BIE_CUDA(cudaMemcpyAsync(weff64_.p, s.wnear, wlen * sizeof(double), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff64_.p, st));
+  if (s.keep_f32) {
+    BIE_CUDA(weff32_.alloc(std::max<size_t>(wlen, 1)));
+    BIE_CUDA(dev::launch_to_f32(weff64_.p, weff32_.p, int64_t(wlen), st));
+  }
+  for (auto& e : ev_) BIE_CUDA(cudaEventCreate(&e));
+  // host vectors above are consumed by async copies: wait before they go
+  BIE_CUDA(cudaStreamSynchronize(st));
+  return kOk;
+}
+
+int Plan::nchunks_for(int precision, int nd) const {
+  return dev::far_nchunks(ntarg, nptso, kind, precision, nd, num_sms);
+}
+
+int Plan::ensure_workspace(int precision, int nd) {
+  const int nch = nchunks_for(precision, nd);
+  const size_t sreals = size_t(nptso) * nd * (cplx ? 4 : 2);
+  BIE_CUDA(str_.alloc(sreals * sizeof(double)));
+  BIE_CUDA(partial_.alloc(std::max<size_t>(1, size_t(nch) * ntarg * nd * (cplx ? 2 : 1))));
+  return kOk;
+}
+
+int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cudaStream_t st) {
+  if (nd < 1) return kErrArg;
+  if (precision == 1 && !weff32_.p) {
+    set_last_error("plan built without an f32 copy of W_eff");
+    return kErrArg;
+  }
+  int ier = ensure_workspace(precision, nd);
+  if (ier) return ier;
+  dev::MatvecArgs a;
+  a.precision = precision;
+  a.nd = nd;
+  a.nchunks = nchunks_for(precision, nd);
+  a.sigma = d_sigma;
+  a.pot = d_pot;
+  a.strengths = str_.p;
+  a.partial = partial_.p;
+  a.weff = precision == 1 ? (const void*)weff32_.p : (const void*)weff64_.p;
+  a.weff_f32 = precision == 1;
+  if (timing) BIE_CUDA(cudaEventRecord(ev_[0], st));
+  BIE_CUDA(dev::launch_strengths(g, kp, a, st));
+  if (timing) BIE_CUDA(cudaEventRecord(ev_[1], st));
+  BIE_CUDA(dev::launch_far(g, kp, a, st));
+  if (timing) BIE_CUDA(cudaEventRecord(ev_[2], st));
+  BIE_CUDA(dev::launch_combine(g, nr, kp, a, st));
+  if (timing) {
+    BIE_CUDA(cudaEventRecord(ev_[3], st));
+    BIE_CUDA(cudaEventSynchronize(ev_[3]));
+    float t01, t12, t23;
+    cudaEventElapsedTime(&t01, ev_[0], ev_[1]);
+    cudaEventElapsedTime(&t12, ev_[1], ev_[2]);
+    cudaEventElapsedTime(&t23, ev_[2], ev_[3]);
+    times.strengths_ms += t01;
+    times.far_ms += t12;
+    times.combine_ms += t23;
+    times.calls += 1;
+  }
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// GMRES
+// ---------------------------------------------------------------------------
+namespace {
+// zrotmat_gmres (rotmat_gmres.f:60-100)
+inline void rotmat(cdouble a, cdouble b, cdouble& c, cdouble& s) {
+  if (a == cdouble(0)) {
+    s = 1.0;
+    c = 0.0;
+  } else {
+    const cdouble t = b / a;
+    c = 1.0 / std::sqrt(1.0 + std::norm(t));
+    s = t * c;
+  }
+}
+
+}  // namespace
+
+int gmres(Plan& P, int precision, int rres_precision, int nd, cdouble zid, const double* d_rhs,
+          const double* d_x0, int64_t numit, double eps_gmres, double* d_soln, GmresOut& out,
+          cudaStream_t st) {
+  if (!P.targets_on_surface || P.ntarg != P.npts) {
+    set_last_error("GMRES needs a plan whose targets are the surface nodes");
+    return kErrArg;
+  }
+  if (numit < 1 || nd < 1 || nd > 256) return kErrArg;
+  const int cplx = P.cplx ? 1 : 0;
+  const int64_t npts = P.npts, n = npts * nd;
+  const int64_t ldv = n * (cplx ? 2 : 1);
+  const int nblk = std::min<int>(2 * P.num_sms, int((npts + 63) / 64) + 1);
+  GmresWorkspace& ws = P.gws;
+  BIE_CUDA(ws.V.alloc(size_t(ldv) * (numit + 1)));
+  BIE_CUDA(ws.w.alloc(size_t(ldv)));
+  BIE_CUDA(ws.partial.alloc(size_t(2) * (numit + 1) * nd * nblk));
+  BIE_CUDA(ws.dots.alloc(size_t(2) * 3 * (numit + 1) * nd));
+  BIE_CUDA(ws.coef.alloc(size_t(2) * (numit + 1) * nd));
+  BIE_CUDA(ws.scale.alloc(size_t(2) * nd));
+  double* d_h1 = ws.dots.p;
+  double* d_h2 = ws.dots.p + 2 * (numit + 1) * nd;
+  double* d_nrm = ws.dots.p + 4 * (numit + 1) * nd;
+  const double* wts = P.d_wts();
+  double* V = ws.V.p;
+  // residual start: r0 = rhs - (zid x0 + K x0)  (stored in V_0 before scaling)
+  if (d_x0) {
+    int ier = P.matvec(precision, nd, d_x0, V, st);
+    if (ier) return ier;
+    // V0 = -(zid x0 + K x0) + rhs
+    BIE_CUDA(dev::launch_axpby(d_x0, V, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
+    BIE_CUDA(dev::launch_axpby(d_rhs, V, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+  } else {
+    BIE_CUDA(cudaMemcpyAsync(V, d_rhs, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  BIE_CUDA(dev::launch_mdot(V, ldv, 1, V, wts, npts, nd, cplx, ws.partial.p, nblk, d_nrm, st));
+  std::vector<double> hbuf(2 * (numit + 1) * nd * 2 + 2 * nd);
+  BIE_CUDA(cudaMemcpyAsync(hbuf.data(), d_nrm, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+  BIE_CUDA(cudaStreamSynchronize(st));
+  std::vector<double> rb(nd);
+  std::vector<double> hscale(2 * nd, 0.0);
+  for (int d = 0; d < nd; ++d) {
+    rb[d] = std::sqrt(std::max(hbuf[2 * d], 0.0));
+    hscale[2 * d] = rb[d] > 0 ? 1.0 / rb[d] : 0.0;
+  }
+  BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nd * sizeof(double), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(dev::launch_dscale(V, V, ws.scale.p, n, nd, cplx, st));
+  // per-system Hessenberg columns, rotations and residual vector
+  const int64_t M = numit;
+  std::vector<cdouble> H(size_t(nd) * (M + 1) * M), cs(size_t(nd) * M), sn(size_t(nd) * M),
+      sv(size_t(nd) * (M + 1));
+  std::vector<int64_t> done(nd, 0);
+  out.niter.assign(nd, 0);
+  out.errs.assign(size_t(nd) * (M + 1), 0.0);
+  out.rres.assign(nd, 0.0);
+  out.status = kOk;
+  int nactive = 0;
+  for (int d = 0; d < nd; ++d) {
+    sv[size_t(d) * (M + 1)] = rb[d];
+    if (rb[d] == 0.0) done[d] = -1;  // zero right-hand side: solution 0
+    else ++nactive;
+  }
+  auto Hc = [&](int d, int64_t row, int64_t col) -> cdouble& {
+    return H[(size_t(d) * M + col) * (M + 1) + row];
+  };
+  std::vector<double> hh1(2 * (M + 1) * nd), hh2(2 * (M + 1) * nd), hn(2 * nd);
+  int64_t it = 0;
+  for (; it < M && nactive > 0; ++it) {
+    double* vit = V + size_t(it) * ldv;
+    double* vnext = V + size_t(it + 1) * ldv;
+    int ier = P.matvec(precision, nd, vit, ws.w.p, st);
+    if (ier) return ier;
+    const int m = int(it + 1);
+    BIE_CUDA(dev::launch_mdot(V, ldv, m, ws.w.p, wts, npts, nd, cplx, ws.partial.p, nblk, d_h1, st));
+    BIE_CUDA(dev::launch_maxpy(V, ldv, m, d_h1, ws.w.p, n, nd, cplx, st));
+    BIE_CUDA(dev::launch_mdot(V, ldv, m, ws.w.p, wts, npts, nd, cplx, ws.partial.p, nblk, d_h2, st));
+    BIE_CUDA(dev::launch_maxpy(V, ldv, m, d_h2, ws.w.p, n, nd, cplx, st));
+    BIE_CUDA(dev::launch_mdot(ws.w.p, ldv, 1, ws.w.p, wts, npts, nd, cplx, ws.partial.p, nblk, d_nrm, st));
+    BIE_CUDA(cudaMemcpyAsync(hh1.data(), d_h1, 2 * m * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaMemcpyAsync(hh2.data(), d_h2, 2 * m * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaMemcpyAsync(hn.data(), d_nrm, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    for (int d = 0; d < nd; ++d) {
+      hscale[2 * d] = 0.0;
+      hscale[2 * d + 1] = 0.0;
+      if (done[d] != 0) continue;
+      for (int k = 0; k < m; ++k)
+        Hc(d, k, it) = cdouble(hh1[2 * (k * nd + d)] + hh2[2 * (k * nd + d)],
+                               hh1[2 * (k * nd + d) + 1] + hh2[2 * (k * nd + d) + 1]);
+      Hc(d, it, it) += zid;
+      const double wnrm = std::sqrt(std::max(hn[2 * d], 0.0));
+      cdouble* c = cs.data() + size_t(d) * M;
+      cdouble* s = sn.data() + size_t(d) * M;
+      cdouble* svd = sv.data() + size_t(d) * (M + 1);
+      for (int64_t k = 0; k < it; ++k) {
+        const cdouble t = c[k] * Hc(d, k, it) + std::conj(s[k]) * Hc(d, k + 1, it);
+        Hc(d, k + 1, it) = -s[k] * Hc(d, k, it) + c[k] * Hc(d, k + 1, it);
+        Hc(d, k, it) = t;
+      }
+      rotmat(Hc(d, it, it), cdouble(wnrm), c[it], s[it]);
+      Hc(d, it, it) = c[it] * Hc(d, it, it) + std::conj(s[it]) * wnrm;
+      svd[it + 1] = -s[it] * svd[it];
+      svd[it] = c[it] * svd[it];
+      const double err = std::abs(svd[it + 1]) / rb[d];
+      out.errs[size_t(d) * (M + 1) + it] = err;
+      if (!(err == err) || !(wnrm == wnrm)) {
+        out.status = kBreakdown;
+        done[d] = it + 1;
+        --nactive;
+        continue;
+      }
+      if (err <= eps_gmres || it == M - 1 || wnrm == 0.0) {
+        done[d] = it + 1;
+        --nactive;
+        continue;
+      }
+      hscale[2 * d] = 1.0 / wnrm;
+    }
+    BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nd * sizeof(double), cudaMemcpyHostToDevice, st));
+    BIE_CUDA(dev::launch_dscale(ws.w.p, vnext, ws.scale.p, n, nd, cplx, st));
+  }
+  // back-substitution per system: y = triu(H)\s, soln = V y (+ x0)
+  std::vector<double> hc(size_t(2) * (M + 1) * nd, 0.0);
+  for (int d = 0; d < nd; ++d) {
+    if (done[d] <= 0) continue;
+    const int64_t k = done[d];
+    std::vector<cdouble> y(k);
+    const cdouble* svd = sv.data() + size_t(d) * (M + 1);
+    for (int64_t j = k - 1; j >= 0; --j) {
+      cdouble acc = svd[j];
+      for (int64_t l = j + 1; l < k; ++l) acc -= Hc(d, j, l) * y[l];
+      y[j] = acc / Hc(d, j, j);
+    }
+    for (int64_t j = 0; j < k; ++j) {
+      hc[2 * (j * nd + d)] = y[j].real();
+      hc[2 * (j * nd + d) + 1] = y[j].imag();
+    }
+    out.niter[d] = k;
+    if (out.errs[size_t(d) * (M + 1) + k - 1] > eps_gmres && out.status == kOk) out.status = kNotConverged;
+  }
+  const int mused = int(std::max<int64_t>(it, 1));
+  BIE_CUDA(cudaMemcpyAsync(ws.coef.p, hc.data(), 2 * mused * nd * sizeof(double), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(dev::launch_combo(V, ldv, mused, ws.coef.p, d_soln, n, nd, cplx, st));
+  if (d_x0) BIE_CUDA(dev::launch_axpby(d_x0, d_soln, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+  // rres = || zid x + K x - rhs ||_w / ||rhs||_w   (one more matvec)
+  if (rres_precision >= 0) {
+    int ier = P.matvec(rres_precision, nd, d_soln, ws.w.p, st);
+    if (ier) return ier;
+    BIE_CUDA(dev::launch_axpby(d_soln, ws.w.p, zid.real(), zid.imag(), 1.0, 0.0, n, cplx, st));
+    BIE_CUDA(dev::launch_axpby(d_rhs, ws.w.p, -1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    BIE_CUDA(dev::launch_mdot(ws.w.p, ldv, 1, ws.w.p, wts, npts, nd, cplx, ws.partial.p, nblk, d_nrm, st));
+    BIE_CUDA(cudaMemcpyAsync(hn.data(), d_nrm, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+    // ||rhs|| (the initial residual norm is ||rhs - A x0||, not ||rhs||)
+    BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, npts, nd, cplx, ws.partial.p, nblk, d_h1, st));
+    std::vector<double> hr(2 * nd);
+    BIE_CUDA(cudaMemcpyAsync(hr.data(), d_h1, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    for (int d = 0; d < nd; ++d) {
+      const double rn = std::sqrt(std::max(hr[2 * d], 0.0));
+      out.rres[d] = rn > 0 ? std::sqrt(std::max(hn[2 * d], 0.0)) / rn : 0.0;
+    }
+  }
+  return out.status;
+}
+
+int solve_mixed(Plan& P, int nd, cdouble zid, const double* d_rhs, const double* d_x0,
+                int64_t numit, double eps_target, double inner_floor, int max_outer,
+                double* d_soln, MixedOut& out, cudaStream_t st) {
+  const int cplx = P.cplx ? 1 : 0;
+  const int64_t npts = P.npts, n = npts * nd;
+  const int64_t ldv = n * (cplx ? 2 : 1);
+  const int nblk = std::min<int>(2 * P.num_sms, int((npts + 63) / 64) + 1);
+  DBuf<double> r, d, tmp, partial, nrm;
+  BIE_CUDA(r.alloc(ldv));
+  BIE_CUDA(d.alloc(ldv));
+  BIE_CUDA(partial.alloc(size_t(2) * nd * nblk));
+  BIE_CUDA(nrm.alloc(size_t(4) * nd));
+  out.inner_iters.assign(nd, 0);
+  out.outer.assign(nd, 0);
+  out.rres.assign(nd, 1.0);
+  out.fp64_matvecs = out.fp32_matvecs = 0;
+  out.status = kOk;
+  const double* wts = P.d_wts();
+  // ||rhs||_w per system
+  std::vector<double> hb(2 * nd), hr(2 * nd);
+  BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, npts, nd, cplx, partial.p, nblk, nrm.p, st));
+  BIE_CUDA(cudaMemcpyAsync(hb.data(), nrm.p, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+  // x = x0 or 0; r = rhs - (zid x + K x)
+  if (d_x0) {
+    BIE_CUDA(cudaMemcpyAsync(d_soln, d_x0, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    int ier = P.matvec(0, nd, d_soln, r.p, st);
+    if (ier) return ier;
+    ++out.fp64_matvecs;
+    BIE_CUDA(dev::launch_axpby(d_soln, r.p, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
+    BIE_CUDA(dev::launch_axpby(d_rhs, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+  } else {
+    BIE_CUDA(cudaMemsetAsync(d_soln, 0, ldv * sizeof(double), st));
+    BIE_CUDA(cudaMemcpyAsync(r.p, d_rhs, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  BIE_CUDA(cudaStreamSynchronize(st));
+  std::vector<double> bn(nd);
+  for (int q = 0; q < nd; ++q) bn[q] = std::sqrt(std::max(hb[2 * q], 0.0));
+  for (int outer = 0; outer <= max_outer; ++outer) {
+    BIE_CUDA(dev::launch_mdot(r.p, ldv, 1, r.p, wts, npts, nd, cplx, partial.p, nblk, nrm.p, st));
+    BIE_CUDA(cudaMemcpyAsync(hr.data(), nrm.p, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    double worst_ratio = 0.0;
+    bool all_done = true;
+    for (int q = 0; q < nd; ++q) {
+      const double rel = bn[q] > 0 ? std::sqrt(std::max(hr[2 * q], 0.0)) / bn[q] : 0.0;
+      out.rres[q] = rel;
+      if (rel > eps_target) {
+        all_done = false;
+        worst_ratio = std::max(worst_ratio, eps_target / rel);
+      }
+    }
+    if (all_done || outer == max_outer) {
+      if (!all_done) out.status = kNotConverged;
+      break;
+    }
+    // inner relative tolerance: what this step must gain, not below the
+    // accuracy the f32 operator can deliver
+    const double tol = std::max(inner_floor, 0.5 * worst_ratio);
+    GmresOut go;
+    int ier = gmres(P, 1, -1, nd, zid, r.p, nullptr, numit, tol, d.p, go, st);
+    if (ier && ier != kNotConverged) return ier;
+    int64_t maxit = 0;
+    for (int q = 0; q < nd; ++q) {
+      out.inner_iters[q] += go.niter[q];
+      out.outer[q] += 1;
+      maxit = std::max(maxit, go.niter[q]);
+    }
+    out.fp32_matvecs += int(maxit);
+    // x += d ; r = rhs - (zid x + K x) in f64
+    BIE_CUDA(dev::launch_axpby(d.p, d_soln, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    ier = P.matvec(0, nd, d_soln, r.p, st);
+    if (ier) return ier;
+    ++out.fp64_matvecs;
+    BIE_CUDA(dev::launch_axpby(d_soln, r.p, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
+    BIE_CUDA(dev::launch_axpby(d_rhs, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+  }
+  return out.status;
+}
+
+}  // namespace bie

@@ -1,0 +1,162 @@
+// Device-resident operator plan for lpcomp_{lap,helm}_comb_dir_addsub and the
+// GMRES solvers built on it.
+#pragma once
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace bie {
+
+using cdouble = std::complex<double>;
+
+// Status codes shared with the C-ABI (include/fmm3dbie_b200.h).
+enum Status {
+  kOk = 0,
+  kErrArg = 1,
+  kErrCuda = 2,
+  kNotConverged = 3,
+  kBreakdown = 4,
+  kErrNoMem = 5,
+  kErrTables = 6,
+  kErrSingular = 7,
+  kErrTimeout = 8,
+};
+
+void set_last_error(const std::string& msg);
+const char* last_error();
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  cudaError_t alloc(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    n = count;
+    return cudaSuccess;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// Host description of one operator (reference calling sequence, 1-based
+// index arrays, complex values interleaved).
+struct PlanSpec {
+  int kind = 0;  // 0 Laplace, 1 Helmholtz
+  cdouble zk = 0, alpha = 1, beta = 1;
+  int64_t npatches = 0, npts = 0;
+  const int64_t* norders = nullptr;
+  const int64_t* ixyzs = nullptr;
+  const int64_t* iptype = nullptr;
+  const double* srccoefs = nullptr;
+  const double* srcvals = nullptr;
+  int ndtarg = 12;
+  int64_t ntarg = 0;
+  const double* targs = nullptr;  // ndtarg x ntarg
+  int64_t nnz = 0, nquad = 0;
+  const int64_t* row_ptr = nullptr;
+  const int64_t* col_ind = nullptr;
+  const int64_t* iquad = nullptr;
+  const double* wnear = nullptr;  // nquad reals (Laplace) or 2*nquad (Helmholtz)
+  const int64_t* novers = nullptr;
+  int64_t nptso = 0;
+  const int64_t* ixyzso = nullptr;
+  const double* srcover = nullptr;  // 12 x nptso
+  const double* whtsover = nullptr;
+  bool keep_f32 = true;  // also keep an f32 copy of W_eff
+};
+
+struct GmresWorkspace {
+  DBuf<double> V, w, partial, dots, coef, scale;
+};
+
+struct StageTimes {
+  double strengths_ms = 0, far_ms = 0, combine_ms = 0;
+  int64_t calls = 0;
+};
+
+class Plan {
+ public:
+  int kind = 0;
+  bool cplx = false;
+  int device = 0, num_sms = 148;
+  dev::KParams kp;
+  dev::Geometry g;
+  dev::Near nr;
+  int64_t npts = 0, ntarg = 0, nptso = 0, npatches = 0, nnz = 0, nquad = 0;
+  bool targets_on_surface = false;
+
+  int build(const PlanSpec& spec, cudaStream_t st);
+  // pot = K sigma (principal value, no identity term), nd densities,
+  // precision 0 = f64, 1 = f32 far field + f32 W_eff.
+  int matvec(int precision, int nd, const double* d_sigma, double* d_pot, cudaStream_t st);
+  int nchunks_for(int precision, int nd) const;
+  const double* d_wts() const { return wts_.p; }
+
+  GmresWorkspace gws;  // reused across solves on this plan
+
+  // per-stage timing with CUDA events on the launch stream (off by default)
+  bool timing = false;
+  StageTimes times;
+
+ private:
+  int ensure_workspace(int precision, int nd);
+  DBuf<double> tx_, ty_, tz_, sx_, sy_, sz_, snx_, sny_, snz_, sw_, imat_, wts_;
+  DBuf<int32_t> pstart_, ostart_, pclass_, col_;
+  DBuf<int64_t> cmoff_, row_ptr_, wofs_;
+  DBuf<double> weff64_;
+  DBuf<float> weff32_;
+  DBuf<char> str_;
+  DBuf<double> partial_;
+  cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+struct GmresOut {
+  std::vector<int64_t> niter;   // per system
+  std::vector<double> errs;     // (numit+1) per system, system-major
+  std::vector<double> rres;     // per system
+  int status = kOk;
+};
+
+// Unrestarted GMRES on (zid I + K) x = rhs for nd independent systems
+// (zgmres_guru / dgmres_guru semantics, gmres_routs.f90:13-375, with
+// classical Gram-Schmidt applied twice in place of modified Gram-Schmidt).
+// The inner matvec uses `precision`; the final relative residual rres uses
+// `rres_precision` (-1 skips it).  d_x0 (optional) is an initial guess.
+int gmres(Plan& P, int precision, int rres_precision, int nd, cdouble zid, const double* d_rhs,
+          const double* d_x0, int64_t numit, double eps_gmres, double* d_soln, GmresOut& out,
+          cudaStream_t st);
+
+// Mixed-precision solve: FP64 residuals and iterative refinement around
+// FP32-matvec GMRES inner solves.  Stops when the FP64 relative residual
+// is <= eps_target (per system) or max_outer refinements were done.
+struct MixedOut {
+  std::vector<int64_t> inner_iters;  // total inner GMRES iterations per system
+  std::vector<double> rres;          // final FP64 relative residual per system
+  std::vector<int64_t> outer;        // refinement steps per system
+  int fp64_matvecs = 0, fp32_matvecs = 0;
+  int status = kOk;
+};
+int solve_mixed(Plan& P, int nd, cdouble zid, const double* d_rhs, const double* d_x0,
+                int64_t numit, double eps_target, double inner_floor, int max_outer,
+                double* d_soln, MixedOut& out, cudaStream_t st);
+
+}  // namespace bie

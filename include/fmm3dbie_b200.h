@@ -1,0 +1,295 @@
+/*
+ * fmm3dbie_b200.h -- C-ABI of libfmm3dbie_b200.so, a B200 (sm_100a)
+ * implementation of fmm3dbie's locally corrected combined-field layer
+ * potentials and the GMRES solvers built on them.
+ *
+ * Conventions (identical to the Fortran calling sequences they replace):
+ *  - integers are int64_t; index arrays (ixyzs, row_ptr, col_ind, iquad,
+ *    ixyzso) are 1-based, exactly as getnearquad_* / findnear produce them;
+ *  - arrays are column-major Fortran layouts: srccoefs(9,npts),
+ *    srcvals(12,npts), targs(ndtarg,ntarg), srcover(12,nptso);
+ *  - complex values are interleaved (re, im) doubles, layout-compatible with
+ *    complex*16 and C99 double _Complex;
+ *  - every function returns an int status (BIE_OK = 0) and never aborts;
+ *    bie_last_error() gives a message for the calling thread.
+ *  - all pointers are HOST pointers unless the name says "_dev"; the
+ *    bie_plan_* family works on device buffers and a caller-supplied CUDA
+ *    stream (NULL = legacy default stream).
+ */
+#ifndef FMM3DBIE_B200_H
+#define FMM3DBIE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BIE_OK 0
+#define BIE_ERR_ARG 1
+#define BIE_ERR_CUDA 2
+#define BIE_NOT_CONVERGED 3
+#define BIE_BREAKDOWN 4
+#define BIE_ERR_NOMEM 5
+#define BIE_ERR_TABLES 6
+#define BIE_ERR_SINGULAR 7
+#define BIE_ERR_TIMEOUT 8
+
+/* ---- library ------------------------------------------------------------ */
+const char* bie_version(void);
+const char* bie_last_error(void);
+/* Load the Vioreanu-Rokhlin node tables (NULL: the file next to the
+ * library).  Called implicitly by every entry point that needs them. */
+int bie_init(const char* table_path);
+
+/* ---- discretisation (src/surface_routs/patch_basis_routs.f90) ------------ */
+/* get_npols (patch_basis_routs.f90:6) */
+int bie_get_npols(int64_t iptype, int64_t norder, int64_t* npols);
+/* get_disc_exps (patch_basis_routs.f90:234): uvs(2,npols), umat/vmat
+ * (npols,npols) column-major as in the reference, wts(npols) */
+int bie_get_disc_exps(int64_t norder, int64_t npols, int64_t iptype, double* uvs, double* umatr,
+                      double* vmatr, double* wts);
+/* get_basis_pols (patch_basis_routs.f90:298) / koorn_pols (koornexps.f90:206) */
+int bie_get_basis_pols(const double* uv, int64_t norder, int64_t npols, int64_t iptype,
+                       double* pols);
+
+/* ---- surfaces (src/surface_routs/xtri_parameterizations.f90) -------------- */
+/* Icosahedron refined nref times, radially projected onto the ellipsoid
+ * center + axes .* x/|x| (xtri_platonic + xtri_refine4_flat +
+ * xtri_ellipsoid_eval, :1335,:1864,:247), order norder RV nodes; arrays are
+ * sized for npatches = 20*4^nref. */
+int64_t bie_icosa_npatches(int64_t nref);
+int bie_surf_icosa_ellipsoid(int64_t nref, int64_t norder, const double* axes,
+                             const double* center, int64_t* norders, int64_t* ixyzs,
+                             int64_t* iptype, double* srcvals, double* srccoefs);
+/* Torus (R + r(p) cos t) (cos p, sin p) + r(p) sin t e_z, r(p) = r0 + r1
+ * cos(m p), nu x nv quad patches with (norder+1)^2 Gauss-Legendre nodes
+ * (iptype 11; chart in the style of xquad_wtorus_eval,
+ * xquad_parametrizations.f90:6). */
+int bie_surf_torus_quad(int64_t nu, int64_t nv, int64_t norder, double R, double r0, double r1,
+                        int64_t m, int64_t* norders, int64_t* ixyzs, int64_t* iptype,
+                        double* srcvals, double* srccoefs);
+
+/* ---- setup (src/surface_routs/surf_routs.f90, src/quadratures/*) --------- */
+/* get_centroid_rads (surf_routs.f90:195) */
+int bie_get_centroid_rads(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                          const int64_t* iptype, int64_t npts, const double* srccoefs,
+                          double* cms, double* rads);
+/* get_rfacs (near_field_routs.f:826) */
+int bie_get_rfacs(int64_t norder, int64_t iptype, double* rfac, double* rfac0);
+/* get_qwts (surf_routs.f90:1598) */
+int bie_get_qwts(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                 const int64_t* iptype, int64_t npts, const double* srcvals, double* qwts);
+/* findnearmem / findnear (near_field_routs.f:193,424): row-sparse list of
+ * patches j with |t_i - cms_j| <= rad_near_j; rows sorted by patch. */
+int bie_findnearmem(const double* cms, int64_t npatches, const double* rad_near, int64_t ndtarg,
+                    const double* targs, int64_t ntarg, int64_t* nnz);
+int bie_findnear(const double* cms, int64_t npatches, const double* rad_near, int64_t ndtarg,
+                 const double* targs, int64_t ntarg, int64_t* row_ptr, int64_t* col_ind);
+/* get_iquad_rsc (near_field_routs.f:765) */
+int bie_get_iquad_rsc(int64_t npatches, const int64_t* ixyzs, int64_t npts, int64_t nnz,
+                      const int64_t* row_ptr, const int64_t* col_ind, int64_t* iquad);
+/* get_far_order (far_field_routs.f90:10); zk complex (2 doubles) */
+int bie_get_far_order(double eps, int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                      const int64_t* iptype, const double* cms, const double* rads, int64_t npts,
+                      const double* srccoefs, int64_t ndtarg, int64_t ntarg,
+                      const double* targvals, int64_t ikerorder, const double* zk, int64_t nnz,
+                      const int64_t* row_ptr, const int64_t* col_ind, double rfac,
+                      int64_t* nfars, int64_t* ixyzso);
+/* oversample_geom (surf_routs.f90:304) */
+int bie_oversample_geom(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                        const int64_t* iptype, int64_t npts, const double* srccoefs,
+                        const double* srcvals, const int64_t* nfars, const int64_t* ixyzso,
+                        int64_t nptso, double* srcover);
+/* oversample_fun_surf (surf_routs.f90:451), nd interleaved real functions */
+int bie_oversample_fun_surf(int64_t nd, int64_t npatches, const int64_t* norders,
+                            const int64_t* ixyzs, const int64_t* iptype, int64_t npts,
+                            const double* u, const int64_t* nfars, const int64_t* ixyzso,
+                            int64_t nptso, double* uover);
+/* get_fmm_thresh (get_fmm_thresh.f:1) */
+int bie_get_fmm_thresh(int64_t nds, int64_t ns, const double* src, int64_t ndt, int64_t nt,
+                       const double* trg, double* thresh);
+/* get_patch_id_uvs (surf_routs.f90:1736) */
+int bie_get_patch_id_uvs(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                         const int64_t* iptype, int64_t npts, int64_t* ipatch_id,
+                         double* uvs_pts);
+/* hkrand (src/common/hkrand.f:3) */
+double bie_hkrand(int64_t iseed);
+
+/* ---- near quadrature ------------------------------------------------------ */
+/* getnearquad_lap_comb_dir_eval (lap_comb_dir.f90:228): dpars = (alpha, beta),
+ * wnear(nquad) real.  getnearquad_lap_comb_dir (:86) is the on-surface case
+ * ntarg = npts, targs = srcvals, ipatch_id/uvs_targ from get_patch_id_uvs. */
+int bie_getnearquad_lap_comb_dir_eval(int64_t npatches, const int64_t* norders,
+                                      const int64_t* ixyzs, const int64_t* iptype, int64_t npts,
+                                      const double* srccoefs, const double* srcvals,
+                                      int64_t ndtarg, int64_t ntarg, const double* targs,
+                                      const int64_t* ipatch_id, const double* uvs_targ,
+                                      double eps, const double* dpars, int64_t iquadtype,
+                                      int64_t nnz, const int64_t* row_ptr,
+                                      const int64_t* col_ind, const int64_t* iquad, double rfac0,
+                                      int64_t nquad, double* wnear);
+/* getnearquad_helm_comb_dir_eval (helm_comb_dir.f:250): zpars = (k, alpha,
+ * beta) complex, wnear(nquad) complex. */
+int bie_getnearquad_helm_comb_dir_eval(int64_t npatches, const int64_t* norders,
+                                       const int64_t* ixyzs, const int64_t* iptype, int64_t npts,
+                                       const double* srccoefs, const double* srcvals,
+                                       int64_t ndtarg, int64_t ntarg, const double* targs,
+                                       const int64_t* ipatch_id, const double* uvs_targ,
+                                       double eps, const double* zpars, int64_t iquadtype,
+                                       int64_t nnz, const int64_t* row_ptr,
+                                       const int64_t* col_ind, const int64_t* iquad,
+                                       double rfac0, int64_t nquad, double* wnear);
+
+/* ---- layer potentials on the GPU (host buffers) --------------------------- */
+/* lpcomp_lap_comb_dir_addsub (lap_comb_dir.f90:633): principal value of
+ * (alpha S_0 + beta D_0) sigma at the surface nodes. ndd=2, dpars=(alpha,beta),
+ * nker=1, ndim=1; work/lwork/zpars/ipars unused as in the reference. */
+int bie_lpcomp_lap_comb_dir_addsub(int64_t npatches, const int64_t* norders,
+                                   const int64_t* ixyzs, const int64_t* iptype, int64_t npts,
+                                   const double* srccoefs, const double* srcvals, double eps,
+                                   int64_t ndd, const double* dpars, int64_t ndz,
+                                   const double* zpars, int64_t ndi, const int64_t* ipars,
+                                   int64_t nnz, const int64_t* row_ptr, const int64_t* col_ind,
+                                   const int64_t* iquad, int64_t nquad, int64_t nker,
+                                   const double* wnear, const int64_t* novers, int64_t nptso,
+                                   const int64_t* ixyzso, const double* srcover,
+                                   const double* whtsover, int64_t lwork, const double* work,
+                                   int64_t ndim, const double* sigma, double* pot);
+/* lpcomp_helm_comb_dir_addsub (helm_comb_dir.f:658): complex wnear, sigma,
+ * pot; zpars = (k, alpha, beta). */
+int bie_lpcomp_helm_comb_dir_addsub(int64_t npatches, const int64_t* norders,
+                                    const int64_t* ixyzs, const int64_t* iptype, int64_t npts,
+                                    const double* srccoefs, const double* srcvals, double eps,
+                                    int64_t ndd, const double* dpars, int64_t ndz,
+                                    const double* zpars, int64_t ndi, const int64_t* ipars,
+                                    int64_t nnz, const int64_t* row_ptr, const int64_t* col_ind,
+                                    const int64_t* iquad, int64_t nquad, int64_t nker,
+                                    const double* wnear, const int64_t* novers, int64_t nptso,
+                                    const int64_t* ixyzso, const double* srcover,
+                                    const double* whtsover, int64_t lwork, const double* work,
+                                    int64_t ndim, const double* sigma, double* pot);
+/* lap_comb_dir_eval_addsub / helm_comb_dir_eval_addsub (lap_comb_dir.f90:806,
+ * helm_comb_dir.f:856): the same at ntarg arbitrary targets targs(ndtarg,
+ * ntarg) with a near list row_ptr(ntarg+1). */
+int bie_lap_comb_dir_eval_addsub(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                                 const int64_t* iptype, int64_t npts, const double* srccoefs,
+                                 const double* srcvals, int64_t ndtarg, int64_t ntarg,
+                                 const double* targs, double eps, const double* dpars,
+                                 int64_t nnz, const int64_t* row_ptr, const int64_t* col_ind,
+                                 const int64_t* iquad, int64_t nquad, const double* wnear,
+                                 const int64_t* novers, int64_t nptso, const int64_t* ixyzso,
+                                 const double* srcover, const double* whtsover,
+                                 const double* sigma, double* pot);
+int bie_helm_comb_dir_eval_addsub(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                                  const int64_t* iptype, int64_t npts, const double* srccoefs,
+                                  const double* srcvals, int64_t ndtarg, int64_t ntarg,
+                                  const double* targs, double eps, const double* zpars,
+                                  int64_t nnz, const int64_t* row_ptr, const int64_t* col_ind,
+                                  const int64_t* iquad, int64_t nquad, const double* wnear,
+                                  const int64_t* novers, int64_t nptso, const int64_t* ixyzso,
+                                  const double* srcover, const double* whtsover,
+                                  const double* sigma, double* pot);
+/* lap_comb_dir_eval (lap_comb_dir.f90:408) / helm_comb_dir_eval
+ * (helm_comb_dir.f:440; exposed by the Python bindings as lpcomp_helm_comb_dir,
+ * python/setup.py:39): setup (near list, far order, oversampling, near
+ * quadrature) on the host, evaluation on the GPU. */
+int bie_lap_comb_dir_eval(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                          const int64_t* iptype, int64_t npts, const double* srccoefs,
+                          const double* srcvals, int64_t ndtarg, int64_t ntarg,
+                          const double* targs, const int64_t* ipatch_id, const double* uvs_targ,
+                          double eps, const double* dpars, const double* sigma, double* pot);
+int bie_helm_comb_dir_eval(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                           const int64_t* iptype, int64_t npts, const double* srccoefs,
+                           const double* srcvals, int64_t ndtarg, int64_t ntarg,
+                           const double* targs, const int64_t* ipatch_id, const double* uvs_targ,
+                           double eps, const double* zpars, const double* sigma, double* pot);
+
+/* ---- solvers (host buffers) ----------------------------------------------- */
+/* lap_comb_dir_solver_guru (lap_comb_dir.f90:1459): dgmres on
+ * (did I + K) x = rhs, did = -(-1)^ifinout beta/2; errs(numit+1). */
+int bie_lap_comb_dir_solver_guru(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                                 const int64_t* iptype, int64_t npts, const double* srccoefs,
+                                 const double* srcvals, double eps, const double* dpars,
+                                 int64_t numit, int64_t ifinout, const double* rhs, int64_t nnz,
+                                 const int64_t* row_ptr, const int64_t* col_ind,
+                                 const int64_t* iquad, int64_t nquad, int64_t nker,
+                                 const double* wnear, const int64_t* novers, int64_t nptso,
+                                 const int64_t* ixyzso, const double* srcover,
+                                 const double* whtsover, double eps_gmres, int64_t* niter,
+                                 double* errs, double* rres, double* soln);
+/* helm_comb_dir_solver_guru (helm_comb_dir.f:2071): zgmres, zid =
+ * -(-1)^ifinout zpars(3)/2. */
+int bie_helm_comb_dir_solver_guru(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                                  const int64_t* iptype, int64_t npts, const double* srccoefs,
+                                  const double* srcvals, double eps, const double* zpars,
+                                  int64_t numit, int64_t ifinout, const double* rhs, int64_t nnz,
+                                  const int64_t* row_ptr, const int64_t* col_ind,
+                                  const int64_t* iquad, int64_t nquad, int64_t nker,
+                                  const double* wnear, const int64_t* novers, int64_t nptso,
+                                  const int64_t* ixyzso, const double* srcover,
+                                  const double* whtsover, double eps_gmres, int64_t* niter,
+                                  double* errs, double* rres, double* soln);
+/* lap_comb_dir_solver (lap_comb_dir.f90:1189) / helm_comb_dir_solver
+ * (helm_comb_dir.f:1808): setup on the host + GMRES on the GPU. */
+int bie_lap_comb_dir_solver(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                            const int64_t* iptype, int64_t npts, const double* srccoefs,
+                            const double* srcvals, double eps, const double* dpars, int64_t numit,
+                            int64_t ifinout, const double* rhs, double eps_gmres, int64_t* niter,
+                            double* errs, double* rres, double* soln);
+int bie_helm_comb_dir_solver(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                             const int64_t* iptype, int64_t npts, const double* srccoefs,
+                             const double* srcvals, double eps, const double* zpars,
+                             int64_t numit, int64_t ifinout, const double* rhs, double eps_gmres,
+                             int64_t* niter, double* errs, double* rres, double* soln);
+/* Extension of helm_comb_dir_solver_guru (no reference counterpart for the
+ * precision/batch arguments): nrhs independent right-hand sides rhs(nrhs,
+ * npts) point-major; iprec 0 = FP64 GMRES (the reference method), 1 = FP32
+ * matvec GMRES inside FP64 iterative refinement to relative residual
+ * eps_gmres.  niter(nrhs), rres(nrhs). */
+int bie_helm_comb_dir_solver_guru_ext(int64_t npatches, const int64_t* norders,
+                                      const int64_t* ixyzs, const int64_t* iptype, int64_t npts,
+                                      const double* srccoefs, const double* srcvals, double eps,
+                                      const double* zpars, int64_t numit, int64_t ifinout,
+                                      int64_t nrhs, const double* rhs, int64_t nnz,
+                                      const int64_t* row_ptr, const int64_t* col_ind,
+                                      const int64_t* iquad, int64_t nquad, const double* wnear,
+                                      const int64_t* novers, int64_t nptso, const int64_t* ixyzso,
+                                      const double* srcover, const double* whtsover,
+                                      double eps_gmres, int64_t iprec, int64_t* niter,
+                                      double* rres, double* soln);
+
+/* ---- device-resident plans (device buffers, caller stream) ---------------- */
+/* kind 0 Laplace (params = alpha, beta), 1 Helmholtz (params = k, alpha, beta
+ * complex). Targets: ntarg = 0 means the surface nodes (lpcomp/solver case),
+ * otherwise targs(ndtarg, ntarg) on the host. Host arrays are copied. */
+int bie_plan_create(int64_t kind, const double* params, int64_t npatches,
+                    const int64_t* norders, const int64_t* ixyzs, const int64_t* iptype,
+                    int64_t npts, const double* srccoefs, const double* srcvals, int64_t ndtarg,
+                    int64_t ntarg, const double* targs, int64_t nnz, const int64_t* row_ptr,
+                    const int64_t* col_ind, const int64_t* iquad, int64_t nquad,
+                    const double* wnear, const int64_t* novers, int64_t nptso,
+                    const int64_t* ixyzso, const double* srcover, const double* whtsover,
+                    void** plan);
+int bie_plan_destroy(void* plan);
+/* info[0..7] = npts, ntarg, nptso, nnz, nquad, nchunks(f64), nchunks(f32),
+ * kind */
+int bie_plan_info(void* plan, int64_t* info);
+/* pot_dev = K sigma_dev for nd densities per point; iprec 0 f64, 1 f32 */
+int bie_plan_matvec(void* plan, int64_t iprec, int64_t nd, const double* sigma_dev,
+                    double* pot_dev, void* stream);
+/* GMRES on (zid I + K) x = rhs, nd independent systems (point-major).
+ * mode 0: FP64 GMRES (reference method); 1: mixed precision refinement.
+ * x0_dev may be NULL. niter(nd), rres(nd), errs((numit+1)*nd) or NULL. */
+int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
+                   const double* rhs_dev, const double* x0_dev, int64_t numit, double eps_gmres,
+                   double* soln_dev, int64_t* niter, double* errs, double* rres, void* stream);
+/* Stage timing with CUDA events on the call's stream: enable != 0 turns it
+ * on and clears the totals; times[0..3] = strengths, far, combine (ms
+ * totals), calls. */
+int bie_plan_timing(void* plan, int64_t enable, double* times);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FMM3DBIE_B200_H */
