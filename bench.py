@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark: Helmholtz combined-field Dirichlet solves per second on one B200.
+
+Workload (the headline configuration): exterior Helmholtz CFIE Dirichlet
+problem on the ellipsoid with semi-axes (1,2,3), an icosahedron refined 3x
+(1280 flat triangles radially projected) discretised with order-6
+Vioreanu-Rokhlin nodes (npts = 35840), zk = 2, zpars = (zk, -i zk, 1),
+eps = 1e-7, right-hand side the field of a unit point source at
+(0.1,-0.2,0.3) inside the surface.  One step = one full solve.
+
+  ours (value)  : FP32/complex64 matvec GMRES inside FP64 iterative
+                  refinement to FP64 relative residual <= 1e-7, inputs resident
+                  on the device (plan built once);
+  fp64 path     : the reference method (FP64 GMRES, eps_gmres 1e-7) on the
+                  same plan, reported beside it;
+  e2e           : the same solve through the host-buffer C-ABI entry point
+                  bie_helm_comb_dir_solver_guru_ext (all operator data, rhs and
+                  solution copied between pinned host memory and the device
+                  inside the timed region);
+  --impl reference : the FP64 CPU restatement of the reference path (oracle/)
+                  timed on the host cores on a bounded sample.
+
+Timing: per-step CUDA events on the launch stream, an L2 flush (write of a
+256 MiB buffer) between timed steps, barrier + synchronize around the timed
+region, max over ranks.  N > 1 runs independent replicas (the path has no
+data exchange between solves): value = all ranks' solves / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/sec at 1e-6 rel err: mixed-prec+batched+warm-start vs plain FP64 GPU"
+WORKLOAD = ("Helmholtz CFIE Dirichlet GMRES solve, ellipsoid (1,2,3), 1280 order-6 RV patches, "
+            "npts 35840, zk=2, zpars=(2,-2i,1), eps=1e-7, interior point-source rhs")
+ZK = 2.0
+ZPARS = (ZK, -1j * ZK, 1.0)
+EPS = 1e-7
+X0 = np.array([0.1, -0.2, 0.3])
+TOL_RES = 1e-7      # FP64 relative residual target of both timed paths
+FLOPS_PER_PAIR = {"helm": 26 + 16, "lap": 15 + 4}   # 1 density
+
+
+def flops_per_pair(kind: str, nd: int = 1) -> int:
+    return (26 + 16 * nd) if kind == "helm" else (15 + 4 * nd)
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), \
+        int(os.environ.get("LOCAL_RANK", 0))
+
+
+def build_problem(nref=3, norder=6):
+    from fmm3dbie_b200 import surface as S
+    s = S.icosa_ellipsoid(nref, norder, (1.0, 2.0, 3.0))
+    t = time.time()
+    st = S.setup(s, 1, EPS, ZPARS)
+    r = np.linalg.norm(s.xyz - X0, axis=1)
+    rhs = np.exp(1j * ZK * r) / (4 * np.pi * r)
+    return s, st, rhs, time.time() - t
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [ln.strip().split(",") for ln in self.f.read().splitlines() if ln.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def cpu_baseline(s, st, niter, nsub_every=16):
+    """Oracle (FP64 C restatement, OpenMP) matvec on every nsub_every-th
+    target, extrapolated to one solve of niter+1 matvecs."""
+    import oracle
+    from fmm3dbie_b200.surface import NearField
+    rng = np.random.default_rng(0)
+    sigma = rng.normal(size=s.npts) + 1j * rng.normal(size=s.npts)
+    idx = np.arange(0, s.npts, nsub_every)
+    rp, ci, iq, w = st.near.row_ptr, st.near.col_ind, st.near.iquad, st.near.wnear
+    rows, cols, iqs, wn = [1], [], [1], []
+    for i in idx:
+        a, b = rp[i] - 1, rp[i + 1] - 1
+        cols.extend(ci[a:b])
+        for k in range(a, b):
+            n = iq[k + 1] - iq[k]
+            wn.append(w[iq[k] - 1: iq[k + 1] - 1])
+            iqs.append(iqs[-1] + n)
+        rows.append(rows[-1] + (b - a))
+    sub = NearField(np.array(rows, np.int64), np.array(cols, np.int64), np.array(iqs, np.int64),
+                    np.concatenate(wn))
+    targ = s.srcvals[idx]
+    oracle.eval_addsub(1, s, targ[:64], ZPARS, NearField(sub.row_ptr[:65], sub.col_ind[:sub.row_ptr[64] - 1],
+                       sub.iquad[:sub.row_ptr[64]], sub.wnear), st.over, sigma)  # warm-up
+    t = time.perf_counter()
+    oracle.eval_addsub(1, s, targ, ZPARS, sub, st.over, sigma)
+    dt = time.perf_counter() - t
+    t_matvec = dt * s.npts / len(idx)
+    solves_per_s = 1.0 / (t_matvec * (niter + 1))
+    cores = len(os.sched_getaffinity(0))
+    return {"value": solves_per_s, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": (f"oracle FP64 matvec on {len(idx)} of {s.npts} targets ({dt:.2f} s), "
+                       f"extrapolated to {niter}+1 full matvecs per FP64 GMRES solve "
+                       f"({t_matvec:.2f} s/matvec); far field is the exact O(N*Nover) direct sum")}
+
+
+def reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    s, st, rhs, _ = build_problem()
+    import oracle
+    from fmm3dbie_b200 import surface as S
+    # iteration count of the reference FP64 GMRES (mesh-independent for this
+    # second-kind equation), measured with the oracle on the same ellipsoid
+    # at one coarser refinement
+    sc = S.icosa_ellipsoid(2, 6, (1.0, 2.0, 3.0))
+    stc = S.setup(sc, 1, EPS, ZPARS)
+    rc = np.linalg.norm(sc.xyz - X0, axis=1)
+    _, niter, _, _, _ = oracle.gmres(1, sc, ZPARS, stc.near, stc.over, 0.5,
+                                     np.exp(1j * ZK * rc) / (4 * np.pi * rc), numit=200,
+                                     eps_gmres=TOL_RES)
+    vals = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(s, st, niter)
+        if i >= args.warmup:
+            vals.append(b["value"])
+            base = b
+    v = float(np.mean(vals))
+    base["value"] = v
+    base["sample"] += f"; niter={niter} from the oracle GMRES on the 320-patch ellipsoid"
+    line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "impl": "reference",
+            "data": "synthetic: seeded ellipsoid surface and point-source rhs",
+            "config": {"workload": WORKLOAD},
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from fmm3dbie_b200 import Plan, layer
+    from fmm3dbie_b200 import _lib as L
+    lib = L.lib()
+
+    s, st, rhs, t_setup = build_problem()
+    P = Plan(1, ZPARS, s, st.near, st.over)
+    stream = torch.cuda.current_stream(dev)
+    r_d = torch.tensor(rhs, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+
+    # accuracy judge: tight FP64 solution
+    x_ref, info_ref = P.solve(r_d, 0.5, mode=0, numit=300, eps_gmres=1e-12)
+    w = torch.tensor(s.qwts(), device=dev)
+
+    def relerr(x):
+        return float(torch.sqrt(torch.sum(w * (x - x_ref).abs() ** 2) /
+                                torch.sum(w * x_ref.abs() ** 2)))
+
+    def timed(fn, k, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ts = []
+        for _ in range(k):
+            flush.fill_(1.0)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out = fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        return ts, out
+
+    # ---- plain FP64 GPU path (the reference method) --------------------------
+    f64 = lambda: P.solve(r_d, 0.5, mode=0, numit=300, eps_gmres=TOL_RES)  # noqa: E731
+    ts64, (x64, info64) = timed(f64, max(1, args.steps // 2), 1)
+    t64 = float(np.mean(ts64))
+
+    # ---- ours: mixed precision, timed region with clocks + stage timing -------
+    mixed = lambda: P.solve(r_d, 0.5, mode=1, numit=300, eps_gmres=TOL_RES)  # noqa: E731
+    for _ in range(args.warmup):
+        mixed()
+    P.timing(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    n0 = lib.bie_launch_count()
+    tsm, (xm, infom) = timed(mixed, args.steps, 0)
+    launches = int(lib.bie_launch_count() - n0)
+    ck = clocks.stop()
+    stages = P.timing(False)
+    tm = float(np.mean(tsm))
+    tmax = float(np.sum(tsm))
+    if world > 1:
+        tt = torch.tensor([tmax], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tmax = float(tt.item())
+    value = world * args.steps / (tmax / 1000.0)
+
+    # roofline of the dominant kernel: the f32 far-field N-body
+    far32 = stages["f32"]
+    far_ms = far32["far_ms"] / max(far32["calls"], 1)
+    pairs = float(P.ntarg) * float(P.nptso)
+    achieved = pairs * flops_per_pair("helm") / (far_ms * 1e-3) / 1e12
+    peak_tf = ctypes_double_pair(lib)
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "far_kernel_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    far64 = stages["f64"]
+    far64_ms = far64["far_ms"] / max(far64["calls"], 1) if far64["calls"] else None
+
+    # ---- e2e through the host-buffer C-ABI (pinned host memory) ---------------
+    e2e = None
+    if args.e2e_steps > 0:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+        hs = {k: pin(getattr(s, k)) for k in ("norders", "ixyzs", "iptype", "srcvals", "srccoefs")}
+        from fmm3dbie_b200.surface import Surface, NearField, Oversampled
+        s_p = Surface(**hs)
+        n_p = NearField(pin(st.near.row_ptr), pin(st.near.col_ind), pin(st.near.iquad),
+                        pin(st.near.wnear))
+        o_p = Oversampled(pin(st.over.novers), pin(st.over.ixyzso), pin(st.over.srcover),
+                          pin(st.over.wover))
+        rhs_p = pin(rhs[:, None])
+        h2d = sum(a.nbytes for a in list(hs.values()) + [n_p.row_ptr, n_p.col_ind, n_p.iquad,
+                                                          n_p.wnear, o_p.novers, o_p.ixyzso,
+                                                          o_p.srcover, o_p.wover, rhs_p])
+        d2h = rhs_p.nbytes
+        run = lambda: layer.helm_comb_dir_solver_guru_ext(s_p, EPS, ZPARS, 300, 1, rhs_p, n_p, o_p,  # noqa: E731
+                                                          TOL_RES, iprec=1)
+        run()
+        torch.cuda.synchronize()
+        te = []
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            out = run()
+            te.append(time.perf_counter() - t0)
+        e2e = {"value": 1.0 / float(np.mean(te)), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "path": "bie_helm_comb_dir_solver_guru_ext (host buffers)",
+               "rres": float(out[1][0])}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(s, st, int(info64["niter"][0]))
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tmax / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 matvec + c128 refinement/Krylov",
+            "data": "synthetic: seeded ellipsoid surface and point-source rhs",
+            "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}",
+                       "l2": "L2 flushed (256 MiB write) between timed steps; W_eff f32 is "
+                             f"{st.near.nquad * 8 / 1e6:.0f} MB"},
+            "fp64_path": {"solves_per_s": 1000.0 / t64, "ms_per_solve": t64,
+                          "niter": int(info64["niter"][0]), "rel_err": relerr(x64)},
+            "speedup_vs_fp64": t64 / tm,
+            "mixed": {"inner_iters": int(infom["niter"][0]), "rres": float(infom["rres"][0]),
+                      "rel_err": relerr(xm), "fp64_matvecs": infom["fp64_matvecs"],
+                      "fp32_matvecs": infom["fp32_matvecs"]},
+            "problem": {"npts": P.npts, "nptso": P.nptso, "nnz": P.nnz, "nquad": P.nquad,
+                        "setup_s": round(t_setup, 2), "far_chunks": list(P.nchunks)},
+            "roofline": {"kernel": "far_kernel<helm,f32>", "bound": "fp32", "achieved": achieved,
+                         "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
+                         "traffic": traffic,
+                         "peak_source": "FP32 FFMA loop measured in this run "
+                                        "(MEASURED_PEAKS.json has no FP32 SIMT figure)",
+                         "flops_per_pair": flops_per_pair("helm"), "pairs_per_launch": pairs,
+                         "avg_launch_ms": far_ms},
+            "stage_ms_per_matvec": {
+                "f32": {k: far32[k] / max(far32["calls"], 1) for k in ("strengths_ms", "far_ms", "combine_ms")},
+                "f64": {k: far64[k] / max(far64["calls"], 1) for k in ("strengths_ms", "far_ms", "combine_ms")}},
+            "gpu_launches": launches,
+            "clocks": ck,
+            "e2e": e2e,
+            "cpu_baseline": base,
+        }
+        print(json.dumps(line), flush=True)
+    P.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_double_pair(lib):
+    import ctypes as C
+    tf, ms = C.c_double(), C.c_double()
+    lib.bie_measure_fp32_peak(C.byref(tf), C.byref(ms))
+    return tf.value
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -885,16 +885,48 @@ int bie_plan_timing(void* plan, int64_t enable, double* times) {
   if (!plan) return BIE_ERR_ARG;
   bie::Plan& P = *static_cast<bie::Plan*>(plan);
   if (times) {
-    times[0] = P.times.strengths_ms;
-    times[1] = P.times.far_ms;
-    times[2] = P.times.combine_ms;
-    times[3] = double(P.times.calls);
+    for (int p = 0; p < 2; ++p) {
+      times[4 * p + 0] = P.times.strengths_ms[p];
+      times[4 * p + 1] = P.times.far_ms[p];
+      times[4 * p + 2] = P.times.combine_ms[p];
+      times[4 * p + 3] = double(P.times.calls[p]);
+    }
   }
   if (enable >= 0) {
     P.timing = enable != 0;
     P.times = bie::StageTimes{};
   }
   return BIE_OK;
+}
+
+int64_t bie_launch_count(void) { return bie::dev::launch_count(); }
+
+int bie_measure_fp32_peak(double* tflops, double* ms) {
+  return guarded([&] {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int threads = 256, blocks = sms * 8, iters = 4096;
+    bie::DBuf<float> out;
+    if (out.alloc(size_t(blocks) * threads)) return BIE_ERR_NOMEM;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    bie::dev::launch_ffma_peak(out.p, blocks, threads, iters / 8, 0);  // warm-up
+    cudaEventRecord(a, 0);
+    bie::dev::launch_ffma_peak(out.p, blocks, threads, iters, 0);
+    cudaEventRecord(b, 0);
+    cudaEventSynchronize(b);
+    float t = 0;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    const double flops = double(blocks) * threads * iters * 16.0 * 8.0 * 2.0;
+    *ms = t;
+    *tflops = flops / (t * 1e-3) / 1e12;
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? BIE_OK : BIE_ERR_CUDA;
+  });
 }
 
 }  // extern "C"

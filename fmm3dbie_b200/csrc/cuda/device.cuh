@@ -110,5 +110,10 @@ cudaError_t launch_axpby(const double* x, double* y, double ar, double ai, doubl
 cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
                          int64_t n, int nd, int cplx, cudaStream_t st);
 
+// Number of kernels this library has launched in the process.
+int64_t launch_count();
+// FFMA throughput probe (flops = blocks*threads*iters*16*8*2).
+cudaError_t launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st);
+
 }  // namespace dev
 }  // namespace bie

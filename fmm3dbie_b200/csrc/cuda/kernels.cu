@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 
 #include "device.cuh"
@@ -22,6 +23,9 @@ namespace bie {
 namespace dev {
 
 namespace {
+
+std::atomic<int64_t> g_launches{0};
+inline void count(int64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 constexpr double kOver4Pi = 0.07957747154594767;
 
@@ -638,6 +642,7 @@ cudaError_t launch_strengths(const Geometry& g, const KParams& kp, const MatvecA
     else
       strengths_kernel<double, 0><<<grid, block, sh, st>>>(g, kp, a.sigma, (double*)a.strengths, a.nd);
   }
+  count();
   return cudaGetLastError();
 }
 
@@ -672,6 +677,7 @@ cudaError_t launch_far(const Geometry& g, const KParams& kp, const MatvecArgs& a
       far_kernel<0, double, kFarThreads, kTptF64, kFarTile, false><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
     }
   }
+  count();
   return cudaGetLastError();
 }
 
@@ -692,6 +698,7 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
     else
       combine_kernel<0, double><<<grid, block, 0, st>>>(g, nr, (const double*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
   }
+  count();
   return cudaGetLastError();
 }
 
@@ -709,12 +716,14 @@ cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp, co
     if (sh > 48 * 1024) cudaFuncSetAttribute(fold_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
     fold_kernel<0><<<grid, block, sh, st>>>(g, nr, kp, wnear, weff);
   }
+  count();
   return cudaGetLastError();
 }
 
 cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   to_f32_kernel<<<grid_for(n, 256), 256, 0, st>>>(in, out, n);
+  count();
   return cudaGetLastError();
 }
 
@@ -729,6 +738,7 @@ cudaError_t launch_mdot(const double* V, int64_t ldv, int m, const double* w, co
   else
     mdot_partial_kernel<0><<<nblk, threads, 0, st>>>(V, ldv, m, w, wts, npts, nd, partial);
   mdot_final_kernel<<<m * nd, 256, 0, st>>>(partial, nblk, out);
+  count(2);
   return cudaGetLastError();
 }
 
@@ -739,6 +749,7 @@ cudaError_t launch_maxpy(const double* V, int64_t ldv, int m, const double* h, d
     maxpy_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, h, w, n, nd);
   else
     maxpy_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, h, w, n, nd);
+  count();
   return cudaGetLastError();
 }
 
@@ -748,6 +759,7 @@ cudaError_t launch_dscale(const double* x, double* y, const double* s, int64_t n
     dscale_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(x, y, s, n, nd);
   else
     dscale_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(x, y, s, n, nd);
+  count();
   return cudaGetLastError();
 }
 
@@ -757,6 +769,7 @@ cudaError_t launch_axpby(const double* x, double* y, double ar, double ai, doubl
     axpby_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(x, y, ar, ai, br, bi, n);
   else
     axpby_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(x, y, ar, ai, br, bi, n);
+  count();
   return cudaGetLastError();
 }
 
@@ -766,8 +779,39 @@ cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, d
     combo_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, c, y, n, nd);
   else
     combo_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, c, y, n, nd);
+  count();
   return cudaGetLastError();
 }
+
+// FFMA throughput probe: every thread runs 8 independent FMA chains; the
+// result is stored so the work cannot be removed.  flops = 2 * 8 * iters
+// per thread.
+__global__ void ffma_peak_kernel(float* out, int iters, float a, float b) {
+  float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5,
+        x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x0 = fmaf(x0, a, b);
+      x1 = fmaf(x1, a, b);
+      x2 = fmaf(x2, a, b);
+      x3 = fmaf(x3, a, b);
+      x4 = fmaf(x4, a, b);
+      x5 = fmaf(x5, a, b);
+      x6 = fmaf(x6, a, b);
+      x7 = fmaf(x7, a, b);
+    }
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+
+cudaError_t launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st) {
+  ffma_peak_kernel<<<blocks, threads, 0, st>>>(out, iters, 0.9999999f, 1e-7f);
+  count();
+  return cudaGetLastError();
+}
+
+int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 }  // namespace dev
 }  // namespace bie

@@ -273,10 +273,10 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
     cudaEventElapsedTime(&t01, ev_[0], ev_[1]);
     cudaEventElapsedTime(&t12, ev_[1], ev_[2]);
     cudaEventElapsedTime(&t23, ev_[2], ev_[3]);
-    times.strengths_ms += t01;
-    times.far_ms += t12;
-    times.combine_ms += t23;
-    times.calls += 1;
+    times.strengths_ms[precision] += t01;
+    times.far_ms[precision] += t12;
+    times.combine_ms[precision] += t23;
+    times.calls[precision] += 1;
   }
   return kOk;
 }

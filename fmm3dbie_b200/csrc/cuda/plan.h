@@ -88,9 +88,10 @@ struct GmresWorkspace {
   DBuf<double> V, w, partial, dots, coef, scale;
 };
 
+// Per-precision stage totals (index 0 = f64 matvecs, 1 = f32 matvecs).
 struct StageTimes {
-  double strengths_ms = 0, far_ms = 0, combine_ms = 0;
-  int64_t calls = 0;
+  double strengths_ms[2] = {0, 0}, far_ms[2] = {0, 0}, combine_ms[2] = {0, 0};
+  int64_t calls[2] = {0, 0};
 };
 
 class Plan {

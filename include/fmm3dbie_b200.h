@@ -280,14 +280,24 @@ int bie_plan_matvec(void* plan, int64_t iprec, int64_t nd, const double* sigma_d
                     double* pot_dev, void* stream);
 /* GMRES on (zid I + K) x = rhs, nd independent systems (point-major).
  * mode 0: FP64 GMRES (reference method); 1: mixed precision refinement.
- * x0_dev may be NULL. niter(nd), rres(nd), errs((numit+1)*nd) or NULL. */
+ * x0_dev may be NULL. niter(nd), rres(nd), errs or NULL: mode 0 fills
+ * errs((numit+1)*nd) with the residual history, mode 1 fills errs[0] =
+ * number of FP64 matvecs, errs[1] = number of FP32 matvecs. */
 int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
                    const double* rhs_dev, const double* x0_dev, int64_t numit, double eps_gmres,
                    double* soln_dev, int64_t* niter, double* errs, double* rres, void* stream);
-/* Stage timing with CUDA events on the call's stream: enable != 0 turns it
- * on and clears the totals; times[0..3] = strengths, far, combine (ms
- * totals), calls. */
+/* Stage timing with CUDA events on the call's stream: enable = 1 turns it
+ * on, 0 off (both clear the totals), -1 only reads; times[0..7] =
+ * strengths, far, combine (ms totals), calls for the f64 matvecs, then the
+ * same four for the f32 matvecs. */
 int bie_plan_timing(void* plan, int64_t enable, double* times);
+
+/* ---- measurement helpers (no reference counterpart) ---------------------- */
+/* Number of kernels this library has launched in the process. */
+int64_t bie_launch_count(void);
+/* FP32 FFMA throughput of the current device (TFLOP/s) from a register-
+ * resident FMA loop kernel, timed with CUDA events on the default stream. */
+int bie_measure_fp32_peak(double* tflops, double* ms);
 
 #ifdef __cplusplus
 }
