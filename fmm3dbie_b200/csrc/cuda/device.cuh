@@ -79,9 +79,12 @@ cudaError_t launch_far(const Geometry& g, const KParams& kp, const MatvecArgs& a
                        cudaStream_t st);
 cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
                            const MatvecArgs& a, cudaStream_t st);
-// W_eff = wnear - [K(t_i, y_l) w_l]_l * imat  for every near pair, in f64.
+// W_eff = wnear - [K(t_i, y_l) w_l]_l * imat  for every near pair.
+// match32 = 0: exact FP64 kernel, weff is double* (may alias wnear);
+// match32 = 1: kernel values as the FP32 far kernel computes them
+// (same centring and pair functions), weff is float*.
 cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp,
-                        const double* wnear, double* weff, cudaStream_t st);
+                        const double* wnear, void* weff, int match32, cudaStream_t st);
 cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t st);
 
 // Number of source chunks the far kernel splits the sources into (the

@@ -147,15 +147,15 @@ __device__ __forceinline__ void pair_lap(R tx, R ty, R tz, const typename Vec<R>
                                          const typename Vec<R>::T2 g1,
                                          const typename Vec<R>::T2 s, R thr2, R& p) {
   const R dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
-  const R r2 = dx * dx + dy * dy + dz * dz;
+  const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
   R rinv;
   if constexpr (sizeof(R) == 4)
     rinv = (r2 >= thr2) ? rsqrtf(r2) : R(0);
   else
     rinv = (r2 >= thr2) ? rsqrt(r2) : R(0);
-  const R dn = dx * g0.w + dy * g1.x + dz * g1.y;
-  const R e = s.x + s.y * dn * (rinv * rinv);
-  p += e * rinv;
+  const R dn = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y));
+  const R e = fma(s.y * dn, rinv * rinv, s.x);
+  p = fma(e, rinv, p);
 }
 
 template <int KIND, typename R, int NT, int TPT, int TILE, bool CK>
@@ -348,10 +348,19 @@ __global__ void combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
 
 // ---------------------------------------------------------------------------
 // fold: W_eff = wnear - (smooth oversampled contribution) for each near pair
+//
+// MATCH32 = 0: the smooth part is the exact FP64 kernel (FP64 matvec path).
+// MATCH32 = 1: the smooth part is evaluated with the FP32 far kernel's own
+// arithmetic (same block-centred coordinates, same pair functions), so that
+// the FP32 far field's error on near pairs -- where n.(t-s) = O(r^2) cancels
+// in single precision -- is removed exactly by the subtraction; only the
+// well-separated pairs are then left to the FP32 far sum.
 // ---------------------------------------------------------------------------
-template <int CPLX>
+constexpr int kFarBlockTargetsF32 = 512;  // kFarThreads * kTptF32 (checked below)
+
+template <int CPLX, int MATCH32, typename OUT>
 __global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __restrict__ wnear,
-                            double* __restrict__ weff) {
+                            OUT* __restrict__ weff) {
   extern __shared__ double sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double* a = sh + size_t(warp) * g.max_nf * 2;
@@ -373,11 +382,40 @@ __global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __res
   const int os = g.ostart[p], nf = g.ostart[p + 1] - os;
   const double* M = g.imat + g.cmoff[g.pclass[p]];
   const double thr2 = kp.thresh * kp.thresh;
+  // block centre of target i in the FP32 far kernel
+  const int64_t tb = (i / kFarBlockTargetsF32) * kFarBlockTargetsF32;
+  const double cx = g.tx[tb], cy = g.ty[tb], cz = g.tz[tb];
+  const float tx32 = float(tx - cx), ty32 = float(ty - cy), tz32 = float(tz - cz);
   for (int l = lane; l < nf; l += 32) {
     const int s = os + l;
+    double vr = 0, vi = 0;
+    if (MATCH32) {
+      const float4 g0 = make_float4(float(g.sx[s] - cx), float(g.sy[s] - cy), float(g.sz[s] - cz),
+                                    float(g.snx[s]));
+      const float2 g1 = make_float2(float(g.sny[s]), float(g.snz[s]));
+      const float thr2f = float(thr2);
+      const double f = g.sw[s] * kOver4Pi;
+      if (CPLX) {
+        // unit charge and unit dipole responses of the FP32 pair function
+        float gr = 0, gi = 0, dr = 0, di = 0;
+        pair_helm(tx32, ty32, tz32, g0, g1, make_float4(1.f, 0.f, 0.f, 0.f), float(kp.kr),
+                  float(kp.ki), thr2f, kp.ki != 0.0, gr, gi);
+        pair_helm(tx32, ty32, tz32, g0, g1, make_float4(0.f, 0.f, 1.f, 0.f), float(kp.kr),
+                  float(kp.ki), thr2f, kp.ki != 0.0, dr, di);
+        vr = (kp.ar * gr - kp.ai * gi + kp.br * dr - kp.bi * di) * f;
+        vi = (kp.ar * gi + kp.ai * gr + kp.br * di + kp.bi * dr) * f;
+      } else {
+        float pc = 0, pd = 0;
+        pair_lap<float>(tx32, ty32, tz32, g0, g1, make_float2(1.f, 0.f), thr2f, pc);
+        pair_lap<float>(tx32, ty32, tz32, g0, g1, make_float2(0.f, 1.f), thr2f, pd);
+        vr = (kp.ar * pc + kp.br * pd) * f;
+      }
+      a[2 * l] = vr;
+      a[2 * l + 1] = vi;
+      continue;
+    }
     const double dx = tx - g.sx[s], dy = ty - g.sy[s], dz = tz - g.sz[s];
     const double r2 = dx * dx + dy * dy + dz * dz;
-    double vr = 0, vi = 0;
     if (r2 >= thr2) {
       const double r = sqrt(r2), rinv = 1.0 / r;
       const double dn = dx * g.snx[s] + dy * g.sny[s] + dz * g.snz[s];
@@ -411,10 +449,10 @@ __global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __res
       si = fma(a[2 * l + 1], mv, si);
     }
     if (CPLX) {
-      weff[2 * (wb + mm)] = wnear[2 * (wb + mm)] - sr;
-      weff[2 * (wb + mm) + 1] = wnear[2 * (wb + mm) + 1] - si;
+      weff[2 * (wb + mm)] = OUT(wnear[2 * (wb + mm)] - sr);
+      weff[2 * (wb + mm) + 1] = OUT(wnear[2 * (wb + mm) + 1] - si);
     } else {
-      weff[wb + mm] = wnear[wb + mm] - sr;
+      weff[wb + mm] = OUT(wnear[wb + mm] - sr);
     }
   }
 }
@@ -603,6 +641,8 @@ constexpr int kFarThreads = 128;
 constexpr int kFarTile = 128;
 constexpr int kTptF32 = 4;
 constexpr int kTptF64 = 2;
+static_assert(kFarThreads * kTptF32 == kFarBlockTargetsF32,
+              "the FP32 fold must centre coordinates exactly like the FP32 far kernel");
 
 }  // namespace
 
@@ -703,18 +743,22 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
 }
 
 cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp, const double* wnear,
-                        double* weff, cudaStream_t st) {
+                        void* weff, int match32, cudaStream_t st) {
   if (nr.nnz == 0) return cudaSuccess;
   const int warps = 4;
   const size_t sh = size_t(warps) * g.max_nf * 2 * sizeof(double);
-  if (sh > 200 * 1024) return cudaErrorInvalidValue;
+  if (sh > 48 * 1024) return cudaErrorInvalidValue;  // max_nf <= 289 keeps this <= 18.5 KB
   const dim3 grid(static_cast<unsigned>((nr.nnz + warps - 1) / warps)), block(32 * warps);
   if (kp.kind == 1) {
-    if (sh > 48 * 1024) cudaFuncSetAttribute(fold_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
-    fold_kernel<1><<<grid, block, sh, st>>>(g, nr, kp, wnear, weff);
+    if (match32)
+      fold_kernel<1, 1, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
+    else
+      fold_kernel<1, 0, double><<<grid, block, sh, st>>>(g, nr, kp, wnear, (double*)weff);
   } else {
-    if (sh > 48 * 1024) cudaFuncSetAttribute(fold_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
-    fold_kernel<0><<<grid, block, sh, st>>>(g, nr, kp, wnear, weff);
+    if (match32)
+      fold_kernel<0, 1, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
+    else
+      fold_kernel<0, 0, double><<<grid, block, sh, st>>>(g, nr, kp, wnear, (double*)weff);
   }
   count();
   return cudaGetLastError();

@@ -219,11 +219,12 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   const size_t wlen = size_t(nquad) * (cplx ? 2 : 1);
   BIE_CUDA(weff64_.alloc(std::max<size_t>(wlen, 1)));
   if (wlen) BIE_CUDA(cudaMemcpyAsync(weff64_.p, s.wnear, wlen * sizeof(double), cudaMemcpyHostToDevice, st));
-  BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff64_.p, st));
   if (s.keep_f32) {
+    // FP32 path: subtract the smooth part as the FP32 far kernel computes it
     BIE_CUDA(weff32_.alloc(std::max<size_t>(wlen, 1)));
-    BIE_CUDA(dev::launch_to_f32(weff64_.p, weff32_.p, int64_t(wlen), st));
+    BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff32_.p, 1, st));
   }
+  BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff64_.p, 0, st));
   for (auto& e : ev_) BIE_CUDA(cudaEventCreate(&e));
   // host vectors above are consumed by async copies: wait before they go
   BIE_CUDA(cudaStreamSynchronize(st));
