@@ -899,6 +899,66 @@ int bie_plan_timing(void* plan, int64_t enable, double* times) {
   return BIE_OK;
 }
 
+int bie_farfield_dev(int64_t kind, const double* zk, int64_t ns, const double* src_dev,
+                     const double* nrm_dev, const double* charge_dev, const double* dipstr_dev,
+                     int64_t nt, const double* targ_dev, double thresh, int64_t iprec,
+                     double* pot_dev, void* stream) {
+  if ((kind != 0 && kind != 1) || (iprec != 0 && iprec != 1) || ns < 0 || nt < 0) {
+    bie::set_last_error("bie_farfield_dev: bad kind/iprec/sizes");
+    return BIE_ERR_ARG;
+  }
+  if (nt == 0) return BIE_OK;
+  return guarded([&] {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int devn = 0, sms = 148;
+    cudaGetDevice(&devn);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, devn);
+    bie::dev::Geometry g;
+    g.ntarg = nt;
+    g.nptso = ns;
+    g.tx = targ_dev;
+    g.ty = targ_dev + nt;
+    g.tz = targ_dev + 2 * nt;
+    g.sx = src_dev;
+    g.sy = src_dev + ns;
+    g.sz = src_dev + 2 * ns;
+    g.snx = nrm_dev;
+    g.sny = nrm_dev + ns;
+    g.snz = nrm_dev + 2 * ns;
+    bie::dev::KParams kp;
+    kp.kind = int(kind);
+    if (kind == 1) {
+      kp.kr = zk[0];
+      kp.ki = zk[1];
+    }
+    kp.thresh = thresh;
+    const int c = kind == 1 ? 2 : 1;
+    const int nch = bie::dev::far_nchunks(nt, std::max<int64_t>(ns, 1), int(kind), int(iprec), 1, sms);
+    bie::DBuf<double> str, partial;
+    if (str.alloc(std::max<int64_t>(ns, 1) * 2 * c) ||
+        partial.alloc(size_t(nch) * nt * c)) {
+      bie::set_last_error("device allocation failed");
+      return BIE_ERR_NOMEM;
+    }
+    bie::dev::MatvecArgs a;
+    a.precision = int(iprec);
+    a.nd = 1;
+    a.nchunks = nch;
+    a.strengths = str.p;
+    a.partial = partial.p;
+    cudaError_t e = bie::dev::launch_pack_strengths(int(kind), int(iprec), ns, charge_dev,
+                                                    dipstr_dev, str.p, st);
+    if (e == cudaSuccess) e = bie::dev::launch_far(g, kp, a, st);
+    if (e == cudaSuccess) e = bie::dev::launch_reduce_partials(int(kind), partial.p, nch, nt, pot_dev, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // scratch is released below
+    if (e != cudaSuccess) {
+      bie::set_last_error(cudaGetErrorString(e));
+      return BIE_ERR_CUDA;
+    }
+    return BIE_OK;
+  });
+}
+
 int64_t bie_launch_count(void) { return bie::dev::launch_count(); }
 
 int bie_measure_fp32_peak(double* tflops, double* ms) {

@@ -86,6 +86,13 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
 cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp,
                         const double* wnear, void* weff, int match32, cudaStream_t st);
 cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t st);
+// Caller strengths (charge, dipole strength per source; complex interleaved
+// when kind == 1) -> far-kernel layout in the far precision, times 1/(4 pi).
+cudaError_t launch_pack_strengths(int kind, int precision, int64_t ns, const double* charge,
+                                  const double* dipstr, void* str, cudaStream_t st);
+// pot[i] = sum_c partial[c][i] (complex when kind == 1).
+cudaError_t launch_reduce_partials(int kind, const double* partial, int nchunks, int64_t ntarg,
+                                   double* pot, cudaStream_t st);
 
 // Number of source chunks the far kernel splits the sources into (the
 // partial-potential scratch holds nchunks*ntarg*nd values).

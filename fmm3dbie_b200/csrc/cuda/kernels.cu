@@ -457,6 +457,51 @@ __global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __res
   }
 }
 
+// Direct far-field evaluation from caller strengths: pack (charge, dipole
+// strength) per source into the far kernel's layout, scaled by 1/(4 pi).
+template <typename R, int CPLX>
+__global__ void pack_strengths_kernel(const double* __restrict__ charge,
+                                      const double* __restrict__ dipstr, int64_t ns,
+                                      R* __restrict__ str) {
+  for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < ns;
+       s += int64_t(gridDim.x) * blockDim.x) {
+    if (CPLX) {
+      str[4 * s + 0] = R(charge[2 * s] * kOver4Pi);
+      str[4 * s + 1] = R(charge[2 * s + 1] * kOver4Pi);
+      str[4 * s + 2] = R(dipstr[2 * s] * kOver4Pi);
+      str[4 * s + 3] = R(dipstr[2 * s + 1] * kOver4Pi);
+    } else {
+      str[2 * s + 0] = R(charge[s] * kOver4Pi);
+      str[2 * s + 1] = R(dipstr[s] * kOver4Pi);
+    }
+  }
+}
+
+// pot[i] = sum over chunks of partial[c][i]
+template <int CPLX>
+__global__ void reduce_partials_kernel(const double* __restrict__ partial, int nchunks,
+                                       int64_t ntarg, double* __restrict__ pot) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < ntarg;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    double ar = 0, ai = 0;
+    for (int c = 0; c < nchunks; ++c) {
+      const size_t o = size_t(c) * ntarg + i;
+      if (CPLX) {
+        ar += partial[2 * o];
+        ai += partial[2 * o + 1];
+      } else {
+        ar += partial[o];
+      }
+    }
+    if (CPLX) {
+      pot[2 * i] = ar;
+      pot[2 * i + 1] = ai;
+    } else {
+      pot[i] = ar;
+    }
+  }
+}
+
 __global__ void to_f32_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
@@ -767,6 +812,36 @@ cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp, co
 cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   to_f32_kernel<<<grid_for(n, 256), 256, 0, st>>>(in, out, n);
+  count();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_strengths(int kind, int precision, int64_t ns, const double* charge,
+                                  const double* dipstr, void* str, cudaStream_t st) {
+  if (ns == 0) return cudaSuccess;
+  const int b = grid_for(ns, 256);
+  if (precision == 1) {
+    if (kind == 1)
+      pack_strengths_kernel<float, 1><<<b, 256, 0, st>>>(charge, dipstr, ns, (float*)str);
+    else
+      pack_strengths_kernel<float, 0><<<b, 256, 0, st>>>(charge, dipstr, ns, (float*)str);
+  } else {
+    if (kind == 1)
+      pack_strengths_kernel<double, 1><<<b, 256, 0, st>>>(charge, dipstr, ns, (double*)str);
+    else
+      pack_strengths_kernel<double, 0><<<b, 256, 0, st>>>(charge, dipstr, ns, (double*)str);
+  }
+  count();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_partials(int kind, const double* partial, int nchunks, int64_t ntarg,
+                                   double* pot, cudaStream_t st) {
+  if (ntarg == 0) return cudaSuccess;
+  if (kind == 1)
+    reduce_partials_kernel<1><<<grid_for(ntarg, 256), 256, 0, st>>>(partial, nchunks, ntarg, pot);
+  else
+    reduce_partials_kernel<0><<<grid_for(ntarg, 256), 256, 0, st>>>(partial, nchunks, ntarg, pot);
   count();
   return cudaGetLastError();
 }

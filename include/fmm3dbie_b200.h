@@ -292,6 +292,23 @@ int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
  * same four for the f32 matvecs. */
 int bie_plan_timing(void* plan, int64_t enable, double* times);
 
+/* ---- far field on device buffers ----------------------------------------- */
+/* The far-field sum that lfmm3d / hfmm3d compute inside lpcomp_*_addsub
+ * (lap_comb_dir.f90:1094, helm_comb_dir.f:1117), evaluated directly:
+ *   pot(t) = sum_s [charge_s G(t,s) + dipstr_s n_s . grad_s G(t,s)],
+ *   G = e^{ikr}/(4 pi r) (k = 0 for Laplace), pairs with r^2 < thresh^2
+ *   skipped (get_fmm_thresh.f:81).
+ * Device pointers; coordinates are SoA: src_dev = x[ns], y[ns], z[ns];
+ * nrm_dev (unit vectors) likewise; targ_dev = x[nt], y[nt], z[nt].
+ * kind 0: real charge/dipstr/pot; kind 1: complex interleaved, zk = (re,im).
+ * iprec 0: FP64 sum, 1: FP32 pair sum accumulated in FP64 per source tile.
+ * Allocates its scratch (per-chunk partial sums) with cudaMalloc and
+ * returns after the stream has finished the call. */
+int bie_farfield_dev(int64_t kind, const double* zk, int64_t ns, const double* src_dev,
+                     const double* nrm_dev, const double* charge_dev, const double* dipstr_dev,
+                     int64_t nt, const double* targ_dev, double thresh, int64_t iprec,
+                     double* pot_dev, void* stream);
+
 /* ---- measurement helpers (no reference counterpart) ---------------------- */
 /* Number of kernels this library has launched in the process. */
 int64_t bie_launch_count(void);
