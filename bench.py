@@ -71,6 +71,62 @@ def build_problem(nref=3, norder=6):
     return s, st, rhs, time.time() - t
 
 
+def gpu_uuid(dev_index):
+    """NVML/nvidia-smi identifier of a CUDA device (CUDA ordinals and NVML
+    indices differ under CUDA_VISIBLE_DEVICES)."""
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(dev_index).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return str(dev_index)
+
+
+class NvmlClockSampler:
+    """Clocks and throttle reasons sampled every 20 ms through NVML from a
+    background thread during the timed region."""
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40}
+
+    def __init__(self, dev_index, period=0.02):
+        import threading
+        import pynvml
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        self.h = pynvml.nvmlDeviceGetHandleByUUID(gpu_uuid(dev_index).encode())
+        self.period = period
+        self.rows = []
+        self.stop_ev = threading.Event()
+        self.th = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_ev.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+                try:
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                except Exception:
+                    rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                self.rows.append((sm, smax, rs))
+            except Exception:
+                pass
+            self.stop_ev.wait(self.period)
+
+    def start(self):
+        self.th.start()
+
+    def stop(self):
+        self.stop_ev.set()
+        self.th.join(timeout=5)
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({k for r in self.rows for k, b in self.BITS.items() if r[2] & b})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(r[1] for r in self.rows) if self.rows else None,
+                "reasons": reasons, "samples": len(self.rows), "sampler": "nvml"}
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -78,7 +134,7 @@ class ClockSampler:
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
-        self.gpu = gpu_index
+        self.gpu = gpu_uuid(gpu_index)
         self.proc = None
         self.f = None
 
@@ -194,14 +250,21 @@ def reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--matvec-only", type=int, default=0,
+                    help="build the workload, run this many matvecs (see --prec) and exit "
+                         "(the command the ncu summaries in profiles/ use)")
+    ap.add_argument("--prec", type=int, default=1, help="matvec precision for --matvec-only")
+    ap.add_argument("--clock-sampler", default="nvml", choices=["nvml", "smi"])
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.matvec_only:
+        return matvec_only(args)
 
     import torch
     import torch.distributed as dist
@@ -260,13 +323,20 @@ def main():
     for _ in range(args.warmup):
         mixed()
     P.timing(True)
-    clocks = ClockSampler(local)
+    if args.clock_sampler == "nvml":
+        try:
+            clocks = NvmlClockSampler(local)
+        except Exception:
+            clocks = ClockSampler(local)
+    else:
+        clocks = ClockSampler(local)
     clocks.start()
     n0 = lib.bie_launch_count()
     tsm, (xm, infom) = timed(mixed, args.steps, 0)
     launches = int(lib.bie_launch_count() - n0)
     ck = clocks.stop()
     stages = P.timing(False)
+    pinfo = P.info()
     tm = float(np.mean(tsm))
     tmax = float(np.sum(tsm))
     if world > 1:
@@ -341,7 +411,9 @@ def main():
                       "rel_err": relerr(xm), "fp64_matvecs": infom["fp64_matvecs"],
                       "fp32_matvecs": infom["fp32_matvecs"]},
             "problem": {"npts": P.npts, "nptso": P.nptso, "nnz": P.nnz, "nquad": P.nquad,
-                        "setup_s": round(t_setup, 2), "far_chunks": list(P.nchunks)},
+                        "setup_s": round(t_setup, 2),
+                        "far_shape_variant_chunks": {"f64": [int(pinfo[8]), int(pinfo[5])],
+                                                     "f32": [int(pinfo[9]), int(pinfo[6])]}},
             "roofline": {"kernel": "far_kernel<helm,f32>", "bound": "fp32", "achieved": achieved,
                          "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
                          "traffic": traffic,
@@ -362,6 +434,23 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+def matvec_only(args):
+    import torch
+    from fmm3dbie_b200 import Plan
+    s, st, rhs, _ = build_problem()
+    P = Plan(1, ZPARS, s, st.near, st.over)
+    r = torch.tensor(rhs, device="cuda")
+    for _ in range(args.matvec_only):
+        P.matvec(r, args.prec)
+    torch.cuda.synchronize()
+    t = P.timing(True)
+    P.matvec(r, args.prec)
+    torch.cuda.synchronize()
+    t = P.timing(False)
+    print(json.dumps({"matvec_prec": args.prec, "stage_ms": t}))
     return 0
 
 

@@ -831,6 +831,8 @@ int bie_plan_info(void* plan, int64_t* info) {
   info[5] = P->nchunks_for(0, 1);
   info[6] = P->nchunks_for(1, 1);
   info[7] = P->kind;
+  info[8] = P->far_config(0, 1).variant;
+  info[9] = P->far_config(1, 1).variant;
   return BIE_OK;
 }
 

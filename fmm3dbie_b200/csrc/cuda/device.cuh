@@ -71,6 +71,7 @@ struct MatvecArgs {
   double* partial = nullptr;      // nchunks*ntarg*nd*(1 or 2)
   const void* weff = nullptr;     // W_eff in f64 or f32
   int weff_f32 = 0;
+  int far_variant = 0;            // far-kernel block shape (see far_block_targets)
 };
 
 cudaError_t launch_strengths(const Geometry& g, const KParams& kp, const MatvecArgs& a,
@@ -97,6 +98,14 @@ cudaError_t launch_reduce_partials(int kind, const double* partial, int nchunks,
 // Number of source chunks the far kernel splits the sources into (the
 // partial-potential scratch holds nchunks*ntarg*nd values).
 int far_nchunks(int64_t ntarg, int64_t nptso, int kind, int precision, int nd, int num_sms);
+// Far-kernel block shapes ("variants"): targets per block of a variant (512
+// for every f32 variant), resident blocks per SM, and the number of source
+// chunks that fills `waves` waves of resident blocks.
+int far_variants();
+int far_block_targets(int precision, int variant);
+int far_blocks_per_sm(const KParams& kp, int precision, int variant);
+int far_chunks_for_waves(int64_t ntarg, int64_t nptso, int precision, int variant, int nd,
+                         int num_sms, int blocks_per_sm, double waves);
 
 // ---- GMRES helpers --------------------------------------------------------
 // Vectors hold npts points x nd densities (point-major), n = npts*nd values

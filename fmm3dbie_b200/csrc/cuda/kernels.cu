@@ -87,12 +87,12 @@ __global__ void strengths_kernel(Geometry g, KParams kp, const double* __restric
 // ---------------------------------------------------------------------------
 // (b) far field: tiled direct N-body
 // ---------------------------------------------------------------------------
-// 2*pi split for Cody-Waite reduction: kHi has 8 significant bits so n*kHi
-// is exact for |n| < 2^16; kLo = 2*pi - kHi rounded to float.
-constexpr float kTwoPiHi = 6.28125f;
-constexpr float kTwoPiLo = 1.9353071795864769253e-3f;
-constexpr float kInvTwoPi = 0.15915494309189533577f;
-
+// Contribution of one source to one target: charge c = (s.x, s.y), dipole
+// strength d = (s.z, s.w) along the source normal n,
+//   e^{ikr}/r [ c + d (n.(t-s)) (1 - ikr) / r^2 ],   (1/(4 pi) is in c, d).
+// The phase kr carries an absolute error of about kr 2^-24 in single
+// precision already; __sincosf's scaled argument adds an error of the same
+// order, so no separate range reduction is done.
 __device__ __forceinline__ void pair_helm(float tx, float ty, float tz, const float4 g0,
                                           const float2 g1, const float4 s, float k, float kim,
                                           float thr2, bool ck, float& pr, float& pi) {
@@ -101,20 +101,18 @@ __device__ __forceinline__ void pair_helm(float tx, float ty, float tz, const fl
   const float rinv = (r2 >= thr2) ? rsqrtf(r2) : 0.0f;
   const float r = r2 * rinv;
   const float kr = k * r;
-  const float nrev = rintf(kr * kInvTwoPi);
-  float xr = fmaf(-nrev, kTwoPiHi, kr);
-  xr = fmaf(-nrev, kTwoPiLo, xr);
   float sn, cs;
-  __sincosf(xr, &sn, &cs);
+  __sincosf(kr, &sn, &cs);
   float rs = rinv;
   if (ck) rs *= __expf(-kim * r);
   const float dn = fmaf(dx, g0.w, fmaf(dy, g1.x, dz * g1.y));
-  // dipole factor d * (n.(t-s)) (1 - i k r) / r^2 with complex k
-  const float q = dn * rinv * rinv;
-  const float wr = ck ? q * (1.0f + kim * r) : q;
-  const float wi = -q * kr;
-  const float er = fmaf(s.z, wr, fmaf(-s.w, wi, s.x)) * rs;
-  const float ei = fmaf(s.z, wi, fmaf(s.w, wr, s.y)) * rs;
+  const float u = dn * (rinv * rinv);
+  // x = c + d u (1 - i k r); complex k = kr + i kim gives (1 + kim r) - i kr r
+  const float ur = ck ? u * (1.0f + kim * r) : u;
+  const float p = u * kr;
+  const float xr = fmaf(s.w, p, fmaf(s.z, ur, s.x));
+  const float xi = fmaf(-s.z, p, fmaf(s.w, ur, s.y));
+  const float er = xr * rs, ei = xi * rs;
   pr = fmaf(cs, er, fmaf(-sn, ei, pr));
   pi = fmaf(cs, ei, fmaf(sn, er, pi));
 }
@@ -212,7 +210,7 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
     R pr[TPT], pi[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) pr[t] = pi[t] = R(0);
-#pragma unroll 2
+#pragma unroll 4
     for (int j = 0; j < TILE; ++j) {
       const R4 a = sg0[j];
       const R2 b = sg1[j];
@@ -731,39 +729,114 @@ cudaError_t launch_strengths(const Geometry& g, const KParams& kp, const MatvecA
   return cudaGetLastError();
 }
 
-cudaError_t launch_far(const Geometry& g, const KParams& kp, const MatvecArgs& a, cudaStream_t st) {
-  if (g.ntarg == 0) return cudaSuccess;
-  const int tpt = a.precision == 1 ? kTptF32 : kTptF64;
-  const int64_t per_block = int64_t(kFarThreads) * tpt;
+namespace {
+// Far-kernel shapes.  Every f32 variant keeps kFarThreads*kTptF32 = 512
+// targets per block (the FP32 fold centres coordinates per 512 targets).
+template <int KIND, typename R, int NT, int TPT, bool CK>
+cudaError_t launch_far_t(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                         cudaStream_t st) {
+  const int64_t per_block = int64_t(NT) * TPT;
   const int64_t tblocks = (g.ntarg + per_block - 1) / per_block;
   int64_t chunk = (g.nptso + a.nchunks - 1) / a.nchunks;
   chunk = ((chunk + kFarTile - 1) / kFarTile) * kFarTile;
-  const dim3 grid(static_cast<unsigned>(tblocks), static_cast<unsigned>(a.nchunks), static_cast<unsigned>(a.nd));
-  const dim3 block(kFarThreads);
-  const bool ck = kp.kind == 1 && kp.ki != 0.0;
-  if (a.precision == 1) {
-    const float* s = (const float*)a.strengths;
-    if (kp.kind == 1) {
-      if (ck)
-        far_kernel<1, float, kFarThreads, kTptF32, kFarTile, true><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
-      else
-        far_kernel<1, float, kFarThreads, kTptF32, kFarTile, false><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
-    } else {
-      far_kernel<0, float, kFarThreads, kTptF32, kFarTile, false><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
-    }
-  } else {
-    const double* s = (const double*)a.strengths;
-    if (kp.kind == 1) {
-      if (ck)
-        far_kernel<1, double, kFarThreads, kTptF64, kFarTile, true><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
-      else
-        far_kernel<1, double, kFarThreads, kTptF64, kFarTile, false><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
-    } else {
-      far_kernel<0, double, kFarThreads, kTptF64, kFarTile, false><<<grid, block, 0, st>>>(g, kp, s, a.partial, chunk, a.nd);
-    }
-  }
-  count();
+  const dim3 grid(static_cast<unsigned>(tblocks), static_cast<unsigned>(a.nchunks),
+                  static_cast<unsigned>(a.nd));
+  far_kernel<KIND, R, NT, TPT, kFarTile, CK><<<grid, NT, 0, st>>>(
+      g, kp, static_cast<const R*>(a.strengths), a.partial, chunk, a.nd);
   return cudaGetLastError();
+}
+
+template <int KIND, typename R, int NT, int TPT, bool CK>
+int occupancy_t() {
+  int b = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, far_kernel<KIND, R, NT, TPT, kFarTile, CK>, NT,
+                                                0);
+  return b;
+}
+
+// (threads, targets per thread) of each variant
+constexpr int kF32Shapes[3][2] = {{128, 4}, {64, 8}, {256, 2}};
+constexpr int kF64Shapes[3][2] = {{128, 2}, {64, 4}, {256, 1}};
+
+template <int KIND, typename R, bool CK, int V>
+cudaError_t far_dispatch(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                         cudaStream_t st, int* occ) {
+  constexpr bool F32 = sizeof(R) == 4;
+  constexpr int NT = F32 ? kF32Shapes[V][0] : kF64Shapes[V][0];
+  constexpr int TPT = F32 ? kF32Shapes[V][1] : kF64Shapes[V][1];
+  if (occ) {
+    *occ = occupancy_t<KIND, R, NT, TPT, CK>();
+    return cudaSuccess;
+  }
+  return launch_far_t<KIND, R, NT, TPT, CK>(g, kp, a, st);
+}
+
+template <int KIND, typename R, bool CK>
+cudaError_t far_variant(int v, const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                        cudaStream_t st, int* occ) {
+  switch (v) {
+    case 1:
+      return far_dispatch<KIND, R, CK, 1>(g, kp, a, st, occ);
+    case 2:
+      return far_dispatch<KIND, R, CK, 2>(g, kp, a, st, occ);
+    default:
+      return far_dispatch<KIND, R, CK, 0>(g, kp, a, st, occ);
+  }
+}
+
+cudaError_t far_any(const Geometry& g, const KParams& kp, const MatvecArgs& a, cudaStream_t st,
+                    int* occ) {
+  const bool ck = kp.kind == 1 && kp.ki != 0.0;
+  const int v = a.far_variant;
+  if (a.precision == 1) {
+    if (kp.kind == 1)
+      return ck ? far_variant<1, float, true>(v, g, kp, a, st, occ)
+                : far_variant<1, float, false>(v, g, kp, a, st, occ);
+    return far_variant<0, float, false>(v, g, kp, a, st, occ);
+  }
+  if (kp.kind == 1)
+    return ck ? far_variant<1, double, true>(v, g, kp, a, st, occ)
+              : far_variant<1, double, false>(v, g, kp, a, st, occ);
+  return far_variant<0, double, false>(v, g, kp, a, st, occ);
+}
+}  // namespace
+
+cudaError_t launch_far(const Geometry& g, const KParams& kp, const MatvecArgs& a, cudaStream_t st) {
+  if (g.ntarg == 0) return cudaSuccess;
+  const cudaError_t e = far_any(g, kp, a, st, nullptr);
+  count();
+  return e;
+}
+
+int far_variants() { return 3; }
+
+int far_block_targets(int precision, int variant) {
+  const int v = variant < 0 || variant > 2 ? 0 : variant;
+  return precision == 1 ? kF32Shapes[v][0] * kF32Shapes[v][1]
+                        : kF64Shapes[v][0] * kF64Shapes[v][1];
+}
+
+int far_blocks_per_sm(const KParams& kp, int precision, int variant) {
+  MatvecArgs a;
+  a.precision = precision;
+  a.far_variant = variant;
+  Geometry g;
+  int occ = 0;
+  far_any(g, kp, a, nullptr, &occ);
+  return occ;
+}
+
+int far_chunks_for_waves(int64_t ntarg, int64_t nptso, int precision, int variant, int nd,
+                         int num_sms, int blocks_per_sm, double waves) {
+  const int64_t bt = far_block_targets(precision, variant);
+  const int64_t tblocks = (ntarg + bt - 1) / bt;
+  const double slots = double(num_sms) * std::max(blocks_per_sm, 1) * waves;
+  int64_t s = std::max<int64_t>(1, int64_t(slots / double(tblocks * nd) + 0.5));
+  s = std::min<int64_t>(s, std::max<int64_t>(1, (nptso + kFarTile - 1) / kFarTile));
+  // drop chunks that the tile rounding would leave empty
+  int64_t chunk = (nptso + s - 1) / s;
+  chunk = ((chunk + kFarTile - 1) / kFarTile) * kFarTile;
+  return int((nptso + chunk - 1) / chunk);
 }
 
 cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,

@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -231,15 +233,102 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   return kOk;
 }
 
-int Plan::nchunks_for(int precision, int nd) const {
-  return dev::far_nchunks(ntarg, nptso, kind, precision, nd, num_sms);
+int Plan::nchunks_for(int precision, int nd) const { return far_config(precision, nd).nchunks; }
+
+namespace {
+// Process-wide cache of tuned far-kernel shapes, keyed by everything the
+// timing depends on.
+using FarKey = std::tuple<int, int, int, int, int, int64_t, int64_t>;
+std::mutex g_far_mu;
+std::map<FarKey, Plan::FarConfig> g_far_cache;
+
+int env_int(const char* name, int dflt) {
+  const char* v = std::getenv(name);
+  return v && *v ? std::atoi(v) : dflt;
+}
+double env_double(const char* name, double dflt) {
+  const char* v = std::getenv(name);
+  return v && *v ? std::atof(v) : dflt;
+}
+}  // namespace
+
+Plan::FarConfig Plan::far_config(int precision, int nd) const {
+  auto it = far_cfg_.find({precision, nd});
+  if (it != far_cfg_.end()) return it->second;
+  // default shape before tuning: variant 0, four waves of resident blocks
+  FarConfig c;
+  c.variant = std::min(std::max(env_int("BIE_FAR_VARIANT", 0), 0), dev::far_variants() - 1);
+  const int bps = dev::far_blocks_per_sm(kp, precision, c.variant);
+  c.nchunks = dev::far_chunks_for_waves(ntarg, nptso, precision, c.variant, nd, num_sms, bps,
+                                        env_double("BIE_FAR_WAVES", 4.0));
+  return c;
 }
 
-int Plan::ensure_workspace(int precision, int nd) {
-  const int nch = nchunks_for(precision, nd);
+int Plan::ensure_workspace(int precision, int nd, int nchunks) {
+  (void)precision;
   const size_t sreals = size_t(nptso) * nd * (cplx ? 4 : 2);
   BIE_CUDA(str_.alloc(sreals * sizeof(double)));
-  BIE_CUDA(partial_.alloc(std::max<size_t>(1, size_t(nch) * ntarg * nd * (cplx ? 2 : 1))));
+  BIE_CUDA(partial_.alloc(std::max<size_t>(1, size_t(nchunks) * ntarg * nd * (cplx ? 2 : 1))));
+  return kOk;
+}
+
+int Plan::tune_far(int precision, int nd, dev::MatvecArgs& a, cudaStream_t st, FarConfig& best) {
+  const FarKey key{device, kind, kp.ki != 0.0 ? 1 : 0, precision, nd, ntarg, nptso};
+  {
+    std::lock_guard<std::mutex> lk(g_far_mu);
+    auto it = g_far_cache.find(key);
+    if (it != g_far_cache.end()) {
+      best = it->second;
+      return kOk;
+    }
+  }
+  best = far_config(precision, nd);
+  const bool fixed = std::getenv("BIE_FAR_VARIANT") || std::getenv("BIE_FAR_WAVES") ||
+                     env_int("BIE_AUTOTUNE", 1) == 0;
+  if (!fixed && ntarg > 0) {
+    std::vector<FarConfig> cand;
+    for (int v = 0; v < dev::far_variants(); ++v) {
+      const int bps = dev::far_blocks_per_sm(kp, precision, v);
+      if (bps <= 0) continue;
+      for (double waves : {1.0, 2.0, 4.0, 8.0}) {
+        FarConfig c;
+        c.variant = v;
+        c.nchunks = dev::far_chunks_for_waves(ntarg, nptso, precision, v, nd, num_sms, bps, waves);
+        bool dup = false;
+        for (const auto& o : cand) dup |= (o.variant == c.variant && o.nchunks == c.nchunks);
+        if (!dup) cand.push_back(c);
+      }
+    }
+    int maxch = 1;
+    for (const auto& c : cand) maxch = std::max(maxch, c.nchunks);
+    int ier = ensure_workspace(precision, nd, maxch);
+    if (ier) return ier;
+    a.partial = partial_.p;
+    cudaEvent_t e0, e1;
+    BIE_CUDA(cudaEventCreate(&e0));
+    BIE_CUDA(cudaEventCreate(&e1));
+    best.ms = 1e30;
+    for (auto& c : cand) {
+      a.far_variant = c.variant;
+      a.nchunks = c.nchunks;
+      BIE_CUDA(dev::launch_far(g, kp, a, st));  // warm
+      BIE_CUDA(cudaEventRecord(e0, st));
+      BIE_CUDA(dev::launch_far(g, kp, a, st));
+      BIE_CUDA(cudaEventRecord(e1, st));
+      BIE_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      c.ms = ms;
+      if (ms < best.ms) best = c;
+      if (env_int("BIE_AUTOTUNE_LOG", 0))
+        std::fprintf(stderr, "far autotune: prec %d nd %d variant %d chunks %d : %.4f ms\n",
+                     precision, nd, c.variant, c.nchunks, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  std::lock_guard<std::mutex> lk(g_far_mu);
+  g_far_cache[key] = best;
   return kOk;
 }
 
@@ -249,12 +338,14 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
     set_last_error("plan built without an f32 copy of W_eff");
     return kErrArg;
   }
-  int ier = ensure_workspace(precision, nd);
+  FarConfig fc = far_config(precision, nd);
+  int ier = ensure_workspace(precision, nd, fc.nchunks);
   if (ier) return ier;
   dev::MatvecArgs a;
   a.precision = precision;
   a.nd = nd;
-  a.nchunks = nchunks_for(precision, nd);
+  a.nchunks = fc.nchunks;
+  a.far_variant = fc.variant;
   a.sigma = d_sigma;
   a.pot = d_pot;
   a.strengths = str_.p;
@@ -263,7 +354,19 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
   a.weff_f32 = precision == 1;
   if (timing) BIE_CUDA(cudaEventRecord(ev_[0], st));
   BIE_CUDA(dev::launch_strengths(g, kp, a, st));
-  if (timing) BIE_CUDA(cudaEventRecord(ev_[1], st));
+  if (far_cfg_.find({precision, nd}) == far_cfg_.end()) {
+    ier = tune_far(precision, nd, a, st, fc);
+    if (ier) return ier;
+    far_cfg_[{precision, nd}] = fc;
+    ier = ensure_workspace(precision, nd, fc.nchunks);
+    if (ier) return ier;
+    a.nchunks = fc.nchunks;
+    a.far_variant = fc.variant;
+    a.partial = partial_.p;
+    if (timing) BIE_CUDA(cudaEventRecord(ev_[1], st));
+  } else if (timing) {
+    BIE_CUDA(cudaEventRecord(ev_[1], st));
+  }
   BIE_CUDA(dev::launch_far(g, kp, a, st));
   if (timing) BIE_CUDA(cudaEventRecord(ev_[2], st));
   BIE_CUDA(dev::launch_combine(g, nr, kp, a, st));

@@ -3,7 +3,9 @@
 #pragma once
 #include <complex>
 #include <cstdint>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -110,6 +112,16 @@ class Plan {
   // precision 0 = f64, 1 = f32 far field + f32 W_eff.
   int matvec(int precision, int nd, const double* d_sigma, double* d_pot, cudaStream_t st);
   int nchunks_for(int precision, int nd) const;
+
+  // Far-kernel launch shape: block-shape variant and number of source
+  // chunks.  Chosen on first use per (precision, nd) by timing the
+  // candidates on this plan's data (cached process-wide per problem shape);
+  // BIE_FAR_VARIANT / BIE_FAR_WAVES fix it, BIE_AUTOTUNE=0 uses the default.
+  struct FarConfig {
+    int variant = 0, nchunks = 1;
+    double ms = 0;
+  };
+  FarConfig far_config(int precision, int nd) const;
   const double* d_wts() const { return wts_.p; }
 
   GmresWorkspace gws;  // reused across solves on this plan
@@ -119,7 +131,9 @@ class Plan {
   StageTimes times;
 
  private:
-  int ensure_workspace(int precision, int nd);
+  int ensure_workspace(int precision, int nd, int nchunks);
+  int tune_far(int precision, int nd, dev::MatvecArgs& a, cudaStream_t st, FarConfig& out);
+  std::map<std::pair<int, int>, FarConfig> far_cfg_;
   DBuf<double> tx_, ty_, tz_, sx_, sy_, sz_, snx_, sny_, snz_, sw_, imat_, wts_;
   DBuf<int32_t> pstart_, ostart_, pclass_, col_;
   DBuf<int64_t> cmoff_, row_ptr_, wofs_;

@@ -59,10 +59,16 @@ class Plan:
                                     L.ptr(over.ixyzso), L.ptr(over.srcover), L.ptr(over.wover),
                                     C.byref(h)), "bie_plan_create")
         self._h = h
-        info = np.zeros(8, np.int64)
-        lib.bie_plan_info(h, L.ptr(info))
+        info = self.info()
         self.npts, self.ntarg, self.nptso, self.nnz, self.nquad = (int(x) for x in info[:5])
         self.nchunks = (int(info[5]), int(info[6]))
+
+    def info(self):
+        """npts, ntarg, nptso, nnz, nquad, far chunks (f64, f32), kind, far
+        variant (f64, f32)."""
+        info = np.zeros(10, np.int64)
+        L.lib().bie_plan_info(self._h, L.ptr(info))
+        return info
 
     def close(self):
         if getattr(self, "_h", None):

@@ -272,8 +272,9 @@ int bie_plan_create(int64_t kind, const double* params, int64_t npatches,
                     const int64_t* ixyzso, const double* srcover, const double* whtsover,
                     void** plan);
 int bie_plan_destroy(void* plan);
-/* info[0..7] = npts, ntarg, nptso, nnz, nquad, nchunks(f64), nchunks(f32),
- * kind */
+/* info[0..9] = npts, ntarg, nptso, nnz, nquad, far-field source chunks (f64),
+ * (f32), kind, far-kernel shape variant (f64), (f32) -- the far-field shape
+ * is the tuned one once a matvec of that precision has run */
 int bie_plan_info(void* plan, int64_t* info);
 /* pot_dev = K sigma_dev for nd densities per point; iprec 0 f64, 1 f32 */
 int bie_plan_matvec(void* plan, int64_t iprec, int64_t nd, const double* sigma_dev,
