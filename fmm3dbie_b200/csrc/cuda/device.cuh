@@ -72,6 +72,7 @@ struct MatvecArgs {
   const void* weff = nullptr;     // W_eff in f64 or f32
   int weff_f32 = 0;
   int far_variant = 0;            // far-kernel block shape (see far_block_targets)
+  const void* ab = nullptr;       // per-source constants for the multi-density kernel
 };
 
 cudaError_t launch_strengths(const Geometry& g, const KParams& kp, const MatvecArgs& a,
@@ -101,11 +102,22 @@ int far_nchunks(int64_t ntarg, int64_t nptso, int kind, int precision, int nd, i
 // Far-kernel block shapes ("variants"): targets per block of a variant (512
 // for every f32 variant), resident blocks per SM, and the number of source
 // chunks that fills `waves` waves of resident blocks.
+// md = 1 selects the multi-density kernel's shapes (nd > 1).
 int far_variants();
-int far_block_targets(int precision, int variant);
-int far_blocks_per_sm(const KParams& kp, int precision, int variant);
+int far_block_targets(int precision, int variant, int md = 0);
+int far_md_group(int variant);
+int far_blocks_per_sm(const KParams& kp, int precision, int variant, int md = 0);
 int far_chunks_for_waves(int64_t ntarg, int64_t nptso, int precision, int variant, int nd,
-                         int num_sms, int blocks_per_sm, double waves);
+                         int num_sms, int blocks_per_sm, double waves, int md = 0);
+// Multi-density far field: a.strengths holds sigma_over[s][nd] (far
+// precision, from launch_oversample) and a.ab the per-source constants
+// (from launch_source_consts).
+cudaError_t launch_far_md(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                          cudaStream_t st);
+cudaError_t launch_oversample(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                              cudaStream_t st);
+cudaError_t launch_source_consts(const Geometry& g, const KParams& kp, int precision, void* ab,
+                                 cudaStream_t st);
 
 // ---- GMRES helpers --------------------------------------------------------
 // Vectors hold npts points x nd densities (point-major), n = npts*nd values

@@ -245,6 +245,181 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
 }
 
 // ---------------------------------------------------------------------------
+// (b') far field for several densities at once.
+//
+// Charge and dipole strengths of a layer potential are both proportional to
+// the same oversampled density, so each pair's kernel value
+//   K(t,s) = a_s G(t,s) + b_s dG/dn_s(t,s),  a_s = alpha w_s/(4pi), b_s = beta w_s/(4pi)
+// is computed once (the single-density pair function with unit density) and
+// applied to MD densities with one complex multiply-add each.  Coordinates
+// are centred on the first target of the enclosing 512-target block, as in
+// the single-density FP32 kernel, so the FP32 error-matched fold applies.
+// ab: per source (a, b) (complex: 4 reals, real: 2); sig: sigma_over[s][nd].
+// ---------------------------------------------------------------------------
+constexpr int kMdCentre = 512;
+
+template <int KIND, typename R, int NT, int TPT, int MD, int TILE, bool CK>
+__global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
+                                                    const R* __restrict__ ab,
+                                                    const R* __restrict__ sig, int nd,
+                                                    double* __restrict__ partial,
+                                                    int64_t chunk_len) {
+  using R2 = typename Vec<R>::T2;
+  using R4 = typename Vec<R>::T4;
+  constexpr int C = (KIND == 1) ? 2 : 1;  // reals per complex value
+  __shared__ R4 sg0[TILE];
+  __shared__ R2 sg1[TILE];
+  __shared__ R sab[TILE * 2 * C];
+  __shared__ R ssig[TILE * MD * C];
+  const int64_t ntarg = g.ntarg, nptso = g.nptso;
+  const int64_t tbase = int64_t(blockIdx.x) * NT * TPT;
+  const int m0 = blockIdx.z * MD;
+  const int64_t tcen = (tbase / kMdCentre) * kMdCentre;
+  const int64_t tc = tcen < ntarg ? tcen : ntarg - 1;
+  const double cx = g.tx[tc], cy = g.ty[tc], cz = g.tz[tc];
+  R tx[TPT], ty[TPT], tz[TPT];
+  double acc[TPT][MD][C];
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    const int64_t it = tbase + threadIdx.x + int64_t(t) * NT;
+    const int64_t ic = it < ntarg ? it : ntarg - 1;
+    tx[t] = R(g.tx[ic] - cx);
+    ty[t] = R(g.ty[ic] - cy);
+    tz[t] = R(g.tz[ic] - cz);
+#pragma unroll
+    for (int m = 0; m < MD; ++m)
+#pragma unroll
+      for (int c = 0; c < C; ++c) acc[t][m][c] = 0.0;
+  }
+  const R thr2 = R(kp.thresh * kp.thresh);
+  const R k = R(kp.kr), kim = R(kp.ki);
+  const int64_t s0 = int64_t(blockIdx.y) * chunk_len;
+  const int64_t s1 = min(s0 + chunk_len, nptso);
+  for (int64_t sb = s0; sb < s1; sb += TILE) {
+    const int ns = int((s1 - sb) < TILE ? (s1 - sb) : TILE);
+    __syncthreads();
+    for (int q = threadIdx.x; q < TILE; q += NT) {
+      const bool ok = q < ns;
+      const int64_t s = sb + q;
+      sg0[q] = ok ? R4{R(g.sx[s] - cx), R(g.sy[s] - cy), R(g.sz[s] - cz), R(g.snx[s])}
+                  : R4{R(0), R(0), R(0), R(0)};
+      sg1[q] = ok ? R2{R(g.sny[s]), R(g.snz[s])} : R2{R(0), R(0)};
+#pragma unroll
+      for (int c = 0; c < 2 * C; ++c) sab[q * 2 * C + c] = ok ? ab[size_t(s) * 2 * C + c] : R(0);
+    }
+    for (int q = threadIdx.x; q < TILE * MD; q += NT) {
+      const int qs = q / MD, mm = q - qs * MD;
+      const bool ok = qs < ns && m0 + mm < nd;
+#pragma unroll
+      for (int c = 0; c < C; ++c)
+        ssig[q * C + c] = ok ? sig[(size_t(sb + qs) * nd + m0 + mm) * C + c] : R(0);
+    }
+    __syncthreads();
+    R tr[TPT][MD][C];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t)
+#pragma unroll
+      for (int m = 0; m < MD; ++m)
+#pragma unroll
+        for (int c = 0; c < C; ++c) tr[t][m][c] = R(0);
+#pragma unroll 2
+    for (int j = 0; j < TILE; ++j) {
+      const R4 a = sg0[j];
+      const R2 b = sg1[j];
+      if constexpr (KIND == 1) {
+        const R4 s = reinterpret_cast<const R4*>(sab)[j];
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+          R kr_ = R(0), ki_ = R(0);
+          pair_helm(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, kr_, ki_);
+          const R2* sv = reinterpret_cast<const R2*>(ssig) + j * MD;
+#pragma unroll
+          for (int m = 0; m < MD; ++m) {
+            const R2 x = sv[m];
+            tr[t][m][0] = fma(kr_, x.x, fma(-ki_, x.y, tr[t][m][0]));
+            tr[t][m][1] = fma(kr_, x.y, fma(ki_, x.x, tr[t][m][1]));
+          }
+        }
+      } else {
+        const R2 s = reinterpret_cast<const R2*>(sab)[j];
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+          R kv = R(0);
+          pair_lap<R>(tx[t], ty[t], tz[t], a, b, s, thr2, kv);
+          const R* sv = ssig + j * MD;
+#pragma unroll
+          for (int m = 0; m < MD; ++m) tr[t][m][0] = fma(kv, sv[m], tr[t][m][0]);
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < TPT; ++t)
+#pragma unroll
+      for (int m = 0; m < MD; ++m)
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[t][m][c] += double(tr[t][m][c]);
+  }
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    const int64_t it = tbase + threadIdx.x + int64_t(t) * NT;
+    if (it >= ntarg) continue;
+#pragma unroll
+    for (int m = 0; m < MD; ++m) {
+      if (m0 + m >= nd) continue;
+      const size_t o = (size_t(blockIdx.y) * ntarg + it) * nd + m0 + m;
+#pragma unroll
+      for (int c = 0; c < C; ++c) partial[C * o + c] = acc[t][m][c];
+    }
+  }
+}
+
+// sigma_over[s][m] = (imat sigma_patch)[s][m] without scaling (several
+// densities); feeds far_md_kernel.
+template <typename R, int CPLX>
+__global__ void oversample_kernel(Geometry g, const double* __restrict__ sigma,
+                                  R* __restrict__ sover, int nd) {
+  extern __shared__ double sh[];
+  const int p = blockIdx.x;
+  const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
+  const int os = g.ostart[p], nf = g.ostart[p + 1] - os;
+  const double* M = g.imat + g.cmoff[g.pclass[p]];
+  const int C = CPLX ? 2 : 1;
+  for (int q = threadIdx.x; q < np * nd * C; q += blockDim.x) sh[q] = sigma[size_t(ps) * nd * C + q];
+  __syncthreads();
+  for (int q = threadIdx.x; q < nf * nd; q += blockDim.x) {
+    const int l = q / nd, m = q - l * nd;
+    const double* row = M + size_t(l) * np;
+    double sr = 0, si = 0;
+    for (int j = 0; j < np; ++j) {
+      const double mv = row[j];
+      sr = fma(mv, sh[C * (j * nd + m)], sr);
+      if (CPLX) si = fma(mv, sh[C * (j * nd + m) + 1], si);
+    }
+    const size_t o = size_t(os + l) * nd + m;
+    sover[C * o] = R(sr);
+    if (CPLX) sover[C * o + 1] = R(si);
+  }
+}
+
+// Per-source constants a_s = alpha w_s/(4pi), b_s = beta w_s/(4pi).
+template <typename R, int CPLX>
+__global__ void source_consts_kernel(Geometry g, KParams kp, R* __restrict__ ab) {
+  for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < g.nptso;
+       s += int64_t(gridDim.x) * blockDim.x) {
+    const double f = g.sw[s] * kOver4Pi;
+    if (CPLX) {
+      ab[4 * s + 0] = R(kp.ar * f);
+      ab[4 * s + 1] = R(kp.ai * f);
+      ab[4 * s + 2] = R(kp.br * f);
+      ab[4 * s + 3] = R(kp.bi * f);
+    } else {
+      ab[2 * s + 0] = R(kp.ar * f);
+      ab[2 * s + 1] = R(kp.br * f);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // (c) combine: far partials + near-correction SpMM, one warp per target row
 // ---------------------------------------------------------------------------
 template <int CPLX, typename W>
@@ -784,6 +959,59 @@ cudaError_t far_variant(int v, const Geometry& g, const KParams& kp, const Matve
   }
 }
 
+// multi-density variants: (threads, targets per thread, densities per block)
+constexpr int kMdShapes[3][3] = {{128, 1, 16}, {128, 2, 8}, {64, 2, 16}};
+
+template <int KIND, typename R, bool CK, int V>
+cudaError_t far_md_dispatch(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                            cudaStream_t st, int* occ) {
+  constexpr int NT = kMdShapes[V][0], TPT = kMdShapes[V][1], MD = kMdShapes[V][2];
+  if (occ) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        occ, far_md_kernel<KIND, R, NT, TPT, MD, kFarTile, CK>, NT, 0);
+    return cudaSuccess;
+  }
+  const int64_t tblocks = (g.ntarg + int64_t(NT) * TPT - 1) / (int64_t(NT) * TPT);
+  const int groups = (a.nd + MD - 1) / MD;
+  int64_t chunk = (g.nptso + a.nchunks - 1) / a.nchunks;
+  chunk = ((chunk + kFarTile - 1) / kFarTile) * kFarTile;
+  const dim3 grid(static_cast<unsigned>(tblocks), static_cast<unsigned>(a.nchunks),
+                  static_cast<unsigned>(groups));
+  far_md_kernel<KIND, R, NT, TPT, MD, kFarTile, CK><<<grid, NT, 0, st>>>(
+      g, kp, static_cast<const R*>(a.ab), static_cast<const R*>(a.strengths), a.nd, a.partial,
+      chunk);
+  return cudaGetLastError();
+}
+
+template <int KIND, typename R, bool CK>
+cudaError_t far_md_variant(int v, const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                           cudaStream_t st, int* occ) {
+  switch (v) {
+    case 1:
+      return far_md_dispatch<KIND, R, CK, 1>(g, kp, a, st, occ);
+    case 2:
+      return far_md_dispatch<KIND, R, CK, 2>(g, kp, a, st, occ);
+    default:
+      return far_md_dispatch<KIND, R, CK, 0>(g, kp, a, st, occ);
+  }
+}
+
+cudaError_t far_md_any(const Geometry& g, const KParams& kp, const MatvecArgs& a, cudaStream_t st,
+                       int* occ) {
+  const bool ck = kp.kind == 1 && kp.ki != 0.0;
+  const int v = a.far_variant;
+  if (a.precision == 1) {
+    if (kp.kind == 1)
+      return ck ? far_md_variant<1, float, true>(v, g, kp, a, st, occ)
+                : far_md_variant<1, float, false>(v, g, kp, a, st, occ);
+    return far_md_variant<0, float, false>(v, g, kp, a, st, occ);
+  }
+  if (kp.kind == 1)
+    return ck ? far_md_variant<1, double, true>(v, g, kp, a, st, occ)
+              : far_md_variant<1, double, false>(v, g, kp, a, st, occ);
+  return far_md_variant<0, double, false>(v, g, kp, a, st, occ);
+}
+
 cudaError_t far_any(const Geometry& g, const KParams& kp, const MatvecArgs& a, cudaStream_t st,
                     int* occ) {
   const bool ck = kp.kind == 1 && kp.ki != 0.0;
@@ -808,30 +1036,89 @@ cudaError_t launch_far(const Geometry& g, const KParams& kp, const MatvecArgs& a
   return e;
 }
 
+cudaError_t launch_far_md(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                          cudaStream_t st) {
+  if (g.ntarg == 0) return cudaSuccess;
+  const cudaError_t e = far_md_any(g, kp, a, st, nullptr);
+  count();
+  return e;
+}
+
+cudaError_t launch_oversample(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                              cudaStream_t st) {
+  const int cplx = kp.kind == 1;
+  const size_t sh = size_t(g.max_np) * a.nd * (cplx ? 2 : 1) * sizeof(double);
+  if (sh > 200 * 1024) return cudaErrorInvalidValue;
+  const dim3 grid(static_cast<unsigned>(g.npatches)), block(128);
+  auto go = [&](auto kern, auto* out) {
+    if (sh > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
+    kern<<<grid, block, sh, st>>>(g, a.sigma, out, a.nd);
+  };
+  if (a.precision == 1) {
+    if (cplx)
+      go(oversample_kernel<float, 1>, (float*)a.strengths);
+    else
+      go(oversample_kernel<float, 0>, (float*)a.strengths);
+  } else {
+    if (cplx)
+      go(oversample_kernel<double, 1>, (double*)a.strengths);
+    else
+      go(oversample_kernel<double, 0>, (double*)a.strengths);
+  }
+  count();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_source_consts(const Geometry& g, const KParams& kp, int precision, void* ab,
+                                 cudaStream_t st) {
+  if (g.nptso == 0) return cudaSuccess;
+  const int b = grid_for(g.nptso, 256);
+  if (precision == 1) {
+    if (kp.kind == 1)
+      source_consts_kernel<float, 1><<<b, 256, 0, st>>>(g, kp, (float*)ab);
+    else
+      source_consts_kernel<float, 0><<<b, 256, 0, st>>>(g, kp, (float*)ab);
+  } else {
+    if (kp.kind == 1)
+      source_consts_kernel<double, 1><<<b, 256, 0, st>>>(g, kp, (double*)ab);
+    else
+      source_consts_kernel<double, 0><<<b, 256, 0, st>>>(g, kp, (double*)ab);
+  }
+  count();
+  return cudaGetLastError();
+}
+
 int far_variants() { return 3; }
 
-int far_block_targets(int precision, int variant) {
+int far_block_targets(int precision, int variant, int md) {
   const int v = variant < 0 || variant > 2 ? 0 : variant;
+  if (md) return kMdShapes[v][0] * kMdShapes[v][1];
   return precision == 1 ? kF32Shapes[v][0] * kF32Shapes[v][1]
                         : kF64Shapes[v][0] * kF64Shapes[v][1];
 }
 
-int far_blocks_per_sm(const KParams& kp, int precision, int variant) {
+int far_md_group(int variant) { return kMdShapes[variant < 0 || variant > 2 ? 0 : variant][2]; }
+
+int far_blocks_per_sm(const KParams& kp, int precision, int variant, int md) {
   MatvecArgs a;
   a.precision = precision;
   a.far_variant = variant;
   Geometry g;
   int occ = 0;
-  far_any(g, kp, a, nullptr, &occ);
+  if (md)
+    far_md_any(g, kp, a, nullptr, &occ);
+  else
+    far_any(g, kp, a, nullptr, &occ);
   return occ;
 }
 
 int far_chunks_for_waves(int64_t ntarg, int64_t nptso, int precision, int variant, int nd,
-                         int num_sms, int blocks_per_sm, double waves) {
-  const int64_t bt = far_block_targets(precision, variant);
+                         int num_sms, int blocks_per_sm, double waves, int md) {
+  const int64_t bt = far_block_targets(precision, variant, md);
   const int64_t tblocks = (ntarg + bt - 1) / bt;
+  const int64_t zdim = md ? (nd + far_md_group(variant) - 1) / far_md_group(variant) : nd;
   const double slots = double(num_sms) * std::max(blocks_per_sm, 1) * waves;
-  int64_t s = std::max<int64_t>(1, int64_t(slots / double(tblocks * nd) + 0.5));
+  int64_t s = std::max<int64_t>(1, int64_t(slots / double(tblocks * zdim) + 0.5));
   s = std::min<int64_t>(s, std::max<int64_t>(1, (nptso + kFarTile - 1) / kFarTile));
   // drop chunks that the tile rounding would leave empty
   int64_t chunk = (nptso + s - 1) / s;

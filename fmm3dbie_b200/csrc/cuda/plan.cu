@@ -227,6 +227,11 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
     BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff32_.p, 1, st));
   }
   BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff64_.p, 0, st));
+  // per-source constants alpha w/(4pi), beta w/(4pi) for the multi-density far kernel
+  BIE_CUDA(ab64_.alloc(size_t(nptso) * (cplx ? 4 : 2)));
+  BIE_CUDA(ab32_.alloc(size_t(nptso) * (cplx ? 4 : 2)));
+  BIE_CUDA(dev::launch_source_consts(g, kp, 0, ab64_.p, st));
+  BIE_CUDA(dev::launch_source_consts(g, kp, 1, ab32_.p, st));
   for (auto& e : ev_) BIE_CUDA(cudaEventCreate(&e));
   // host vectors above are consumed by async copies: wait before they go
   BIE_CUDA(cudaStreamSynchronize(st));
@@ -257,11 +262,16 @@ Plan::FarConfig Plan::far_config(int precision, int nd) const {
   if (it != far_cfg_.end()) return it->second;
   // default shape before tuning: variant 0, four waves of resident blocks
   FarConfig c;
+  const int md = nd > 1;
   c.variant = std::min(std::max(env_int("BIE_FAR_VARIANT", 0), 0), dev::far_variants() - 1);
-  const int bps = dev::far_blocks_per_sm(kp, precision, c.variant);
+  const int bps = dev::far_blocks_per_sm(kp, precision, c.variant, md);
   c.nchunks = dev::far_chunks_for_waves(ntarg, nptso, precision, c.variant, nd, num_sms, bps,
-                                        env_double("BIE_FAR_WAVES", 4.0));
+                                        env_double("BIE_FAR_WAVES", md ? 2.0 : 4.0), md);
   return c;
+}
+
+cudaError_t Plan::launch_far_stage(const dev::MatvecArgs& a, cudaStream_t st) {
+  return a.nd > 1 ? dev::launch_far_md(g, kp, a, st) : dev::launch_far(g, kp, a, st);
 }
 
 int Plan::ensure_workspace(int precision, int nd, int nchunks) {
@@ -287,13 +297,17 @@ int Plan::tune_far(int precision, int nd, dev::MatvecArgs& a, cudaStream_t st, F
                      env_int("BIE_AUTOTUNE", 1) == 0;
   if (!fixed && ntarg > 0) {
     std::vector<FarConfig> cand;
+    const int md = nd > 1;
     for (int v = 0; v < dev::far_variants(); ++v) {
-      const int bps = dev::far_blocks_per_sm(kp, precision, v);
+      const int bps = dev::far_blocks_per_sm(kp, precision, v, md);
       if (bps <= 0) continue;
       for (double waves : {1.0, 2.0, 4.0, 8.0}) {
         FarConfig c;
         c.variant = v;
-        c.nchunks = dev::far_chunks_for_waves(ntarg, nptso, precision, v, nd, num_sms, bps, waves);
+        c.nchunks =
+            dev::far_chunks_for_waves(ntarg, nptso, precision, v, nd, num_sms, bps, waves, md);
+        // the partial sums grow with nchunks * nd: keep them under ~1 GiB
+        if (double(c.nchunks) * ntarg * nd * 16.0 > double(1 << 30) && waves > 1.0) continue;
         bool dup = false;
         for (const auto& o : cand) dup |= (o.variant == c.variant && o.nchunks == c.nchunks);
         if (!dup) cand.push_back(c);
@@ -311,9 +325,9 @@ int Plan::tune_far(int precision, int nd, dev::MatvecArgs& a, cudaStream_t st, F
     for (auto& c : cand) {
       a.far_variant = c.variant;
       a.nchunks = c.nchunks;
-      BIE_CUDA(dev::launch_far(g, kp, a, st));  // warm
+      BIE_CUDA(launch_far_stage(a, st));  // warm
       BIE_CUDA(cudaEventRecord(e0, st));
-      BIE_CUDA(dev::launch_far(g, kp, a, st));
+      BIE_CUDA(launch_far_stage(a, st));
       BIE_CUDA(cudaEventRecord(e1, st));
       BIE_CUDA(cudaEventSynchronize(e1));
       float ms = 0;
@@ -352,8 +366,12 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
   a.partial = partial_.p;
   a.weff = precision == 1 ? (const void*)weff32_.p : (const void*)weff64_.p;
   a.weff_f32 = precision == 1;
+  a.ab = precision == 1 ? (const void*)ab32_.p : (const void*)ab64_.p;
   if (timing) BIE_CUDA(cudaEventRecord(ev_[0], st));
-  BIE_CUDA(dev::launch_strengths(g, kp, a, st));
+  if (nd > 1)
+    BIE_CUDA(dev::launch_oversample(g, kp, a, st));
+  else
+    BIE_CUDA(dev::launch_strengths(g, kp, a, st));
   if (far_cfg_.find({precision, nd}) == far_cfg_.end()) {
     ier = tune_far(precision, nd, a, st, fc);
     if (ier) return ier;
@@ -367,7 +385,7 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
   } else if (timing) {
     BIE_CUDA(cudaEventRecord(ev_[1], st));
   }
-  BIE_CUDA(dev::launch_far(g, kp, a, st));
+  BIE_CUDA(launch_far_stage(a, st));
   if (timing) BIE_CUDA(cudaEventRecord(ev_[2], st));
   BIE_CUDA(dev::launch_combine(g, nr, kp, a, st));
   if (timing) {

@@ -133,6 +133,9 @@ class Plan {
  private:
   int ensure_workspace(int precision, int nd, int nchunks);
   int tune_far(int precision, int nd, dev::MatvecArgs& a, cudaStream_t st, FarConfig& out);
+  cudaError_t launch_far_stage(const dev::MatvecArgs& a, cudaStream_t st);
+  DBuf<double> ab64_;
+  DBuf<float> ab32_;
   std::map<std::pair<int, int>, FarConfig> far_cfg_;
   DBuf<double> tx_, ty_, tz_, sx_, sy_, sz_, snx_, sny_, snz_, sw_, imat_, wts_;
   DBuf<int32_t> pstart_, ostart_, pclass_, col_;
