@@ -259,7 +259,10 @@ def main():
                     help="build the workload, run this many matvecs (see --prec) and exit "
                          "(the command the ncu summaries in profiles/ use)")
     ap.add_argument("--prec", type=int, default=1, help="matvec precision for --matvec-only")
+    ap.add_argument("--nd", type=int, default=1, help="densities per matvec for --matvec-only")
     ap.add_argument("--clock-sampler", default="nvml", choices=["nvml", "smi"])
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the config-3 batched (64 right-hand sides) leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -393,6 +396,10 @@ def main():
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(s, st, int(info64["niter"][0]))
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        P.close()
+        batched = batched_leg(dev)
 
     if rank == 0:
         line = {
@@ -428,6 +435,7 @@ def main():
             "clocks": ck,
             "e2e": e2e,
             "cpu_baseline": base,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     P.close()
@@ -437,12 +445,66 @@ def main():
     return 0
 
 
+def batched_leg(dev, steps=1):
+    """Config 3: 64 incident plane waves on the same (1,2,3) ellipsoid at
+    zk = 5, zpars = (5, -5i, 1); rhs = -incident field at the nodes.  All 64
+    systems share every launch.  Reports solves/s (64 per batch) for the
+    mixed-precision and the plain FP64 paths and their error against a
+    tight FP64 solution."""
+    import torch
+    from fmm3dbie_b200 import Plan
+    from fmm3dbie_b200 import surface as S
+    zk = 5.0
+    zp = (zk, -1j * zk, 1.0)
+    s = S.icosa_ellipsoid(3, 6, (1.0, 2.0, 3.0))
+    t0 = time.time()
+    st = S.setup(s, 1, EPS, zp)
+    t_setup = time.time() - t0
+    rng = np.random.default_rng(3)
+    d = rng.normal(size=(64, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    rhs = -np.exp(1j * zk * (s.xyz @ d.T))
+    P = Plan(1, zp, s, st.near, st.over)
+    R = torch.tensor(np.ascontiguousarray(rhs), device=dev)
+    w = torch.tensor(s.qwts(), device=dev)[:, None]
+    xref, _ = P.solve(R, 0.5, mode=0, numit=300, eps_gmres=1e-12)
+
+    def relerr(x):
+        num = torch.sum(w * (x - xref).abs() ** 2, 0)
+        den = torch.sum(w * xref.abs() ** 2, 0)
+        return float(torch.max(torch.sqrt(num / den)))
+
+    out = {"workload": "config 3: 64 plane waves, ellipsoid (1,2,3), 1280 order-6 patches, "
+                       "zk=5, zpars=(5,-5i,1), eps=1e-7", "nrhs": 64, "setup_s": round(t_setup, 2),
+           "nptso": P.nptso}
+    for mode, tag in ((1, "mixed"), (0, "fp64")):
+        P.solve(R, 0.5, mode=mode, numit=300, eps_gmres=TOL_RES)  # warm-up (tunes the kernels)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            x, info = P.solve(R, 0.5, mode=mode, numit=300, eps_gmres=TOL_RES)
+            b.record()
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        t = float(np.mean(ts))
+        out[tag] = {"solves_per_s": 64 * 1000.0 / t, "ms_per_batch": t,
+                    "max_niter": int(np.max(info["niter"])), "max_rel_err": relerr(x)}
+    out["speedup_vs_fp64"] = out["fp64"]["ms_per_batch"] / out["mixed"]["ms_per_batch"]
+    P.close()
+    return out
+
+
 def matvec_only(args):
     import torch
     from fmm3dbie_b200 import Plan
     s, st, rhs, _ = build_problem()
     P = Plan(1, ZPARS, s, st.near, st.over)
     r = torch.tensor(rhs, device="cuda")
+    if args.nd > 1:
+        r = r[:, None].repeat(1, args.nd).contiguous()
     for _ in range(args.matvec_only):
         P.matvec(r, args.prec)
     torch.cuda.synchronize()

@@ -70,6 +70,65 @@ class Surface:
         return self.srcvals[:, 9:12]
 
 
+def disc_exps(iptype: int, norder: int):
+    """(uvs, umat, vmat, wts) of a patch type/order (get_disc_exps); umat maps
+    nodal values to basis coefficients (coefs = umat @ vals)."""
+    lib = _init()
+    npols = (norder + 1) * (norder + 2) // 2 if iptype == 1 else (norder + 1) ** 2
+    uvs = np.zeros((npols, 2))
+    um = np.zeros((npols, npols), order="F")
+    vm = np.zeros((npols, npols), order="F")
+    w = np.zeros(npols)
+    L.check(lib.bie_get_disc_exps(norder, npols, iptype, L.ptr(uvs), um.ctypes.data_as(L.PDBL),
+                                  vm.ctypes.data_as(L.PDBL), L.ptr(w)), "get_disc_exps")
+    return uvs, np.ascontiguousarray(um), np.ascontiguousarray(vm), w
+
+
+def from_srcvals(norders, iptype, srcvals) -> "Surface":
+    """Surface from nodal values only: srccoefs = umat * srcvals(1:9) per
+    patch (as getgeominfo / open_gov3_geometry do)."""
+    norders = np.ascontiguousarray(norders, np.int64)
+    iptype = np.ascontiguousarray(iptype, np.int64)
+    srcvals = np.ascontiguousarray(srcvals, float)
+    npols = np.array([(n + 1) * (n + 2) // 2 if t == 1 else (n + 1) ** 2
+                      for n, t in zip(norders, iptype)], np.int64)
+    ixyzs = np.concatenate([[1], 1 + np.cumsum(npols)]).astype(np.int64)
+    srccoefs = np.zeros((srcvals.shape[0], 9))
+    for key in set(zip(iptype.tolist(), norders.tolist())):
+        _, um, _, _ = disc_exps(*key)
+        sel = np.nonzero((iptype == key[0]) & (norders == key[1]))[0]
+        np_ = um.shape[0]
+        idx = (ixyzs[sel] - 1)[:, None] + np.arange(np_)[None, :]
+        vals = srcvals[idx, :9]                     # (npatch, npols, 9)
+        srccoefs[idx] = np.einsum("lj,pjk->plk", um, vals)
+    return Surface(norders, ixyzs, iptype, srcvals, srccoefs)
+
+
+def read_go3(path) -> "Surface":
+    """.go3 triangle mesh (open_gov3_geometry, src/surface_routs/in_go3.f90:1):
+    order, number of patches, then x, y, z, dx/du, dy/du, dz/du, dx/dv, dy/dv,
+    dz/dv, nx, ny, nz, each as npts consecutive values; RV nodes."""
+    with open(path) as f:
+        norder = int(f.readline().split()[0])
+        npatches = int(f.readline().split()[0])
+        vals = np.array(f.read().split(), dtype=float)
+    npols = (norder + 1) * (norder + 2) // 2
+    npts = npatches * npols
+    if vals.size < 12 * npts:
+        raise ValueError(f"{path}: expected {12 * npts} values, found {vals.size}")
+    srcvals = np.ascontiguousarray(vals[: 12 * npts].reshape(12, npts).T)
+    return from_srcvals(np.full(npatches, norder, np.int64), np.ones(npatches, np.int64), srcvals)
+
+
+def write_go3(surf: "Surface", path) -> None:
+    """Write a single-order triangle surface in .go3 layout."""
+    if len(set(surf.norders.tolist())) != 1 or np.any(surf.iptype != 1):
+        raise ValueError(".go3 holds triangles of one order")
+    with open(path, "w") as f:
+        f.write(f"{int(surf.norders[0])}\n{surf.npatches}\n")
+        np.savetxt(f, surf.srcvals.T.reshape(-1), fmt="%.17g")
+
+
 def icosa_ellipsoid(nref: int, norder: int, axes=(1.0, 1.0, 1.0), center=(0.0, 0.0, 0.0)):
     """Icosahedron refined nref times, projected radially onto the ellipsoid
     center + axes * x/|x|, order-norder Vioreanu-Rokhlin nodes."""

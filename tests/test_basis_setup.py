@@ -156,3 +156,22 @@ def test_fmm_thresh(sphere4):
     t = S.get_fmm_thresh(sphere4.srcvals, sphere4.srcvals)
     x = sphere4.xyz
     assert t == 2.0 ** -51 * float(np.max(x.max(0) - x.min(0)))
+
+
+def test_go3_roundtrip(tmp_path, sphere4):
+    p = tmp_path / "s.go3"
+    S.write_go3(sphere4, p)
+    t = S.read_go3(p)
+    assert t.npatches == sphere4.npatches and t.npts == sphere4.npts
+    assert np.allclose(t.srcvals, sphere4.srcvals, atol=1e-15)
+    assert np.allclose(t.srccoefs, sphere4.srccoefs, atol=1e-13)
+
+
+def test_reference_go3_mesh_if_present(built):
+    import os
+    path = "/root/reference/geometries/sphere_192_o03.go3"
+    if not os.path.exists(path):
+        pytest.skip("reference geometry not present")
+    s = S.read_go3(path)
+    assert s.npatches == 192 and s.npts == 1920
+    assert abs(s.qwts().sum() - 4 * np.pi) < 1e-3
