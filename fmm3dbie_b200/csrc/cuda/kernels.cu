@@ -267,10 +267,11 @@ __global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
   using R2 = typename Vec<R>::T2;
   using R4 = typename Vec<R>::T4;
   constexpr int C = (KIND == 1) ? 2 : 1;  // reals per complex value
+  static_assert(MD % 2 == 0, "densities are read from shared memory two at a time");
   __shared__ R4 sg0[TILE];
   __shared__ R2 sg1[TILE];
-  __shared__ R sab[TILE * 2 * C];
-  __shared__ R ssig[TILE * MD * C];
+  __shared__ __align__(16) R sab[TILE * 2 * C];
+  __shared__ __align__(16) R ssig[TILE * MD * C];
   const int64_t ntarg = g.ntarg, nptso = g.nptso;
   const int64_t tbase = int64_t(blockIdx.x) * NT * TPT;
   const int m0 = blockIdx.z * MD;
@@ -332,12 +333,14 @@ __global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
         for (int t = 0; t < TPT; ++t) {
           R kr_ = R(0), ki_ = R(0);
           pair_helm(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, kr_, ki_);
-          const R2* sv = reinterpret_cast<const R2*>(ssig) + j * MD;
+          const R4* sv = reinterpret_cast<const R4*>(ssig) + j * (MD / 2);
 #pragma unroll
-          for (int m = 0; m < MD; ++m) {
-            const R2 x = sv[m];
-            tr[t][m][0] = fma(kr_, x.x, fma(-ki_, x.y, tr[t][m][0]));
-            tr[t][m][1] = fma(kr_, x.y, fma(ki_, x.x, tr[t][m][1]));
+          for (int m2 = 0; m2 < MD / 2; ++m2) {
+            const R4 x = sv[m2];  // densities 2*m2 and 2*m2+1
+            tr[t][2 * m2][0] = fma(kr_, x.x, fma(-ki_, x.y, tr[t][2 * m2][0]));
+            tr[t][2 * m2][1] = fma(kr_, x.y, fma(ki_, x.x, tr[t][2 * m2][1]));
+            tr[t][2 * m2 + 1][0] = fma(kr_, x.z, fma(-ki_, x.w, tr[t][2 * m2 + 1][0]));
+            tr[t][2 * m2 + 1][1] = fma(kr_, x.w, fma(ki_, x.z, tr[t][2 * m2 + 1][1]));
           }
         }
       } else {

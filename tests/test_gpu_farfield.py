@@ -61,8 +61,10 @@ def torch():
     return torch
 
 
-@pytest.mark.parametrize("kind,zk", [(0, 0j), (1, 2.5 + 0j), (1, 1.5 + 0.3j)])
+@pytest.mark.parametrize("kind,zk", [(0, 0j), (1, 2.5 + 0j), (1, 1.5 + 0.3j), (1, 40.0 + 0j)])
 def test_farfield_matches_direct_sum(torch, kind, zk):
+    """zk = 40 puts k r up to ~200 (many quadrants of the FP64 sine/cosine
+    reduction); the FP32 bound there reflects the phase error k r 2^-24."""
     src, nrm, ch, dp, targ = problem(1)
     thresh = 1e-14
     ref = direct(kind, zk, src, nrm, ch if kind else ch.real, dp if kind else dp.real, targ, thresh)
@@ -70,4 +72,5 @@ def test_farfield_matches_direct_sum(torch, kind, zk):
     got32 = run(torch, kind, zk, src, nrm, ch, dp, targ, thresh, 1)
     scale = np.max(np.abs(ref))
     assert np.max(np.abs(got64 - ref)) < 1e-12 * scale
-    assert np.max(np.abs(got32 - ref)) < 2e-5 * scale
+    tol32 = 2e-5 if abs(zk) < 10 else 2e-4
+    assert np.max(np.abs(got32 - ref)) < tol32 * scale
