@@ -263,6 +263,8 @@ def main():
     ap.add_argument("--clock-sampler", default="nvml", choices=["nvml", "smi"])
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the config-3 batched (64 right-hand sides) leg")
+    ap.add_argument("--uneven", action="store_true",
+                    help="add the config-4 uneven batch leg (32 surfaces; ~2 min of CPU setup)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -400,6 +402,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_batched:
         P.close()
         batched = batched_leg(dev)
+    uneven = None
+    if rank == 0 and world == 1 and args.uneven:
+        P.close()
+        uneven = uneven_leg(dev)
 
     if rank == 0:
         line = {
@@ -436,6 +442,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": base,
             "batched": batched,
+            "uneven": uneven,
         }
         print(json.dumps(line), flush=True)
     P.close()
@@ -494,6 +501,36 @@ def batched_leg(dev, steps=1):
                     "max_niter": int(np.max(info["niter"])), "max_rel_err": relerr(x)}
     out["speedup_vs_fp64"] = out["fp64"]["ms_per_batch"] / out["mixed"]["ms_per_batch"]
     P.close()
+    return out
+
+
+def uneven_leg(dev, kinds=(0, 1)):
+    """Config 4: 32 ellipsoids (semi-axes U(0.5,3), 80/320/1280 patches,
+    orders {4,6,8}, zk U(1,6)), 4 interior point sources each, Laplace and
+    Helmholtz batches.  Every surface solves its 4 systems as one
+    multi-density batch on its own stream; all surfaces run concurrently.
+    Reports systems solved per second for the mixed and FP64 paths and for
+    the mixed path run surface after surface."""
+    import torch
+    from fmm3dbie_b200.batch import SurfaceBatch, uneven_ellipsoids
+    out = {"workload": "config 4: 32 ellipsoids, npts 1200-57600, 4 point-source rhs each"}
+    for kind in kinds:
+        t0 = time.time()
+        items, rhs, _ = uneven_ellipsoids(kind)
+        B = SurfaceBatch(items, EPS)
+        t_setup = time.time() - t0
+        R = [torch.tensor(np.ascontiguousarray(r), device=dev) for r in rhs]
+        nsys = sum(r.shape[1] for r in rhs)
+        res = {"setup_s": round(t_setup, 1), "npts_total": int(sum(it.surf.npts for it in items)),
+               "systems": nsys}
+        for mode, tag, conc in ((1, "mixed", True), (0, "fp64", True), (1, "mixed_sequential", False)):
+            B.solve(R, mode=mode, eps_gmres=TOL_RES, concurrent=conc)  # warm-up / tuning
+            _, infos, ms = B.solve(R, mode=mode, eps_gmres=TOL_RES, concurrent=conc)
+            res[tag] = {"solves_per_s": nsys * 1000.0 / ms, "ms": ms,
+                        "max_rres": float(max(np.max(i["rres"]) for i in infos))}
+        res["speedup_vs_fp64"] = res["fp64"]["ms"] / res["mixed"]["ms"]
+        out["laplace" if kind == 0 else "helmholtz"] = res
+        B.close()
     return out
 
 

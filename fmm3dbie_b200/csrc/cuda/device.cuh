@@ -104,9 +104,9 @@ int far_nchunks(int64_t ntarg, int64_t nptso, int kind, int precision, int nd, i
 // chunks that fills `waves` waves of resident blocks.
 // md = 1 selects the multi-density kernel's shapes (nd > 1).
 int far_variants();
-int far_block_targets(int precision, int variant, int md = 0);
-int far_md_group(int variant);
-int far_blocks_per_sm(const KParams& kp, int precision, int variant, int md = 0);
+int far_block_targets(int precision, int variant, int md = 0, int nd = 1);
+int far_md_group(int variant, int nd);
+int far_blocks_per_sm(const KParams& kp, int precision, int variant, int md = 0, int nd = 1);
 int far_chunks_for_waves(int64_t ntarg, int64_t nptso, int precision, int variant, int nd,
                          int num_sms, int blocks_per_sm, double waves, int md = 0);
 // Multi-density far field: a.strengths holds sigma_over[s][nd] (far

@@ -962,13 +962,20 @@ cudaError_t far_variant(int v, const Geometry& g, const KParams& kp, const Matve
   }
 }
 
-// multi-density variants: (threads, targets per thread, densities per block)
-constexpr int kMdShapes[3][3] = {{128, 1, 16}, {128, 2, 8}, {64, 2, 16}};
+// multi-density shapes (threads, targets per thread, densities per block):
+// one class per density-group size, chosen by nd (<= 4, <= 8, more), and
+// three block shapes per class for the autotuner.
+constexpr int kMdShapes[3][3][3] = {
+    {{128, 1, 4}, {128, 2, 4}, {256, 1, 4}},
+    {{128, 1, 8}, {128, 2, 8}, {64, 2, 8}},
+    {{128, 1, 16}, {64, 1, 16}, {256, 1, 16}}};
 
-template <int KIND, typename R, bool CK, int V>
+inline int md_class(int nd) { return nd <= 4 ? 0 : (nd <= 8 ? 1 : 2); }
+
+template <int KIND, typename R, bool CK, int CL, int V>
 cudaError_t far_md_dispatch(const Geometry& g, const KParams& kp, const MatvecArgs& a,
                             cudaStream_t st, int* occ) {
-  constexpr int NT = kMdShapes[V][0], TPT = kMdShapes[V][1], MD = kMdShapes[V][2];
+  constexpr int NT = kMdShapes[CL][V][0], TPT = kMdShapes[CL][V][1], MD = kMdShapes[CL][V][2];
   if (occ) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         occ, far_md_kernel<KIND, R, NT, TPT, MD, kFarTile, CK>, NT, 0);
@@ -986,16 +993,29 @@ cudaError_t far_md_dispatch(const Geometry& g, const KParams& kp, const MatvecAr
   return cudaGetLastError();
 }
 
+template <int KIND, typename R, bool CK, int CL>
+cudaError_t far_md_class(int v, const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                         cudaStream_t st, int* occ) {
+  switch (v) {
+    case 1:
+      return far_md_dispatch<KIND, R, CK, CL, 1>(g, kp, a, st, occ);
+    case 2:
+      return far_md_dispatch<KIND, R, CK, CL, 2>(g, kp, a, st, occ);
+    default:
+      return far_md_dispatch<KIND, R, CK, CL, 0>(g, kp, a, st, occ);
+  }
+}
+
 template <int KIND, typename R, bool CK>
 cudaError_t far_md_variant(int v, const Geometry& g, const KParams& kp, const MatvecArgs& a,
                            cudaStream_t st, int* occ) {
-  switch (v) {
+  switch (md_class(a.nd)) {
+    case 0:
+      return far_md_class<KIND, R, CK, 0>(v, g, kp, a, st, occ);
     case 1:
-      return far_md_dispatch<KIND, R, CK, 1>(g, kp, a, st, occ);
-    case 2:
-      return far_md_dispatch<KIND, R, CK, 2>(g, kp, a, st, occ);
+      return far_md_class<KIND, R, CK, 1>(v, g, kp, a, st, occ);
     default:
-      return far_md_dispatch<KIND, R, CK, 0>(g, kp, a, st, occ);
+      return far_md_class<KIND, R, CK, 2>(v, g, kp, a, st, occ);
   }
 }
 
@@ -1093,19 +1113,22 @@ cudaError_t launch_source_consts(const Geometry& g, const KParams& kp, int preci
 
 int far_variants() { return 3; }
 
-int far_block_targets(int precision, int variant, int md) {
+int far_block_targets(int precision, int variant, int md, int nd) {
   const int v = variant < 0 || variant > 2 ? 0 : variant;
-  if (md) return kMdShapes[v][0] * kMdShapes[v][1];
+  if (md) return kMdShapes[md_class(nd)][v][0] * kMdShapes[md_class(nd)][v][1];
   return precision == 1 ? kF32Shapes[v][0] * kF32Shapes[v][1]
                         : kF64Shapes[v][0] * kF64Shapes[v][1];
 }
 
-int far_md_group(int variant) { return kMdShapes[variant < 0 || variant > 2 ? 0 : variant][2]; }
+int far_md_group(int variant, int nd) {
+  return kMdShapes[md_class(nd)][variant < 0 || variant > 2 ? 0 : variant][2];
+}
 
-int far_blocks_per_sm(const KParams& kp, int precision, int variant, int md) {
+int far_blocks_per_sm(const KParams& kp, int precision, int variant, int md, int nd) {
   MatvecArgs a;
   a.precision = precision;
   a.far_variant = variant;
+  a.nd = nd;
   Geometry g;
   int occ = 0;
   if (md)
@@ -1117,9 +1140,9 @@ int far_blocks_per_sm(const KParams& kp, int precision, int variant, int md) {
 
 int far_chunks_for_waves(int64_t ntarg, int64_t nptso, int precision, int variant, int nd,
                          int num_sms, int blocks_per_sm, double waves, int md) {
-  const int64_t bt = far_block_targets(precision, variant, md);
+  const int64_t bt = far_block_targets(precision, variant, md, nd);
   const int64_t tblocks = (ntarg + bt - 1) / bt;
-  const int64_t zdim = md ? (nd + far_md_group(variant) - 1) / far_md_group(variant) : nd;
+  const int64_t zdim = md ? (nd + far_md_group(variant, nd) - 1) / far_md_group(variant, nd) : nd;
   const double slots = double(num_sms) * std::max(blocks_per_sm, 1) * waves;
   int64_t s = std::max<int64_t>(1, int64_t(slots / double(tblocks * zdim) + 0.5));
   s = std::min<int64_t>(s, std::max<int64_t>(1, (nptso + kFarTile - 1) / kFarTile));

@@ -264,7 +264,7 @@ Plan::FarConfig Plan::far_config(int precision, int nd) const {
   FarConfig c;
   const int md = nd > 1;
   c.variant = std::min(std::max(env_int("BIE_FAR_VARIANT", 0), 0), dev::far_variants() - 1);
-  const int bps = dev::far_blocks_per_sm(kp, precision, c.variant, md);
+  const int bps = dev::far_blocks_per_sm(kp, precision, c.variant, md, nd);
   c.nchunks = dev::far_chunks_for_waves(ntarg, nptso, precision, c.variant, nd, num_sms, bps,
                                         env_double("BIE_FAR_WAVES", md ? 2.0 : 4.0), md);
   return c;
@@ -299,7 +299,7 @@ int Plan::tune_far(int precision, int nd, dev::MatvecArgs& a, cudaStream_t st, F
     std::vector<FarConfig> cand;
     const int md = nd > 1;
     for (int v = 0; v < dev::far_variants(); ++v) {
-      const int bps = dev::far_blocks_per_sm(kp, precision, v, md);
+      const int bps = dev::far_blocks_per_sm(kp, precision, v, md, nd);
       if (bps <= 0) continue;
       for (double waves : {1.0, 2.0, 4.0, 8.0}) {
         FarConfig c;
@@ -592,7 +592,12 @@ int solve_mixed(Plan& P, int nd, cdouble zid, const double* d_rhs, const double*
   const int64_t npts = P.npts, n = npts * nd;
   const int64_t ldv = n * (cplx ? 2 : 1);
   const int nblk = std::min<int>(2 * P.num_sms, int((npts + 63) / 64) + 1);
-  DBuf<double> r, d, tmp, partial, nrm;
+  // buffers live in the plan: after the first solve no call allocates (a
+  // cudaFree would synchronise the device and serialise concurrent solves)
+  DBuf<double>& r = P.mws.r;
+  DBuf<double>& d = P.mws.d;
+  DBuf<double>& partial = P.mws.partial;
+  DBuf<double>& nrm = P.mws.nrm;
   BIE_CUDA(r.alloc(ldv));
   BIE_CUDA(d.alloc(ldv));
   BIE_CUDA(partial.alloc(size_t(2) * nd * nblk));

@@ -90,6 +90,10 @@ struct GmresWorkspace {
   DBuf<double> V, w, partial, dots, coef, scale;
 };
 
+struct MixedWorkspace {
+  DBuf<double> r, d, partial, nrm;
+};
+
 // Per-precision stage totals (index 0 = f64 matvecs, 1 = f32 matvecs).
 struct StageTimes {
   double strengths_ms[2] = {0, 0}, far_ms[2] = {0, 0}, combine_ms[2] = {0, 0};
@@ -125,6 +129,7 @@ class Plan {
   const double* d_wts() const { return wts_.p; }
 
   GmresWorkspace gws;  // reused across solves on this plan
+  MixedWorkspace mws;
 
   // per-stage timing with CUDA events on the launch stream (off by default)
   bool timing = false;
