@@ -107,6 +107,17 @@ _SIGS = {
     "bie_farfield_dev": (C.c_int, [I64, PDBL, I64, VP, VP, VP, VP, I64, VP, DBL, I64, VP, VP]),
     "bie_farfield_dev_noalloc": (C.c_int, [I64, PDBL, I64, VP, VP, VP, VP, I64, VP, DBL, I64, VP,
                                            VP]),
+    "bie_mlp_create": (C.c_int, [I64, C.POINTER(VP)]),
+    "bie_mlp_destroy": (C.c_int, [VP]),
+    "bie_mlp_info": (C.c_int, [VP, PI64]),
+    "bie_mlp_set_params": (C.c_int, [VP, VP, VP]),
+    "bie_mlp_get_params": (C.c_int, [VP, VP, VP]),
+    "bie_mlp_forward": (C.c_int, [VP, VP, I64, VP, VP]),
+    "bie_mlp_grad": (C.c_int, [VP, VP, VP, I64, VP, VP, VP]),
+    "bie_mlp_train_step": (C.c_int, [VP, VP, VP, I64, DBL, VP, VP]),
+    "bie_mlp_gather": (C.c_int, [VP, I64, VP, I64, VP, PDBL, C.c_uint64, I64, VP, VP, VP]),
+    "bie_mlp_demodulate": (C.c_int, [VP, I64, VP, I64, VP, VP, VP]),
+    "bie_mlp_predict_density": (C.c_int, [VP, VP, I64, VP, I64, PDBL, VP, VP]),
     "bie_launch_count": (I64, []),
     "bie_measure_fp32_peak": (C.c_int, [PDBL, PDBL]),
 }

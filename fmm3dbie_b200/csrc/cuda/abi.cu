@@ -877,6 +877,8 @@ int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
       if (errs) {
         errs[0] = mo.fp64_matvecs;
         errs[1] = mo.fp32_matvecs;
+        if (x0_dev && (numit + 1) * nd >= 2 + nd)
+          for (int64_t q = 0; q < nd; ++q) errs[2 + q] = double(mo.x0_dropped[q]);
       }
     }
     return s;

@@ -143,6 +143,8 @@ cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, d
 
 // Number of kernels this library has launched in the process.
 int64_t launch_count();
+// Adds n launches made by kernels defined outside kernels.cu to that count.
+void note_launches(int64_t n);
 // FFMA throughput probe (flops = blocks*threads*iters*16*8*2).
 cudaError_t launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st);
 

@@ -1317,6 +1317,7 @@ cudaError_t launch_ffma_peak(float* out, int blocks, int threads, int iters, cud
 }
 
 int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void note_launches(int64_t n) { count(n); }
 
 }  // namespace dev
 }  // namespace bie

@@ -459,11 +459,21 @@ int gmres(Plan& P, int precision, int rres_precision, int nd, cdouble zid, const
   std::vector<double> hbuf(2 * (numit + 1) * nd * 2 + 2 * nd);
   BIE_CUDA(cudaMemcpyAsync(hbuf.data(), d_nrm, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
   BIE_CUDA(cudaStreamSynchronize(st));
-  std::vector<double> rb(nd);
+  std::vector<double> rb(nd), bnorm(nd);
   std::vector<double> hscale(2 * nd, 0.0);
   for (int d = 0; d < nd; ++d) {
     rb[d] = std::sqrt(std::max(hbuf[2 * d], 0.0));
     hscale[2 * d] = rb[d] > 0 ? 1.0 / rb[d] : 0.0;
+    bnorm[d] = rb[d];
+  }
+  // With an initial guess the stopping test stays relative to ||rhs||_w, so a
+  // warm-started solve meets the same accuracy as one from zero.
+  if (d_x0) {
+    BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, npts, nd, cplx, ws.partial.p, nblk, d_nrm, st));
+    std::vector<double> hb(2 * nd);
+    BIE_CUDA(cudaMemcpyAsync(hb.data(), d_nrm, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    for (int d = 0; d < nd; ++d) bnorm[d] = std::sqrt(std::max(hb[2 * d], 0.0));
   }
   BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nd * sizeof(double), cudaMemcpyHostToDevice, st));
   BIE_CUDA(dev::launch_dscale(V, V, ws.scale.p, n, nd, cplx, st));
@@ -523,7 +533,7 @@ int gmres(Plan& P, int precision, int rres_precision, int nd, cdouble zid, const
       Hc(d, it, it) = c[it] * Hc(d, it, it) + std::conj(s[it]) * wnrm;
       svd[it + 1] = -s[it] * svd[it];
       svd[it] = c[it] * svd[it];
-      const double err = std::abs(svd[it + 1]) / rb[d];
+      const double err = bnorm[d] > 0 ? std::abs(svd[it + 1]) / bnorm[d] : 0.0;
       out.errs[size_t(d) * (M + 1) + it] = err;
       if (!(err == err) || !(wnrm == wnrm)) {
         out.status = kBreakdown;
@@ -612,20 +622,53 @@ int solve_mixed(Plan& P, int nd, cdouble zid, const double* d_rhs, const double*
   std::vector<double> hb(2 * nd), hr(2 * nd);
   BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, npts, nd, cplx, partial.p, nblk, nrm.p, st));
   BIE_CUDA(cudaMemcpyAsync(hb.data(), nrm.p, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-  // x = x0 or 0; r = rhs - (zid x + K x)
+  // x = x0 or 0; r = rhs - (zid x + K x).  The residual of a guess is taken
+  // with the FP32 operator: it only seeds the first correction, and every
+  // convergence decision below is made on an FP64 residual.
+  bool r_is_f64 = true;
+  std::vector<double> bn(nd);
   if (d_x0) {
     BIE_CUDA(cudaMemcpyAsync(d_soln, d_x0, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    int ier = P.matvec(0, nd, d_soln, r.p, st);
+    int ier = P.matvec(1, nd, d_soln, r.p, st);
     if (ier) return ier;
-    ++out.fp64_matvecs;
+    ++out.fp32_matvecs;
     BIE_CUDA(dev::launch_axpby(d_soln, r.p, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
     BIE_CUDA(dev::launch_axpby(d_rhs, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    r_is_f64 = false;
+    // fallback per system: a guess whose residual is not below ||rhs|| is
+    // replaced by zero (x = 0, r = rhs)
+    BIE_CUDA(dev::launch_mdot(r.p, ldv, 1, r.p, wts, npts, nd, cplx, partial.p, nblk, nrm.p, st));
+    BIE_CUDA(cudaMemcpyAsync(hr.data(), nrm.p, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    std::vector<double> keep(2 * nd, 0.0), drop(2 * nd, 0.0);
+    bool any_drop = false;
+    out.x0_dropped.assign(nd, 0);
+    for (int q = 0; q < nd; ++q) {
+      const double b = std::sqrt(std::max(hb[2 * q], 0.0));
+      const double rr = std::sqrt(std::max(hr[2 * q], 0.0));
+      const bool ok = rr < b;
+      keep[2 * q] = ok ? 1.0 : 0.0;
+      drop[2 * q] = ok ? 0.0 : 1.0;
+      if (!ok) {
+        any_drop = true;
+        out.x0_dropped[q] = 1;
+      }
+    }
+    if (any_drop) {
+      double* s = nrm.p + 2 * nd;
+      BIE_CUDA(cudaMemcpyAsync(s, keep.data(), 2 * nd * sizeof(double), cudaMemcpyHostToDevice, st));
+      BIE_CUDA(dev::launch_dscale(d_soln, d_soln, s, n, nd, cplx, st));
+      BIE_CUDA(dev::launch_dscale(r.p, r.p, s, n, nd, cplx, st));
+      BIE_CUDA(cudaStreamSynchronize(st));
+      BIE_CUDA(cudaMemcpyAsync(s, drop.data(), 2 * nd * sizeof(double), cudaMemcpyHostToDevice, st));
+      BIE_CUDA(dev::launch_dscale(d_rhs, d.p, s, n, nd, cplx, st));
+      BIE_CUDA(dev::launch_axpby(d.p, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    }
   } else {
     BIE_CUDA(cudaMemsetAsync(d_soln, 0, ldv * sizeof(double), st));
     BIE_CUDA(cudaMemcpyAsync(r.p, d_rhs, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
   }
   BIE_CUDA(cudaStreamSynchronize(st));
-  std::vector<double> bn(nd);
   for (int q = 0; q < nd; ++q) bn[q] = std::sqrt(std::max(hb[2 * q], 0.0));
   for (int outer = 0; outer <= max_outer; ++outer) {
     BIE_CUDA(dev::launch_mdot(r.p, ldv, 1, r.p, wts, npts, nd, cplx, partial.p, nblk, nrm.p, st));
@@ -641,7 +684,17 @@ int solve_mixed(Plan& P, int nd, cdouble zid, const double* d_rhs, const double*
         worst_ratio = std::max(worst_ratio, eps_target / rel);
       }
     }
-    if (all_done || outer == max_outer) {
+    if (!r_is_f64 && all_done) {
+      // the guess already meets the target in FP32: confirm it in FP64
+      int ier = P.matvec(0, nd, d_soln, r.p, st);
+      if (ier) return ier;
+      ++out.fp64_matvecs;
+      BIE_CUDA(dev::launch_axpby(d_soln, r.p, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
+      BIE_CUDA(dev::launch_axpby(d_rhs, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+      r_is_f64 = true;
+      continue;
+    }
+    if (r_is_f64 && (all_done || outer == max_outer)) {
       if (!all_done) out.status = kNotConverged;
       break;
     }
@@ -665,6 +718,7 @@ int solve_mixed(Plan& P, int nd, cdouble zid, const double* d_rhs, const double*
     ++out.fp64_matvecs;
     BIE_CUDA(dev::launch_axpby(d_soln, r.p, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
     BIE_CUDA(dev::launch_axpby(d_rhs, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    r_is_f64 = true;
   }
   return out.status;
 }

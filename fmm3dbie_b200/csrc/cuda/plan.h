@@ -175,6 +175,7 @@ struct MixedOut {
   std::vector<int64_t> inner_iters;  // total inner GMRES iterations per system
   std::vector<double> rres;          // final FP64 relative residual per system
   std::vector<int64_t> outer;        // refinement steps per system
+  std::vector<int64_t> x0_dropped;   // 1 where the initial guess was replaced by 0
   int fp64_matvecs = 0, fp32_matvecs = 0;
   int status = kOk;
 };

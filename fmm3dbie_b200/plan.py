@@ -109,7 +109,10 @@ class Plan:
         """Solve (zid I + K) x = rhs; rhs (npts,) or (npts, nd) independent systems.
 
         mode 0: FP64 GMRES (the reference method); 1: FP32-matvec GMRES inside
-        FP64 iterative refinement.  Returns (x, info dict)."""
+        FP64 iterative refinement.  x0: initial guess; the stopping test stays
+        relative to ||rhs||, and in mode 1 a guess whose residual is not
+        below ||rhs|| is replaced by zero (info["x0_dropped"]).  Returns (x,
+        info dict)."""
         torch = self.torch
         nd = 1 if rhs.dim() == 1 else rhs.shape[1]
         self._check(rhs, self.npts, nd)
@@ -133,6 +136,8 @@ class Plan:
         else:
             info["fp64_matvecs"] = int(errs[0])
             info["fp32_matvecs"] = int(errs[1])
+            if x0 is not None:
+                info["x0_dropped"] = errs[2:2 + nd].astype(bool)
         return out, info
 
     def timing(self, enable: bool | None = None):

@@ -281,9 +281,14 @@ int bie_plan_matvec(void* plan, int64_t iprec, int64_t nd, const double* sigma_d
                     double* pot_dev, void* stream);
 /* GMRES on (zid I + K) x = rhs, nd independent systems (point-major).
  * mode 0: FP64 GMRES (reference method); 1: mixed precision refinement.
- * x0_dev may be NULL. niter(nd), rres(nd), errs or NULL: mode 0 fills
- * errs((numit+1)*nd) with the residual history, mode 1 fills errs[0] =
- * number of FP64 matvecs, errs[1] = number of FP32 matvecs. */
+ * x0_dev (initial guess) may be NULL; with a guess the stopping test stays
+ * relative to ||rhs||_w, and mode 1 takes the guess's residual with the
+ * FP32 operator and replaces, per system, a guess whose residual is not
+ * below ||rhs||_w by zero.  niter(nd), rres(nd), errs or NULL: mode 0 fills
+ * errs((numit+1)*nd) with the residual history (relative to ||rhs||_w),
+ * mode 1 fills errs[0] = number of FP64 matvecs, errs[1] = number of FP32
+ * matvecs and, with a guess, errs[2+q] = 1 where system q's guess was
+ * replaced by zero. */
 int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
                    const double* rhs_dev, const double* x0_dev, int64_t numit, double eps_gmres,
                    double* soln_dev, int64_t* niter, double* errs, double* rres, void* stream);
@@ -323,6 +328,55 @@ int bie_farfield_dev_noalloc(int64_t kind, const double* zk, int64_t ns, const d
                              const double* nrm_dev, const double* charge_dev,
                              const double* dipstr_dev, int64_t nt, const double* targ_dev,
                              double thresh, int64_t iprec, double* pot_dev, void* stream);
+
+/* ---- learned warm start (no reference counterpart) ----------------------
+ * The reference solvers always start GMRES from zero
+ * (helm_comb_dir_solver_guru, helm_comb_dir.f:2071, calls zgmres_guru at
+ * helm_comb_dir.f:2222; gmres_routs.f90:13).  These entry points train and run a per-node MLP
+ * that predicts the density of the plane-wave problem
+ * (zid I + K) sigma = -exp(i k d.x); the prediction is passed as x0 to
+ * bie_plan_solve.  Network 10 -> 256 -> 256 -> 256 -> 256 -> 2 (tanh),
+ * bf16 weights, fp32 accumulation, fp32 master weights, Adam.  Inputs per
+ * row: d (3), (k - kc)/ks, x/xs (3), unit normal (3); output: the
+ * demodulated density tau = sigma exp(-i k d.x) (re, im).
+ * params: 200,706 floats: W0[256][10], W1..W3[256][256], W4[2][256], then
+ * b0..b3[256], b4[2].  dirk: per solve (dx, dy, dz, k).  norm: (xs, kc, ks).
+ * srcvals_dev: the surface's srcvals (12 x npts, reference layout) on the
+ * device.  All pointers are device pointers; calls are asynchronous on
+ * `stream`. */
+/* Allocates the network (zero parameters) and its workspace for batches
+ * of up to max_rows rows. */
+int bie_mlp_create(int64_t max_rows, void** mlp);
+int bie_mlp_destroy(void* mlp);
+/* info[8]: nparams, max_rows, inputs, width, hidden layers, outputs, Adam
+ * steps taken, number of weight (non-bias) parameters. */
+int bie_mlp_info(void* mlp, int64_t* info);
+/* Sets the fp32 parameters (and their bf16 copy) and resets Adam. */
+int bie_mlp_set_params(void* mlp, const float* params_dev, void* stream);
+int bie_mlp_get_params(void* mlp, float* params_dev, void* stream);
+/* y[m][2] = MLP(x[m][10]), 1 <= m <= max_rows. */
+int bie_mlp_forward(void* mlp, const float* x_dev, int64_t m, float* y_dev, void* stream);
+/* Gradient of mean_r |MLP(x_r) - t_r|^2 into grad_dev[nparams] (may be NULL)
+ * and the loss into loss_dev[0] (may be NULL). */
+int bie_mlp_grad(void* mlp, const float* x_dev, const float* t_dev, int64_t m, float* grad_dev,
+                 float* loss_dev, void* stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on that loss. */
+int bie_mlp_train_step(void* mlp, const float* x_dev, const float* t_dev, int64_t m, double lr,
+                       float* loss_dev, void* stream);
+/* m training rows drawn from nsolves solves: row r takes sample
+ * hash(seed, r) mod (nsolves * npts); tau_dev[(j*npts + i)] complex fp32. */
+int bie_mlp_gather(const double* srcvals_dev, int64_t npts, const double* dirk_dev,
+                   int64_t nsolves, const float* tau_dev, const double* norm, uint64_t seed,
+                   int64_t m, float* x_dev, float* t_dev, void* stream);
+/* tau[(q*npts + i)] = sigma[(i*nd + q)] exp(-i k_q d_q.x_i) (complex fp32 out,
+ * complex128 point-major in). */
+int bie_mlp_demodulate(const double* srcvals_dev, int64_t npts, const double* dirk_dev,
+                       int64_t nd, const double* sigma_dev, float* tau_dev, void* stream);
+/* x0[(i*nd + q)] = tau_hat(d_q, k_q, x_i, n_i) exp(i k_q d_q.x_i), complex128
+ * point-major: the initial guess for nd plane-wave systems. */
+int bie_mlp_predict_density(void* mlp, const double* srcvals_dev, int64_t npts,
+                            const double* dirk_dev, int64_t nd, const double* norm,
+                            double* x0_dev, void* stream);
 
 /* ---- measurement helpers (no reference counterpart) ---------------------- */
 /* Number of kernels this library has launched in the process. */
