@@ -49,7 +49,8 @@ ZPARS = (ZK, -1j * ZK, 1.0)
 EPS = 1e-7
 X0 = np.array([0.1, -0.2, 0.3])
 TOL_RES = 1e-7      # FP64 relative residual target of both timed paths
-FLOPS_PER_PAIR = {"helm": 26 + 16, "lap": 15 + 4}   # 1 density
+TOL_WARM = 3e-7     # residual target of the torus warm-start solves (error <= 1e-6)
+FLOPS_PER_PAIR = {"helm": 26 + 16, "lap": 15 + 4}   # 1 density: geometry + per-density MACs
 
 
 def flops_per_pair(kind: str, nd: int = 1) -> int:
@@ -262,9 +263,11 @@ def main():
     ap.add_argument("--nd", type=int, default=1, help="densities per matvec for --matvec-only")
     ap.add_argument("--clock-sampler", default="nvml", choices=["nvml", "smi"])
     ap.add_argument("--no-batched", action="store_true",
-                    help="skip the config-3 batched (64 right-hand sides) leg")
+                    help="skip the batched leg (64 plane-wave right-hand sides)")
+    ap.add_argument("--torus", action="store_true",
+                    help="also run the torus warm-start leg (trained warm start; ~1-2 min host setup)")
     ap.add_argument("--uneven", action="store_true",
-                    help="add the config-4 uneven batch leg (32 surfaces; ~2 min of CPU setup)")
+                    help="add the uneven batch leg (32 ellipsoids; ~2 min of CPU setup)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -406,6 +409,10 @@ def main():
     if rank == 0 and world == 1 and args.uneven:
         P.close()
         uneven = uneven_leg(dev)
+    torus = None
+    if rank == 0 and world == 1 and args.torus:
+        P.close()
+        torus = torus_leg(dev)
 
     if rank == 0:
         line = {
@@ -443,6 +450,7 @@ def main():
             "cpu_baseline": base,
             "batched": batched,
             "uneven": uneven,
+            "torus_warm_start": torus,
         }
         print(json.dumps(line), flush=True)
     P.close()
@@ -453,7 +461,7 @@ def main():
 
 
 def batched_leg(dev, steps=1):
-    """Config 3: 64 incident plane waves on the same (1,2,3) ellipsoid at
+    """64 incident plane waves on the same (1,2,3) ellipsoid at
     zk = 5, zpars = (5, -5i, 1); rhs = -incident field at the nodes.  All 64
     systems share every launch.  Reports solves/s (64 per batch) for the
     mixed-precision and the plain FP64 paths and their error against a
@@ -481,7 +489,7 @@ def batched_leg(dev, steps=1):
         den = torch.sum(w * xref.abs() ** 2, 0)
         return float(torch.max(torch.sqrt(num / den)))
 
-    out = {"workload": "config 3: 64 plane waves, ellipsoid (1,2,3), 1280 order-6 patches, "
+    out = {"workload": "64 plane waves, ellipsoid (1,2,3), 1280 order-6 patches, "
                        "zk=5, zpars=(5,-5i,1), eps=1e-7", "nrhs": 64, "setup_s": round(t_setup, 2),
            "nptso": P.nptso}
     for mode, tag in ((1, "mixed"), (0, "fp64")):
@@ -500,12 +508,113 @@ def batched_leg(dev, steps=1):
         out[tag] = {"solves_per_s": 64 * 1000.0 / t, "ms_per_batch": t,
                     "max_niter": int(np.max(info["niter"])), "max_rel_err": relerr(x)}
     out["speedup_vs_fp64"] = out["fp64"]["ms_per_batch"] / out["mixed"]["ms_per_batch"]
+    # the reference method proper: plain FP64 GMRES, one right-hand side at a time
+    P.solve(R[:, 0].contiguous(), 0.5, mode=0, numit=300, eps_gmres=TOL_RES)  # warm-up / tuning
+    torch.cuda.synchronize()
+    ts, its = [], []
+    for q in range(2):
+        r1 = R[:, q].contiguous()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        _, info = P.solve(r1, 0.5, mode=0, numit=300, eps_gmres=TOL_RES)
+        b.record()
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+        its.append(int(info["niter"][0]))
+    out["fp64_single"] = {"solves_per_s": 1000.0 / float(np.mean(ts)), "ms_per_solve": float(np.mean(ts)),
+                          "niter": its, "sample": "2 of the 64 systems, one at a time"}
+    out["speedup_vs_fp64_single"] = out["mixed"]["solves_per_s"] / out["fp64_single"]["solves_per_s"]
     P.close()
     return out
 
 
+WARMSTART_WEIGHTS = os.path.join(ROOT, "fmm3dbie_b200", "weights", "warmstart_torus.npz")
+
+
+def torus_leg(dev, nd=16, weights=WARMSTART_WEIGHTS):
+    """Plane-wave Helmholtz solves on the 64 x 32 quad torus
+    (73,728 nodes) at two of the training grid's wavenumbers, 16 held-out
+    directions each.  Times the plain FP64 GMRES path one right-hand side at
+    a time (the reference method), the mixed-precision path on the batch of
+    16 from zero, and the same from the trained network's guess."""
+    import torch
+    from fmm3dbie_b200.warmstart import (PlaneWaveProblem, WarmStartMLP, random_directions,
+                                         torus_surface)
+    if not os.path.exists(weights):
+        return {"skipped": f"no trained network at {os.path.relpath(weights, ROOT)}"}
+    z = np.load(weights)
+    meta = json.loads(str(z["meta"]))
+    ks_grid = meta["ks"]
+    ks = [ks_grid[len(ks_grid) // 4], ks_grid[(3 * len(ks_grid)) // 4]]
+    surf = torus_surface(*meta["surface"])
+    t0 = time.time()
+    prob = PlaneWaveProblem(surf, ks)
+    t_setup = time.time() - t0
+    mlp = WarmStartMLP.load(weights)
+    hold = np.random.default_rng(int(meta["seed"]) + 1000)
+    out = {"workload": "torus R=2, r=0.6+0.15cos3p, 64x32 quads, 6x6 nodes "
+                       f"(npts {surf.npts}), plane waves, zpars=(k,-ik,1), eps=1e-7, "
+                       f"{nd} held-out directions per k, tolerance {TOL_WARM:g}",
+           "setup_s": round(t_setup, 1), "network": meta, "per_k": []}
+    w = torch.tensor(surf.qwts(), device=dev)[:, None]
+    tot = {"mixed_zero": 0.0, "mixed_warm": 0.0, "fp64_single": 0.0}
+    n_single = 0
+    for k in ks:
+        dirs = random_directions(nd, hold)
+        dirk = PlaneWaveProblem.dirk(k, dirs)
+        xref, _ = prob.solve(k, dirs, mode=0, eps=1e-11)
+
+        def relerr(x):
+            return float(torch.max(torch.sqrt(torch.sum(w * (x - xref).abs() ** 2, 0) /
+                                              torch.sum(w * xref.abs() ** 2, 0))))
+
+        def timed(fn):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            r = fn()
+            b.record()
+            b.synchronize()
+            return r, a.elapsed_time(b)
+
+        prob.solve(k, dirs, mode=1, eps=TOL_WARM)  # warm-up (tunes the kernels)
+        (xz, iz), mz = timed(lambda: prob.solve(k, dirs, mode=1, eps=TOL_WARM))
+        (xw, iw), mw = timed(lambda: prob.solve(k, dirs, mode=1, eps=TOL_WARM,
+                                                x0=mlp.predict_density(prob.srcvals, dirk)))
+        x0 = mlp.predict_density(prob.srcvals, dirk)
+        prob.solve(k, dirs[:1], mode=0, eps=TOL_WARM)  # warm-up / tuning of the nd=1 FP64 path
+        pe = torch.sqrt(torch.sum(w * (x0 - xref).abs() ** 2, 0) / torch.sum(w * xref.abs() ** 2, 0))
+        (x1, i1), m1 = timed(lambda: prob.solve(k, dirs[:1], mode=0, eps=TOL_WARM))
+        tot["mixed_zero"] += mz
+        tot["mixed_warm"] += mw
+        tot["fp64_single"] += m1
+        n_single += 1
+        out["per_k"].append({
+            "k": k, "pred_err_median": float(torch.median(pe)),
+            "mixed_zero": {"ms": mz, "inner_iters_mean": float(iz["niter"].mean()),
+                           "fp64_matvecs": iz["fp64_matvecs"], "max_rel_err": relerr(xz),
+                           "max_rres": float(iz["rres"].max())},
+            "mixed_warm": {"ms": mw, "inner_iters_mean": float(iw["niter"].mean()),
+                           "fp64_matvecs": iw["fp64_matvecs"], "max_rel_err": relerr(xw),
+                           "max_rres": float(iw["rres"].max()),
+                           "x0_dropped": int(iw["x0_dropped"].sum())},
+            "fp64_single": {"ms_per_solve": m1, "niter": int(i1["niter"][0]),
+                            "rres": float(i1["rres"][0])}})
+    n = nd * len(ks)
+    out["solves_per_s"] = {"mixed_batched_warm": n * 1000.0 / tot["mixed_warm"],
+                           "mixed_batched_zero": n * 1000.0 / tot["mixed_zero"],
+                           "fp64_single": n_single * 1000.0 / tot["fp64_single"]}
+    sp = out["solves_per_s"]
+    out["speedup_vs_fp64_single"] = sp["mixed_batched_warm"] / sp["fp64_single"]
+    out["warm_gain"] = sp["mixed_batched_warm"] / sp["mixed_batched_zero"]
+    mlp.close()
+    prob.close()
+    return out
+
+
 def uneven_leg(dev, kinds=(0, 1)):
-    """Config 4: 32 ellipsoids (semi-axes U(0.5,3), 80/320/1280 patches,
+    """32 ellipsoids (semi-axes U(0.5,3), 80/320/1280 patches,
     orders {4,6,8}, zk U(1,6)), 4 interior point sources each, Laplace and
     Helmholtz batches.  Every surface solves its 4 systems as one
     multi-density batch on its own stream; all surfaces run concurrently.
@@ -513,7 +622,7 @@ def uneven_leg(dev, kinds=(0, 1)):
     the mixed path run surface after surface."""
     import torch
     from fmm3dbie_b200.batch import SurfaceBatch, uneven_ellipsoids
-    out = {"workload": "config 4: 32 ellipsoids, npts 1200-57600, 4 point-source rhs each"}
+    out = {"workload": "32 ellipsoids, npts 1200-57600, 4 point-source rhs each"}
     for kind in kinds:
         t0 = time.time()
         items, rhs, _ = uneven_ellipsoids(kind)

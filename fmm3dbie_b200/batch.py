@@ -89,7 +89,7 @@ class SurfaceBatch:
 
 
 def uneven_ellipsoids(kind: int, nsurf: int = 32, nrhs: int = 4, seed: int = 4):
-    """Config 4: ellipsoids with semi-axes U(0.5,3), 80/320/1280 patches,
+    """Uneven batch: 32 ellipsoids with semi-axes U(0.5,3), 80/320/1280 patches,
     orders {4,6,8}, zk U(1,6) (Helmholtz, zpars = (k, -ik, 1)) or alpha =
     beta = 1 (Laplace), and nrhs interior point sources inside 0.3 x the
     semi-axes.  Returns (items, rhs arrays, source points)."""

@@ -8,7 +8,8 @@
 //                   pclass[npatches] -> interpolation matrix of the class
 //                   (iptype, norder, nfar): imat[nf x np] f64 (row-major)
 //   near matrix   : row_ptr[ntarg+1] (into col/wofs), col[nnz] patch index,
-//                   wofs[nnz+1] entry offsets (iquad-1),
+//                   wofs[nnz+1] entry offsets (iquad-1), nps[nnz] first
+//                   node of each near patch,
 //                   W_eff[nquad] = wnear - smooth oversampled part, stored
 //                   f64 (and f32 for the mixed-precision path);
 //                   complex values are interleaved (re, im).
@@ -50,6 +51,7 @@ struct Near {
   const int64_t* row_ptr = nullptr;  // ntarg+1
   const int32_t* col = nullptr;      // nnz
   const int64_t* wofs = nullptr;     // nnz+1
+  const int32_t* nps = nullptr;      // nnz: first node of patch col[k] (pstart[col[k]])
 };
 
 // Kernel constants. kind 0: Laplace (real alpha, beta), 1: Helmholtz.

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <cmath>
 
 #include "device.cuh"
@@ -425,49 +426,133 @@ __global__ void source_consts_kernel(Geometry g, KParams kp, R* __restrict__ ab)
 // ---------------------------------------------------------------------------
 // (c) combine: far partials + near-correction SpMM, one warp per target row
 // ---------------------------------------------------------------------------
+template <typename W>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  using T = float2;
+};
+template <>
+struct Vec2<double> {
+  using T = double2;
+};
+
+constexpr int kCombineThreads = 256;  // 8 warps = 8 consecutive target rows per block
+constexpr int kCombineUnroll = 4;     // W_eff entries per lane in flight
+
+
 template <int CPLX, typename W>
-__global__ void combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
-                               const double* __restrict__ sigma, const double* __restrict__ partial,
-                               int nchunks, double* __restrict__ pot, int nd) {
+__global__ void __launch_bounds__(kCombineThreads)
+    combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
+                   const double* __restrict__ sigma, const double* __restrict__ partial,
+                   int nchunks, double* __restrict__ pot, int nd) {
   const int lane = threadIdx.x & 31;
   const int64_t i = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  if (i >= g.ntarg) return;
   const int64_t ntarg = g.ntarg;
-  const int64_t k0 = nr.row_ptr[i], k1 = nr.row_ptr[i + 1];
   if (nd == 1) {
-    double ar = 0, ai = 0;
-    for (int c = lane; c < nchunks; c += 32) {
-      const size_t o = size_t(c) * ntarg + i;
-      if (CPLX) {
-        ar += partial[2 * o];
-        ai += partial[2 * o + 1];
-      } else {
-        ar += partial[o];
-      }
-    }
-    // lanes are grouped per near patch: G lanes per patch, 32/G patches at once
-    for (int64_t kb = k0; kb < k1;) {
-      const int p0 = nr.col[kb];
-      const int npv = g.pstart[p0 + 1] - g.pstart[p0];
-      const int G = npv > 16 ? 32 : (npv > 8 ? 16 : 8);
-      const int per = 32 / G;
-      const int64_t k = kb + lane / G;
-      if (k < k1) {
-        const int p = nr.col[k];
-        const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
-        const int64_t wb = nr.wofs[k];
-        for (int mm = lane % G; mm < np; mm += G) {
+    __shared__ double sred[32][8][2];
+    // far-field partial sums of the block's 8 rows, read cooperatively: thread
+    // t takes row t % 8 of chunks t / 8, t / 8 + 32, ..., so every warp load
+    // covers four whole 8-row segments
+    {
+      const int r = threadIdx.x & 7, c0 = threadIdx.x >> 3;
+      const int64_t row = int64_t(blockIdx.x) * 8 + r;
+      double pr = 0, pi = 0;
+      if (row < ntarg)
+        for (int c = c0; c < nchunks; c += 32) {
+          const size_t o = size_t(c) * ntarg + row;
           if (CPLX) {
-            const double wr = double(weff[2 * (wb + mm)]), wi = double(weff[2 * (wb + mm) + 1]);
-            const double sr = sigma[2 * (ps + mm)], si = sigma[2 * (ps + mm) + 1];
-            ar = fma(wr, sr, fma(-wi, si, ar));
-            ai = fma(wr, si, fma(wi, sr, ai));
+            const double2 v = reinterpret_cast<const double2*>(partial)[o];
+            pr += v.x;
+            pi += v.y;
           } else {
-            ar = fma(double(weff[wb + mm]), sigma[ps + mm], ar);
+            pr += partial[o];
+          }
+        }
+      sred[c0][r][0] = pr;
+      sred[c0][r][1] = pi;
+    }
+    __syncthreads();
+    if (i >= ntarg) return;
+    const int64_t k0 = nr.row_ptr[i], k1 = nr.row_ptr[i + 1];
+    const int wrow = threadIdx.x >> 5;
+    double ar = sred[lane][wrow][0], ai = sred[lane][wrow][1];
+    // Near patches of the row, 32 at a time: one lane-parallel load of their
+    // first nodes and entry offsets (no dependent index loads), then the
+    // row's W_eff span (contiguous: wofs[k+1] = wofs[k] + np) streamed with
+    // coalesced loads, kCombineUnroll entries per lane in flight.
+    constexpr unsigned kFull = 0xffffffffu;
+    constexpr int kU = kCombineUnroll;
+    for (int64_t kc = k0; kc < k1; kc += 32) {
+      const int nkc = int(k1 - kc < 32 ? k1 - kc : 32);
+      int ps = 0, np = 0;
+      int64_t wb = 0;
+      if (lane < nkc) {
+        ps = nr.nps[kc + lane];
+        wb = nr.wofs[kc + lane];
+        np = int(nr.wofs[kc + lane + 1] - wb);
+      }
+      const int np0 = __shfl_sync(kFull, np, 0);
+      const int64_t e0 = __shfl_sync(kFull, wb, 0);
+      if (__all_sync(kFull, lane >= nkc || np == np0)) {
+        // every patch of this group has np0 nodes: entry e belongs to patch
+        // e / np0 (exact in FP32: the fraction stays >= 0.5/np0 from an integer)
+        const int ne = nkc * np0;
+        const float inv = 1.0f / float(np0);
+        for (int eb = 0; eb < ne; eb += 32 * kU) {
+          double wr[kU], wi[kU], sr[kU], si[kU];
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            const int e = eb + 32 * u + lane;
+            const bool ok = e < ne;
+            const int kk = ok ? int((float(e) + 0.5f) * inv) : 0;
+            const int psk = __shfl_sync(kFull, ps, kk);
+            wr[u] = wi[u] = sr[u] = si[u] = 0.0;
+            if (ok) {
+              const int node = psk + (e - kk * np0);
+              if (CPLX) {
+                const typename Vec2<W>::T wv =
+                    reinterpret_cast<const typename Vec2<W>::T*>(weff)[e0 + e];
+                const double2 sv = reinterpret_cast<const double2*>(sigma)[node];
+                wr[u] = double(wv.x);
+                wi[u] = double(wv.y);
+                sr[u] = sv.x;
+                si[u] = sv.y;
+              } else {
+                wr[u] = double(weff[e0 + e]);
+                sr[u] = sigma[node];
+              }
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            if (CPLX) {
+              ar = fma(wr[u], sr[u], fma(-wi[u], si[u], ar));
+              ai = fma(wr[u], si[u], fma(wi[u], sr[u], ai));
+            } else {
+              ar = fma(wr[u], sr[u], ar);
+            }
+          }
+        }
+      } else {
+        // mixed patch sizes: one patch of the group at a time
+        for (int j = 0; j < nkc; ++j) {
+          const int psj = __shfl_sync(kFull, ps, j);
+          const int npj = __shfl_sync(kFull, np, j);
+          const int64_t wbj = __shfl_sync(kFull, wb, j);
+          for (int mm = lane; mm < npj; mm += 32) {
+            if (CPLX) {
+              const double wr = double(weff[2 * (wbj + mm)]);
+              const double wi = double(weff[2 * (wbj + mm) + 1]);
+              const double sr = sigma[2 * (psj + mm)], si = sigma[2 * (psj + mm) + 1];
+              ar = fma(wr, sr, fma(-wi, si, ar));
+              ai = fma(wr, si, fma(wi, sr, ai));
+            } else {
+              ar = fma(double(weff[wbj + mm]), sigma[psj + mm], ar);
+            }
           }
         }
       }
-      kb += per;
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -485,6 +570,8 @@ __global__ void combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
     return;
   }
   // several densities per point: lanes run over densities
+  if (i >= ntarg) return;
+  const int64_t k0 = nr.row_ptr[i], k1 = nr.row_ptr[i + 1];
   for (int m = lane; m < nd; m += 32) {
     double ar = 0, ai = 0;
     for (int c = 0; c < nchunks; ++c) {
@@ -1155,7 +1242,7 @@ int far_chunks_for_waves(int64_t ntarg, int64_t nptso, int precision, int varian
 cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
                            const MatvecArgs& a, cudaStream_t st) {
   if (g.ntarg == 0) return cudaSuccess;
-  const int threads = 256;
+  const int threads = kCombineThreads;
   const int64_t blocks = (g.ntarg * 32 + threads - 1) / threads;
   const dim3 grid(static_cast<unsigned>(blocks)), block(threads);
   if (kp.kind == 1) {

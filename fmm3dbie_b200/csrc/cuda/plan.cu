@@ -142,10 +142,11 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
     hpc[p] = it->second;
   }
   std::vector<int64_t> hrp(ntarg + 1), hwo(nnz + 1);
-  std::vector<int32_t> hcol(nnz);
+  std::vector<int32_t> hcol(nnz), hnps(nnz);
   for (int64_t i = 0; i <= ntarg; ++i) hrp[i] = s.row_ptr[i] - 1;
   for (int64_t k = 0; k < nnz; ++k) {
     hcol[k] = int32_t(s.col_ind[k] - 1);
+    hnps[k] = hps[hcol[k]];
     hwo[k] = s.iquad[k] - 1;
   }
   hwo[nnz] = nquad;
@@ -189,6 +190,7 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   BIE_CUDA(upload(imat_, him, st));
   BIE_CUDA(upload(row_ptr_, hrp, st));
   BIE_CUDA(upload(col_, hcol, st));
+  BIE_CUDA(upload(nps_, hnps, st));
   BIE_CUDA(upload(wofs_, hwo, st));
   BIE_CUDA(upload(wts_, hqw, st));
   g.ntarg = ntarg;
@@ -216,6 +218,7 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   nr.nquad = nquad;
   nr.row_ptr = row_ptr_.p;
   nr.col = col_.p;
+  nr.nps = nps_.p;
   nr.wofs = wofs_.p;
   // ---- fold the smooth near part into W_eff (in place over wnear) -----------
   const size_t wlen = size_t(nquad) * (cplx ? 2 : 1);

@@ -37,7 +37,7 @@ def built():
 
 @pytest.fixture(scope="session")
 def sphere4(built):
-    """Config-1 surface: icosahedron x2 refinements, order 4, npts 4800."""
+    """Sphere: icosahedron x2 refinements, order 4, npts 4800."""
     from fmm3dbie_b200 import surface as S
     return S.icosa_sphere(2, 4)
 
@@ -50,7 +50,7 @@ def sphere_lap_setup(sphere4):
 
 @pytest.fixture(scope="session")
 def ellipsoid_small(built):
-    """Reduced config-2 ellipsoid (1,2,3): 80 order-6 patches, npts 2240."""
+    """Reduced ellipsoid (1,2,3): 80 order-6 patches, npts 2240."""
     from fmm3dbie_b200 import surface as S
     return S.icosa_ellipsoid(1, 6, (1.0, 2.0, 3.0))
 

@@ -1,4 +1,4 @@
-"""Concurrent solves of an uneven batch of surfaces (config-4 shape, reduced):
+"""Concurrent solves of an uneven batch of surfaces (32-ellipsoid shape, reduced):
 each surface's solve on its own stream equals the same solve run alone."""
 import numpy as np
 import pytest

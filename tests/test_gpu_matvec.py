@@ -25,7 +25,7 @@ def torch():
     return torch
 
 
-def test_laplace_config1_parity(torch, sphere4, sphere_lap_setup):
+def test_laplace_sphere_parity(torch, sphere4, sphere_lap_setup):
     s, st = sphere4, sphere_lap_setup
     params = (1.0, 1.0)
     rng = np.random.default_rng(1)
@@ -126,7 +126,7 @@ def test_off_surface_eval(torch, ellipsoid_small):
 
 
 def test_single_layer_sphere_on_gpu(torch, sphere4):
-    """Known answer through the GPU path: S_0 Y_1^0 = Y_1^0/3 (config 1 surface)."""
+    """Known answer through the GPU path: S_0 Y_1^0 = Y_1^0/3 (sphere, 320 order-4 patches)."""
     st = S.setup(sphere4, 0, 1e-6, (1.0, 0.0))
     z = sphere4.xyz[:, 2]
     pot = layer.lap_comb_dir_eval(sphere4, sphere4.srcvals, *sphere4.patch_id_uvs(), 1e-6,

@@ -40,8 +40,8 @@ def test_laplace_sphere_spectrum(sphere8, params, which):
     assert _rel(s.qwts(), pot, ev * z) < 2e-6
 
 
-def test_laplace_config1_single_layer(sphere4):
-    # config 1 surface (order 4, 320 patches): S_0 Y_1^0 = Y_1^0 / 3 to eps
+def test_laplace_sphere_single_layer(sphere4):
+    # sphere, 320 order-4 patches: S_0 Y_1^0 = Y_1^0 / 3 to eps
     st = S.setup(sphere4, 0, 1e-6, (1.0, 0.0))
     z = sphere4.xyz[:, 2]
     pot = oracle.lpcomp(0, sphere4, (1.0, 0.0), st.near, st.over, z)
@@ -91,7 +91,7 @@ def test_greens_identity(built, kind):
 
 
 def test_interior_point_source_solve(ellipsoid_small, ellipsoid_helm_setup):
-    """Second oracle: exterior field of an interior source (config-2 shape)."""
+    """Second oracle: exterior field of an interior source (ellipsoid (1,2,3) point-source shape)."""
     s = ellipsoid_small
     k = 2.0
     zp = (k, -1j * k, 1.0)
