@@ -359,6 +359,8 @@ def main():
     pairs = float(P.ntarg) * float(P.nptso)
     achieved = pairs * flops_per_pair("helm") / (far_ms * 1e-3) / 1e12
     peak_tf = ctypes_double_pair(lib)
+    mufu_pk = mufu_peak(lib)
+    mufu_ach = pairs * MUFU_PER_PAIR["helm"] / (far_ms * 1e-3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "far_kernel_traffic.json")
     if os.path.exists(tp):
@@ -440,7 +442,10 @@ def main():
                          "peak_source": "FP32 FFMA loop measured in this run "
                                         "(MEASURED_PEAKS.json has no FP32 SIMT figure)",
                          "flops_per_pair": flops_per_pair("helm"), "pairs_per_launch": pairs,
-                         "avg_launch_ms": far_ms},
+                         "avg_launch_ms": far_ms,
+                         "mufu": {"ops_per_pair": MUFU_PER_PAIR["helm"], "achieved_gops": mufu_ach,
+                                  "peak_gops": mufu_pk, "frac": mufu_ach / mufu_pk,
+                                  "peak_source": "rsqrt.approx loop measured in this run"}},
             "stage_ms_per_matvec": {
                 "f32": {k: far32[k] / max(far32["calls"], 1) for k in ("strengths_ms", "far_ms", "combine_ms")},
                 "f64": {k: far64[k] / max(far64["calls"], 1) for k in ("strengths_ms", "far_ms", "combine_ms")}},
@@ -667,6 +672,17 @@ def ctypes_double_pair(lib):
     tf, ms = C.c_double(), C.c_double()
     lib.bie_measure_fp32_peak(C.byref(tf), C.byref(ms))
     return tf.value
+
+
+def mufu_peak(lib):
+    """Measured MUFU throughput in G ops/s (rsqrt.approx loop)."""
+    import ctypes as C
+    g, ms = C.c_double(), C.c_double()
+    lib.bie_measure_mufu_peak(C.byref(g), C.byref(ms))
+    return g.value
+
+
+MUFU_PER_PAIR = {"helm": 3, "lap": 1}   # rsqrt, sin, cos (Helmholtz); rsqrt (Laplace)
 
 
 if __name__ == "__main__":

@@ -120,6 +120,7 @@ _SIGS = {
     "bie_mlp_predict_density": (C.c_int, [VP, VP, I64, VP, I64, PDBL, VP, VP]),
     "bie_launch_count": (I64, []),
     "bie_measure_fp32_peak": (C.c_int, [PDBL, PDBL]),
+    "bie_measure_mufu_peak": (C.c_int, [PDBL, PDBL]),
 }
 
 _lib = None

@@ -993,4 +993,32 @@ int bie_measure_fp32_peak(double* tflops, double* ms) {
   });
 }
 
+int bie_measure_mufu_peak(double* gops, double* ms) {
+  return guarded([&] {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int threads = 256, blocks = sms * 8, iters = 1024;
+    bie::DBuf<float> out;
+    if (out.alloc(size_t(blocks) * threads)) return BIE_ERR_NOMEM;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    bie::dev::launch_mufu_peak(out.p, blocks, threads, iters / 8, 0);  // warm-up
+    cudaEventRecord(a, 0);
+    bie::dev::launch_mufu_peak(out.p, blocks, threads, iters, 0);
+    cudaEventRecord(b, 0);
+    cudaEventSynchronize(b);
+    float t = 0;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    const double ops = double(blocks) * threads * iters * 16.0 * 8.0;
+    *ms = t;
+    *gops = ops / (t * 1e-3) / 1e9;
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? BIE_OK : BIE_ERR_CUDA;
+  });
+}
+
 }  // extern "C"

@@ -44,7 +44,16 @@ struct Geometry {
   const int64_t* cmoff = nullptr;    // per class offset into imat
   const double* imat = nullptr;
   int max_np = 0, max_nf = 0;
+  // Bounding boxes (lo xyz, hi xyz) of the FP32 far kernel's target blocks
+  // (kFarBlockTargets32 targets) and source tiles (kFarTileSources sources),
+  // and the squared gap below which a tile may hold a pair closer than the
+  // self-interaction threshold (threshold plus a margin for FP32 rounding).
+  const double* tbox = nullptr;
+  const double* sbox = nullptr;
+  double box_margin2 = 0.0;
 };
+constexpr int kFarBlockTargets32 = 512;
+constexpr int kFarTileSources = 128;
 
 struct Near {
   int64_t nnz = 0, nquad = 0;
@@ -149,6 +158,8 @@ int64_t launch_count();
 void note_launches(int64_t n);
 // FFMA throughput probe (flops = blocks*threads*iters*16*8*2).
 cudaError_t launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st);
+// MUFU throughput probe (ops = blocks*threads*iters*16*8 reciprocal square roots).
+cudaError_t launch_mufu_peak(float* out, int blocks, int threads, int iters, cudaStream_t st);
 
 }  // namespace dev
 }  // namespace bie

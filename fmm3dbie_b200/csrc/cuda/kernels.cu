@@ -947,6 +947,8 @@ inline int grid_for(int64_t n, int threads) {
 // Far-kernel launch shapes.
 constexpr int kFarThreads = 128;
 constexpr int kFarTile = 128;
+static_assert(kFarTile == kFarTileSources, "source tiles of the box table");
+static_assert(kFarBlockTargetsF32 == kFarBlockTargets32, "target blocks of the box table");
 constexpr int kTptF32 = 4;
 constexpr int kTptF64 = 2;
 static_assert(kFarThreads * kTptF32 == kFarBlockTargetsF32,
@@ -1399,6 +1401,34 @@ __global__ void ffma_peak_kernel(float* out, int iters, float a, float b) {
 
 cudaError_t launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st) {
   ffma_peak_kernel<<<blocks, threads, 0, st>>>(out, iters, 0.9999999f, 1e-7f);
+  count();
+  return cudaGetLastError();
+}
+
+// MUFU throughput probe: 8 independent reciprocal-square-root chains per
+// thread (rsqrt.approx.ftz.f32, one MUFU operation each; the chains settle at
+// 1).  ops = 16 * 8 * iters per thread.
+__global__ void mufu_peak_kernel(float* out, int iters) {
+  float x0 = 1.0f + threadIdx.x * 1e-3f, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4,
+        x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      asm("rsqrt.approx.ftz.f32 %0, %0;" : "+f"(x0));
+      asm("rsqrt.approx.ftz.f32 %0, %0;" : "+f"(x1));
+      asm("rsqrt.approx.ftz.f32 %0, %0;" : "+f"(x2));
+      asm("rsqrt.approx.ftz.f32 %0, %0;" : "+f"(x3));
+      asm("rsqrt.approx.ftz.f32 %0, %0;" : "+f"(x4));
+      asm("rsqrt.approx.ftz.f32 %0, %0;" : "+f"(x5));
+      asm("rsqrt.approx.ftz.f32 %0, %0;" : "+f"(x6));
+      asm("rsqrt.approx.ftz.f32 %0, %0;" : "+f"(x7));
+    }
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+
+cudaError_t launch_mufu_peak(float* out, int blocks, int threads, int iters, cudaStream_t st) {
+  mufu_peak_kernel<<<blocks, threads, 0, st>>>(out, iters);
   count();
   return cudaGetLastError();
 }

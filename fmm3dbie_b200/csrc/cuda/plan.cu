@@ -172,6 +172,37 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   kp.ki = s.zk.imag();
   if (kind == 0) kp.ai = kp.bi = kp.kr = kp.ki = 0.0;
   kp.thresh = fmm_thresh(nptso, s.srcover, 12, ntarg, s.targs, s.ndtarg);
+  // bounding boxes of the FP32 far kernel's target blocks and source tiles;
+  // margin: the threshold plus 2^-12 of the extent, far above the FP32
+  // rounding of the centred coordinates
+  auto boxes = [](const std::vector<double>& x, const std::vector<double>& y,
+                  const std::vector<double>& z, int64_t per, std::vector<double>& out) {
+    const int64_t n = int64_t(x.size()), nb = (n + per - 1) / per;
+    out.assign(size_t(6) * std::max<int64_t>(nb, 1), 0.0);
+    for (int64_t b = 0; b < nb; ++b) {
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (int64_t j = b * per; j < std::min(n, (b + 1) * per); ++j) {
+        const double v[3] = {x[j], y[j], z[j]};
+        for (int c = 0; c < 3; ++c) {
+          lo[c] = std::min(lo[c], v[c]);
+          hi[c] = std::max(hi[c], v[c]);
+        }
+      }
+      for (int c = 0; c < 3; ++c) {
+        out[6 * b + c] = lo[c];
+        out[6 * b + 3 + c] = hi[c];
+      }
+    }
+  };
+  std::vector<double> htb, hsb;
+  boxes(htx, hty, htz, dev::kFarBlockTargets32, htb);
+  boxes(hsx, hsy, hsz, dev::kFarTileSources, hsb);
+  double ext = 0.0;
+  for (size_t b = 0; b + 5 < htb.size(); b += 6)
+    for (int c = 0; c < 3; ++c) ext = std::max(ext, std::fabs(htb[b + c]) + std::fabs(htb[b + 3 + c]));
+  for (size_t b = 0; b + 5 < hsb.size(); b += 6)
+    for (int c = 0; c < 3; ++c) ext = std::max(ext, std::fabs(hsb[b + c]) + std::fabs(hsb[b + 3 + c]));
+  const double margin = kp.thresh + std::ldexp(ext, -12);
   // ---- upload ----------------------------------------------------------------
   BIE_CUDA(upload(tx_, htx, st));
   BIE_CUDA(upload(ty_, hty, st));
@@ -193,6 +224,8 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   BIE_CUDA(upload(nps_, hnps, st));
   BIE_CUDA(upload(wofs_, hwo, st));
   BIE_CUDA(upload(wts_, hqw, st));
+  BIE_CUDA(upload(tbox_, htb, st));
+  BIE_CUDA(upload(sbox_, hsb, st));
   g.ntarg = ntarg;
   g.nptso = nptso;
   g.npatches = npatches;
@@ -214,6 +247,9 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   g.imat = imat_.p;
   g.max_np = max_np;
   g.max_nf = max_nf;
+  g.tbox = ntarg > 0 ? tbox_.p : nullptr;
+  g.sbox = sbox_.p;
+  g.box_margin2 = margin * margin;
   nr.nnz = nnz;
   nr.nquad = nquad;
   nr.row_ptr = row_ptr_.p;

@@ -142,7 +142,7 @@ class Plan {
   DBuf<double> ab64_;
   DBuf<float> ab32_;
   std::map<std::pair<int, int>, FarConfig> far_cfg_;
-  DBuf<double> tx_, ty_, tz_, sx_, sy_, sz_, snx_, sny_, snz_, sw_, imat_, wts_;
+  DBuf<double> tx_, ty_, tz_, sx_, sy_, sz_, snx_, sny_, snz_, sw_, imat_, wts_, tbox_, sbox_;
   DBuf<int32_t> pstart_, ostart_, pclass_, col_, nps_;
   DBuf<int64_t> cmoff_, row_ptr_, wofs_;
   DBuf<double> weff64_;

@@ -384,6 +384,9 @@ int64_t bie_launch_count(void);
 /* FP32 FFMA throughput of the current device (TFLOP/s) from a register-
  * resident FMA loop kernel, timed with CUDA events on the default stream. */
 int bie_measure_fp32_peak(double* tflops, double* ms);
+/* MUFU (special-function unit) throughput of the current device in G ops/s
+ * from a register-resident rsqrt.approx loop kernel, timed with CUDA events. */
+int bie_measure_mufu_peak(double* gops, double* ms);
 
 #ifdef __cplusplus
 }
