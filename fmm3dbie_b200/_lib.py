@@ -110,6 +110,7 @@ _SIGS = {
     "bie_mlp_create": (C.c_int, [I64, C.POINTER(VP)]),
     "bie_mlp_destroy": (C.c_int, [VP]),
     "bie_mlp_info": (C.c_int, [VP, PI64]),
+    "bie_mlp_set_engine": (C.c_int, [VP, I64]),
     "bie_mlp_set_params": (C.c_int, [VP, VP, VP]),
     "bie_mlp_get_params": (C.c_int, [VP, VP, VP]),
     "bie_mlp_forward": (C.c_int, [VP, VP, I64, VP, VP]),

@@ -94,12 +94,52 @@ __global__ void strengths_kernel(Geometry g, KParams kp, const double* __restric
 // The phase kr carries an absolute error of about kr 2^-24 in single
 // precision already; __sincosf's scaled argument adds an error of the same
 // order, so no separate range reduction is done.
+// Table-driven sine and cosine for the FP64 far field (the table-driven
+// reduction of P. T. P. Tang, ACM TOMS 15 (1989) / 16 (1990)):
+//   x = j (2 pi / N) + rho,  |rho| <= pi / N,
+//   sin x = S_j cos rho + C_j sin rho,  cos x = C_j cos rho - S_j sin rho,
+// with (C_j, S_j) = (cos, sin)(2 pi j / N) from a per-block table and the
+// Taylor series of sin rho (to rho^5) and cos rho (to rho^6), whose first
+// omitted terms are below 1e-17 for |rho| <= pi/256.  2 pi / N is split as
+// C1 + C2 with C1 rounded to 24 bits, so j C1 is exact for |j| < 2^29.
+constexpr int kTrigN = 256;
+constexpr double kTrigStep = 0.02454369260617026;     // 2 pi / 256
+constexpr double kTrigInvStep = 40.74366543152521;    // 256 / (2 pi)
+constexpr double kTrigC1 = 0.02454369328916073;       // float(2 pi / 256)
+constexpr double kTrigC2 = -6.829904687791004e-10;    // 2 pi / 256 - C1
+
+// Fills tab[q] = (cos, sin)(2 pi q / N) with the block's threads.
+__device__ __forceinline__ void fill_trig_table(double2* tab) {
+  for (int q = threadIdx.x; q < kTrigN; q += blockDim.x) {
+    double sq, cq;
+    sincos(double(q) * kTrigStep, &sq, &cq);
+    tab[q] = make_double2(cq, sq);
+  }
+}
+
+__device__ __forceinline__ void sincos_tab(double x, const double2* tab, double& s, double& c) {
+  const double jd = rint(x * kTrigInvStep);
+  const int j = int(jd) & (kTrigN - 1);
+  double rho = fma(-jd, kTrigC1, x);
+  rho = fma(-jd, kTrigC2, rho);
+  const double r2 = rho * rho;
+  const double sp = fma(rho * r2, fma(r2, 1.0 / 120.0, -1.0 / 6.0), rho);
+  const double cp = fma(r2, fma(r2, fma(r2, -1.0 / 720.0, 1.0 / 24.0), -0.5), 1.0);
+  const double2 t = tab[j];
+  s = fma(t.y, cp, t.x * sp);
+  c = fma(t.x, cp, -(t.y * sp));
+}
+
+// CHECK = false drops the r^2 >= thresh^2 test; callers use it only where no
+// pair of the tile can fall below the threshold, so the result is the same.
+template <bool CHECK = true>
 __device__ __forceinline__ void pair_helm(float tx, float ty, float tz, const float4 g0,
                                           const float2 g1, const float4 s, float k, float kim,
-                                          float thr2, bool ck, float& pr, float& pi) {
+                                          float thr2, bool ck, float& pr, float& pi,
+                                          const double2* = nullptr) {
   const float dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float rinv = (r2 >= thr2) ? rsqrtf(r2) : 0.0f;
+  const float rinv = (!CHECK || r2 >= thr2) ? rsqrtf(r2) : 0.0f;
   const float r = r2 * rinv;
   const float kr = k * r;
   float sn, cs;
@@ -108,27 +148,38 @@ __device__ __forceinline__ void pair_helm(float tx, float ty, float tz, const fl
   if (ck) rs *= __expf(-kim * r);
   const float dn = fmaf(dx, g0.w, fmaf(dy, g1.x, dz * g1.y));
   const float u = dn * (rinv * rinv);
-  // x = c + d u (1 - i k r); complex k = kr + i kim gives (1 + kim r) - i kr r
-  const float ur = ck ? u * (1.0f + kim * r) : u;
-  const float p = u * kr;
-  const float xr = fmaf(s.w, p, fmaf(s.z, ur, s.x));
-  const float xi = fmaf(-s.z, p, fmaf(s.w, ur, s.y));
+  float xr, xi;
+  if (ck) {
+    // x = c + d u ((1 + kim r) - i kr)  for complex k = kr + i kim
+    const float ur = u * (1.0f + kim * r);
+    const float p = u * kr;
+    xr = fmaf(s.w, p, fmaf(s.z, ur, s.x));
+    xi = fmaf(-s.z, p, fmaf(s.w, ur, s.y));
+  } else {
+    // x = c + d u (1 - i kr) = c + u (d_r + d_i kr, d_i - d_r kr)
+    xr = fmaf(u, fmaf(s.w, kr, s.z), s.x);
+    xi = fmaf(u, fmaf(-s.z, kr, s.w), s.y);
+  }
   const float er = xr * rs, ei = xi * rs;
   pr = fmaf(cs, er, fmaf(-sn, ei, pr));
   pi = fmaf(cs, ei, fmaf(sn, er, pi));
 }
 
+template <bool CHECK = true>
 __device__ __forceinline__ void pair_helm(double tx, double ty, double tz, const double4 g0,
                                           const double2 g1, const double4 s, double k, double kim,
-                                          double thr2, bool ck, double& pr, double& pi) {
+                                          double thr2, bool ck, double& pr, double& pi,
+                                          const double2* tab = nullptr) {
   const double dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
   const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-  const bool ok = r2 >= thr2;
-  const double rinv = ok ? rsqrt(r2) : 0.0;
+  const double rinv = (!CHECK || r2 >= thr2) ? rsqrt(r2) : 0.0;
   const double r = r2 * rinv;
   const double kr = k * r;
   double sn, cs;
-  sincos(kr, &sn, &cs);
+  if (tab)
+    sincos_tab(kr, tab, sn, cs);
+  else
+    sincos(kr, &sn, &cs);
   double rs = rinv;
   if (ck) rs *= exp(-kim * r);
   const double dn = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y));
@@ -141,7 +192,7 @@ __device__ __forceinline__ void pair_helm(double tx, double ty, double tz, const
   pi = fma(cs, ei, fma(sn, er, pi));
 }
 
-template <typename R>
+template <typename R, bool CHECK = true>
 __device__ __forceinline__ void pair_lap(R tx, R ty, R tz, const typename Vec<R>::T4 g0,
                                          const typename Vec<R>::T2 g1,
                                          const typename Vec<R>::T2 s, R thr2, R& p) {
@@ -149,9 +200,9 @@ __device__ __forceinline__ void pair_lap(R tx, R ty, R tz, const typename Vec<R>
   const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
   R rinv;
   if constexpr (sizeof(R) == 4)
-    rinv = (r2 >= thr2) ? rsqrtf(r2) : R(0);
+    rinv = (!CHECK || r2 >= thr2) ? rsqrtf(r2) : R(0);
   else
-    rinv = (r2 >= thr2) ? rsqrt(r2) : R(0);
+    rinv = (!CHECK || r2 >= thr2) ? rsqrt(r2) : R(0);
   const R dn = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y));
   const R e = fma(s.y * dn, rinv * rinv, s.x);
   p = fma(e, rinv, p);
@@ -167,6 +218,12 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
   __shared__ R4 sg0[TILE];
   __shared__ R2 sg1[TILE];
   __shared__ R sst[TILE * SW];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  const double2* tab = nullptr;
+  if constexpr (sizeof(R) == 8 && KIND == 1) {
+    fill_trig_table(stab);  // published by the first __syncthreads of the tile loop
+    tab = stab;
+  }
   const int64_t ntarg = g.ntarg, nptso = g.nptso;
   const int64_t tbase = int64_t(blockIdx.x) * NT * TPT;
   const int m = blockIdx.z;  // density index
@@ -188,6 +245,12 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
   }
   const R thr2 = R(kp.thresh * kp.thresh);
   const R k = R(kp.kr), kim = R(kp.ki);
+  // bounding box of this block's targets (FP32 blocks of kFarBlockTargets32)
+  double tbx[6] = {0, 0, 0, 0, 0, 0};
+  const bool boxes = sizeof(R) == 4 && NT * TPT == kFarBlockTargets32 && g.sbox && g.tbox;
+  if (boxes)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tbx[c] = g.tbox[6 * blockIdx.x + c];
   const int64_t s0 = int64_t(blockIdx.y) * chunk_len;
   const int64_t s1 = min(s0 + chunk_len, nptso);
   for (int64_t sb = s0; sb < s1; sb += TILE) {
@@ -211,18 +274,52 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
     R pr[TPT], pi[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) pr[t] = pi[t] = R(0);
+    // FP32: a full tile whose bounding box stays farther than the margin from
+    // the block's targets cannot hold an excluded pair, so it skips the test.
+    // A partial tile keeps it: its zero padding sits at the block centre,
+    // which is the block's first target.
+    bool check = true;
+    if (boxes && ns == TILE) {
+      const double* sbx = g.sbox + 6 * (sb / kFarTileSources);
+      double gap2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double gap = fmax(fmax(sbx[c] - tbx[c + 3], tbx[c] - sbx[c + 3]), 0.0);
+        gap2 += gap * gap;
+      }
+      check = gap2 <= g.box_margin2;
+    }
+    if (check) {
 #pragma unroll 4
-    for (int j = 0; j < TILE; ++j) {
-      const R4 a = sg0[j];
-      const R2 b = sg1[j];
-      if constexpr (KIND == 1) {
-        const R4 s = reinterpret_cast<const R4*>(sst)[j];
+      for (int j = 0; j < TILE; ++j) {
+        const R4 a = sg0[j];
+        const R2 b = sg1[j];
+        if constexpr (KIND == 1) {
+          const R4 s = reinterpret_cast<const R4*>(sst)[j];
 #pragma unroll
-        for (int t = 0; t < TPT; ++t) pair_helm(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, pr[t], pi[t]);
-      } else {
-        const R2 s = reinterpret_cast<const R2*>(sst)[j];
+          for (int t = 0; t < TPT; ++t)
+            pair_helm(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, pr[t], pi[t], tab);
+        } else {
+          const R2 s = reinterpret_cast<const R2*>(sst)[j];
 #pragma unroll
-        for (int t = 0; t < TPT; ++t) pair_lap<R>(tx[t], ty[t], tz[t], a, b, s, thr2, pr[t]);
+          for (int t = 0; t < TPT; ++t) pair_lap<R>(tx[t], ty[t], tz[t], a, b, s, thr2, pr[t]);
+        }
+      }
+    } else {
+#pragma unroll 4
+      for (int j = 0; j < TILE; ++j) {
+        const R4 a = sg0[j];
+        const R2 b = sg1[j];
+        if constexpr (KIND == 1) {
+          const R4 s = reinterpret_cast<const R4*>(sst)[j];
+#pragma unroll
+          for (int t = 0; t < TPT; ++t)
+            pair_helm<false>(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, pr[t], pi[t], tab);
+        } else {
+          const R2 s = reinterpret_cast<const R2*>(sst)[j];
+#pragma unroll
+          for (int t = 0; t < TPT; ++t) pair_lap<R, false>(tx[t], ty[t], tz[t], a, b, s, thr2, pr[t]);
+        }
       }
     }
 #pragma unroll
@@ -273,6 +370,12 @@ __global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
   __shared__ R2 sg1[TILE];
   __shared__ __align__(16) R sab[TILE * 2 * C];
   __shared__ __align__(16) R ssig[TILE * MD * C];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  const double2* tab = nullptr;
+  if constexpr (sizeof(R) == 8 && KIND == 1) {
+    fill_trig_table(stab);  // published by the first __syncthreads of the tile loop
+    tab = stab;
+  }
   const int64_t ntarg = g.ntarg, nptso = g.nptso;
   const int64_t tbase = int64_t(blockIdx.x) * NT * TPT;
   const int m0 = blockIdx.z * MD;
@@ -333,7 +436,7 @@ __global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
           R kr_ = R(0), ki_ = R(0);
-          pair_helm(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, kr_, ki_);
+          pair_helm(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, kr_, ki_, tab);
           const R4* sv = reinterpret_cast<const R4*>(ssig) + j * (MD / 2);
 #pragma unroll
           for (int m2 = 0; m2 < MD / 2; ++m2) {

@@ -222,6 +222,138 @@ __global__ void __launch_bounds__(256) mlp_gemm_kernel(GemmArgs g) {
     }
 }
 
+// ---- hidden-layer forward on the 5th-generation tensor cores (tcgen05) ---------
+// H_l[m0:m0+128, n0:n0+128] = tanh(H_{l-1}[m0:m0+128, :] W_l[n0:n0+128, :]^T + b_l)
+// One CTA of 128 threads per 128 x 128 output tile.  Both operands are
+// K-major (rows of 256 bf16) and are staged with cp.async in the canonical
+// no-swizzle K-major layout of the UMMA shared-memory descriptor: 8-row x
+// 16-byte core matrices, core matrix (row group g, K chunk c) at byte
+// c * 2048 + g * 128, so the K-direction core-matrix stride (LBO) is 2048 B
+// and the row-group stride (SBO) is 128 B.  One thread issues the 16
+// tcgen05.mma (M = 128, N = 128, K = 16, kind::f16 with bf16 inputs and an
+// fp32 accumulator in 128 TMEM columns) and commits them to an mbarrier;
+// every warp then reads its 32 TMEM lanes (rows) with tcgen05.ld and writes
+// the bias + tanh epilogue.  The wait on the mbarrier is bounded: on timeout
+// the kernel records the tile in *err, still frees its TMEM and returns.
+constexpr int kTcM = 128, kTcN = 128, kTcK = 256;
+constexpr int kTcThreads = 128;
+constexpr uint32_t kTcTileBytes = kTcM * kTcK * 2;         // 64 KB per operand
+constexpr uint32_t kTcSmemBytes = 2 * kTcTileBytes + 1024;   // + alignment slack
+constexpr uint32_t kTcLbo = 2048, kTcSbo = 128;
+constexpr uint32_t kTcWaitLimit = 1u << 24;
+
+__device__ __forceinline__ uint64_t umma_desc_kmajor(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= uint64_t((saddr >> 4) & 0x3FFFu);          // start address
+  d |= uint64_t((kTcLbo >> 4) & 0x3FFFu) << 16;   // leading (K-direction) byte offset
+  d |= uint64_t((kTcSbo >> 4) & 0x3FFFu) << 32;   // stride (row-group) byte offset
+  d |= uint64_t(1) << 46;                          // descriptor version for sm_100
+  return d;                                        // base offset 0, no swizzle
+}
+
+// kind::f16 instruction descriptor: fp32 accumulator, bf16 A and B, both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t umma_idesc_bf16(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    mlp_fwd_tc_kernel(const bf16* __restrict__ A, const bf16* __restrict__ Wt,
+                      const float* __restrict__ bias, bf16* __restrict__ out,
+                      int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t m0 = int64_t(blockIdx.x) * kTcM;
+  const int n0 = blockIdx.y * kTcN;
+  unsigned char* sA = tc_smem + ((1024 - (smem_u32(tc_smem) & 1023)) & 1023);
+  unsigned char* sB = sA + kTcTileBytes;
+  // TMEM accumulator (warp 0) and the completion barrier (thread 0)
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base)),
+                 "r"(uint32_t(kTcN)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::);
+  }
+  // operands -> shared memory: 16-byte chunk (row r, K chunk c)
+  for (int q = tid; q < kTcM * (kTcK / 8); q += kTcThreads) {
+    const int r = q >> 5, c = q & 31;
+    const uint32_t off = uint32_t(c) * kTcLbo + uint32_t(r >> 3) * kTcSbo + uint32_t(r & 7) * 16;
+    cp_async16(sA + off, A + (m0 + r) * kTcK + c * 8);
+    cp_async16(sB + off, Wt + int64_t(n0 + r) * kTcK + c * 8);
+  }
+  cp_async_commit();
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  // make the shared-memory writes visible to the tensor core (async proxy)
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  if (tid == 0) {
+    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+    constexpr uint32_t idesc = umma_idesc_bf16(kTcM, kTcN);
+#pragma unroll 1
+    for (int s = 0; s < kTcK / 16; ++s) {
+      const uint64_t da = umma_desc_kmajor(a0 + uint32_t(2 * s) * kTcLbo);
+      const uint64_t db = umma_desc_kmajor(b0 + uint32_t(2 * s) * kTcLbo);
+      const uint32_t acc = s > 0 ? 1u : 0u;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+          "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(&bar))
+                 : "memory");
+  }
+  // bounded wait for the MMAs (phase 0 of the barrier)
+  uint32_t done = 0;
+  for (uint32_t it = 0; it < kTcWaitLimit && !done; ++it) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(smem_u32(&bar)), "r"(0u)
+        : "memory");
+  }
+  done = __all_sync(0xffffffffu, done);  // tcgen05.ld below is warp-collective
+  if (!done && lane == 0) atomicExch(err, 1 + int(blockIdx.x));
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (done) {
+    // warp w owns TMEM lanes (rows) 32w .. 32w+31; 16 columns per load
+    const int64_t row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTcN; c0 += 16) {
+      uint32_t v[16];
+      const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+            "=r"(v[14]), "=r"(v[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      __align__(16) bf16 o[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        o[j] = f2bf(tanhf(__uint_as_float(v[j]) + bias[n0 + c0 + j]));
+      uint4* dst = reinterpret_cast<uint4*>(out + row * kW + n0 + c0);
+      dst[0] = reinterpret_cast<const uint4*>(o)[0];
+      dst[1] = reinterpret_cast<const uint4*>(o)[1];
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(kTcN)));
+}
+
 // ---- first layer (K = 10) ----------------------------------------------------
 // H0[r][n] = tanh(b0[n] + sum_c W0[n][c] X[r][c]); rows r >= m read X = 0.
 __global__ void __launch_bounds__(256) mlp_in_kernel(const float* __restrict__ X, int64_t m,
@@ -533,6 +665,8 @@ struct Net {
   int64_t step = 0;
   DBuf<float> P, G, Mo, V, Xs, Ys, wg_part, l0_part, cs_part, out_part, loss;
   DBuf<bf16> Wb, H, dZ;
+  DBuf<int> tc_err;   // set by the tcgen05 kernel if its completion wait times out
+  int engine = 0;     // hidden-layer forward GEMM: 0 mma.sync, 1 tcgen05
 
   int init(int64_t rows) {
     MLP_CUDA(cudaGetDevice(&device));
@@ -557,6 +691,10 @@ struct Net {
     MLP_CUDA(cs_part.alloc(size_t(3) * nblk_cs * kW));
     MLP_CUDA(out_part.alloc(size_t(nblk_out) * kOutPartial));
     MLP_CUDA(loss.alloc(1));
+    MLP_CUDA(tc_err.alloc(1));
+    MLP_CUDA(cudaMemset(tc_err.p, 0, sizeof(int)));
+    MLP_CUDA(cudaFuncSetAttribute(mlp_fwd_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(kTcSmemBytes)));
     MLP_CUDA(cudaMemset(P.p, 0, kNParams * sizeof(float)));
     MLP_CUDA(cudaMemset(Mo.p, 0, kNParams * sizeof(float)));
     MLP_CUDA(cudaMemset(V.p, 0, kNParams * sizeof(float)));
@@ -582,6 +720,11 @@ struct Net {
     const int64_t mp = (m + kRowTile - 1) / kRowTile * kRowTile;
     mlp_in_kernel<<<unsigned(mp / 32), 256, 0, st>>>(X, m, Wb.p + kOffW0, P.p + kOffB0, Hl(0));
     for (int l = 1; l <= 3; ++l) {
+      if (engine == 1) {
+        mlp_fwd_tc_kernel<<<dim3(unsigned(mp / kTcM), kW / kTcN, 1), kTcThreads, kTcSmemBytes, st>>>(
+            Hl(l - 1), Wb.p + kOffW[l], P.p + kOffB[l], Hl(l), tc_err.p);
+        continue;
+      }
       GemmArgs g;
       g.A = Hl(l - 1);
       g.lda = kW;
@@ -725,6 +868,17 @@ extern "C" int bie_mlp_info(void* mlp, int64_t* info) {
   info[5] = bie::mlp::kOut;
   info[6] = n->step;
   info[7] = bie::mlp::kNW;
+  info[8] = n->engine;
+  int flag = 0;
+  if (cudaMemcpy(&flag, n->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return BIE_ERR_CUDA;
+  info[9] = flag;
+  return BIE_OK;
+}
+
+extern "C" int bie_mlp_set_engine(void* mlp, int64_t engine) {
+  if (!mlp || (engine != 0 && engine != 1)) return bad("mlp: engine must be 0 (mma.sync) or 1 (tcgen05)");
+  static_cast<Net*>(mlp)->engine = int(engine);
   return BIE_OK;
 }
 

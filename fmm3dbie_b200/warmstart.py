@@ -96,9 +96,15 @@ class WarmStartMLP:
         return _stream(self.torch, self.device)
 
     def info(self):
-        out = np.zeros(8, np.int64)
+        """nparams, max_rows, inputs, width, hidden layers, outputs, Adam steps,
+        weight count, engine, tcgen05 timeout flag."""
+        out = np.zeros(10, np.int64)
         L.check(L.lib().bie_mlp_info(self._h, L.ptr(out)), "bie_mlp_info")
         return out
+
+    def set_engine(self, engine: int):
+        """0: mma.sync hidden-layer forward GEMMs; 1: tcgen05 (tensor memory)."""
+        L.check(L.lib().bie_mlp_set_engine(self._h, int(engine)), "bie_mlp_set_engine")
 
     def set_params(self, params):
         t = self.torch.as_tensor(np.asarray(params, np.float32) if not
@@ -338,8 +344,8 @@ def main(argv=None):
     ap.add_argument("--norder", type=int, default=5)
     ap.add_argument("--nk", type=int, default=8)
     ap.add_argument("--nsolves", type=int, default=2000)
-    ap.add_argument("--steps", type=int, default=30000)
-    ap.add_argument("--batch", type=int, default=16384)
+    ap.add_argument("--steps", type=int, default=300000)
+    ap.add_argument("--batch", type=int, default=32768)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--eps", type=float, default=1e-7)
     ap.add_argument("--seed", type=int, default=5)

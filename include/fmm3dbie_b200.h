@@ -348,9 +348,14 @@ int bie_farfield_dev_noalloc(int64_t kind, const double* zk, int64_t ns, const d
  * of up to max_rows rows. */
 int bie_mlp_create(int64_t max_rows, void** mlp);
 int bie_mlp_destroy(void* mlp);
-/* info[8]: nparams, max_rows, inputs, width, hidden layers, outputs, Adam
- * steps taken, number of weight (non-bias) parameters. */
+/* info[10]: nparams, max_rows, inputs, width, hidden layers, outputs, Adam
+ * steps taken, number of weight (non-bias) parameters, engine, and a flag
+ * that is non-zero if a tcgen05 kernel's completion wait ever timed out
+ * (reading it synchronises the device). */
 int bie_mlp_info(void* mlp, int64_t* info);
+/* Hidden-layer forward GEMM engine: 0 = mma.sync bf16 tiles, 1 = tcgen05
+ * (UMMA with the accumulator in tensor memory).  Backward GEMMs use mma.sync. */
+int bie_mlp_set_engine(void* mlp, int64_t engine);
 /* Sets the fp32 parameters (and their bf16 copy) and resets Adam. */
 int bie_mlp_set_params(void* mlp, const float* params_dev, void* stream);
 int bie_mlp_get_params(void* mlp, float* params_dev, void* stream);

@@ -126,3 +126,25 @@ def test_predict_density_matches_forward(net):
     for q in range(3):
         back = tau_back[q].cpu().numpy() * np.exp(1j * dirk[q, 3] * (x @ dirk[q, :3]))
         assert _rel(back, x0[:, q].cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("m", [128, 1000, 4096])
+def test_tcgen05_forward_matches(net, m):
+    """Hidden-layer forward on tcgen05 (tensor memory accumulator) against
+    the mma.sync tiles and the oracle."""
+    import torch
+    n, p = net
+    X, _ = _batch(m, 40 + m)
+    Xd = torch.from_numpy(X).cuda()
+    n.set_engine(0)
+    Y0 = n.forward(Xd).cpu().numpy()
+    n.set_engine(1)
+    try:
+        Y1 = n.forward(Xd).cpu().numpy()
+        info = n.info()
+    finally:
+        n.set_engine(0)
+    assert info[9] == 0, "tcgen05 completion wait timed out"
+    Ye, _ = M.forward(p, X.astype(np.float64), emulate_bf16=True)
+    assert _rel(Y1, Y0) < 1e-3
+    assert _rel(Y1, Ye) < 2e-3
