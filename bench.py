@@ -255,7 +255,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--matvec-only", type=int, default=0,
                     help="build the workload, run this many matvecs (see --prec) and exit "
                          "(the command the ncu summaries in profiles/ use)")

@@ -227,6 +227,7 @@ int eval_on_gpu(int kind, cdouble zk, cdouble alpha, cdouble beta, int64_t npatc
                 int64_t nptso, const int64_t* ixyzso, const double* srcover,
                 const double* whtsover, const double* sigma, double* pot) {
   Stage stg;
+  bie::AllocStreamScope alloc_scope(stg.st);  // plan buffers return to the pool on stg.st
   bie::Plan P;
   int ier = plan_from_arrays(P, kind, zk, alpha, beta, npatches, norders, ixyzs, iptype, npts,
                              srccoefs, srcvals, ndtarg, ntarg, targs, nnz, row_ptr, col_ind, iquad,
@@ -263,6 +264,7 @@ int solve_on_gpu(int kind, cdouble zk, cdouble alpha, cdouble beta, int64_t npat
     return BIE_ERR_ARG;
   }
   Stage stg;
+  bie::AllocStreamScope alloc_scope(stg.st);  // plan buffers return to the pool on stg.st
   bie::Plan P;
   int ier = plan_from_arrays(P, kind, zk, alpha, beta, npatches, norders, ixyzs, iptype, npts,
                              srccoefs, srcvals, 12, npts, srcvals, nnz, row_ptr, col_ind, iquad,

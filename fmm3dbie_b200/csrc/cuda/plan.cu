@@ -39,6 +39,30 @@ cudaError_t upload(DBuf<T>& b, const std::vector<T>& h, cudaStream_t st) {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
 
+cudaStream_t& alloc_stream() {
+  thread_local cudaStream_t s = nullptr;
+  return s;
+}
+
+AllocStreamScope::AllocStreamScope(cudaStream_t s) : prev(alloc_stream()) {
+  // keep the default pool's memory between calls (no release at syncs)
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done[dev]) {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+      done[dev] = true;
+    }
+  }
+  alloc_stream() = s;
+}
+
 int Plan::build(const PlanSpec& s, cudaStream_t st) {
   BIE_CUDA(cudaGetDevice(&device));
   BIE_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));

@@ -32,10 +32,28 @@ enum Status {
 void set_last_error(const std::string& msg);
 const char* last_error();
 
+// Stream on which the calling thread's DBuf allocations are stream-ordered
+// (cudaMallocAsync / cudaFreeAsync from the device's default memory pool,
+// which keeps freed memory for reuse); null means cudaMalloc / cudaFree.
+cudaStream_t& alloc_stream();
+// Sets alloc_stream() for a scope.  Used by entry points that build a plan,
+// run it and release it on one private stream: their buffers come back to
+// the pool without a device-wide synchronisation, and the next call reuses
+// them.  Every buffer allocated in the scope must be released before the
+// stream is destroyed.
+struct AllocStreamScope {
+  cudaStream_t prev;
+  explicit AllocStreamScope(cudaStream_t s);
+  ~AllocStreamScope() { alloc_stream() = prev; }
+  AllocStreamScope(const AllocStreamScope&) = delete;
+  AllocStreamScope& operator=(const AllocStreamScope&) = delete;
+};
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t st = nullptr;  // stream of a stream-ordered allocation
   DBuf() = default;
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
@@ -44,18 +62,27 @@ struct DBuf {
     if (count <= n && p) return cudaSuccess;
     release();
     if (count == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    cudaStream_t s = alloc_stream();
+    cudaError_t e = s ? cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), s)
+                      : cudaMalloc(&p, count * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;
       return e;
     }
     n = count;
+    st = s;
     return cudaSuccess;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (st)
+        cudaFreeAsync(p, st);
+      else
+        cudaFree(p);
+    }
     p = nullptr;
     n = 0;
+    st = nullptr;
   }
 };
 

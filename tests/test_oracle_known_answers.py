@@ -90,6 +90,26 @@ def test_greens_identity(built, kind):
     assert err < 5e-6, err
 
 
+@pytest.mark.parametrize("kind", [0, 1])
+def test_greens_identity_quad_torus(built, kind):
+    """Quad patches (iptype 11, tensor Gauss-Legendre nodes): the warm-start
+    torus family at 16 x 8 patches of 6 x 6 nodes; the source sits above the
+    hole, outside the tube."""
+    from fmm3dbie_b200.warmstart import torus_surface
+    s = torus_surface(16, 8, 5)
+    k = 3.0
+    x0 = np.array([0.3, 0.2, 1.7])
+    u, dudn = _point_source(kind, k, x0, s.xyz, s.normals)
+    pS = (1.0, 0.0) if kind == 0 else (k, 1.0, 0.0)
+    pD = (0.0, 1.0) if kind == 0 else (k, 0.0, 1.0)
+    stS = S.setup(s, kind, 1e-7, pS)
+    stD = S.setup(s, kind, 1e-7, pD)
+    sl = oracle.lpcomp(kind, s, pS, stS.near, stS.over, dudn)
+    dl = oracle.lpcomp(kind, s, pD, stD.near, stD.over, u)
+    err = _rel(s.qwts(), 2 * (sl - dl), u)
+    assert err < 3e-5, err   # 1.0e-5 measured (3.4e-7 at 32 x 16 patches)
+
+
 def test_interior_point_source_solve(ellipsoid_small, ellipsoid_helm_setup):
     """Second oracle: exterior field of an interior source (ellipsoid (1,2,3) point-source shape)."""
     s = ellipsoid_small
