@@ -282,12 +282,12 @@ int solve_on_gpu(int kind, cdouble zk, cdouble alpha, cdouble beta, int64_t npat
   cudaMemcpyAsync(dr.p, rhs, sizeof(double) * len, cudaMemcpyHostToDevice, stg.st);
   // zid = -(-1)^ifinout beta/2 (helm_comb_dir.f:2215, lap_comb_dir.f90:1619)
   const double sgn = (ifinout % 2 == 0) ? -1.0 : 1.0;
-  const cdouble zid = sgn * beta / 2.0;
+  const std::vector<cdouble> zid(size_t(nrhs), sgn * beta / 2.0);  // one per system
   int status = BIE_OK;
   if (iprec == 1) {
     bie::MixedOut mo;
-    status = bie::solve_mixed(P, int(nrhs), zid, dr.p, nullptr, numit, eps_gmres, 1e-5, 6, dx.p,
-                              mo, stg.st);
+    status = bie::solve_mixed(P, int(nrhs), zid.data(), dr.p, nullptr, numit, eps_gmres, 1e-5, 6,
+                              dx.p, mo, stg.st);
     if (status != BIE_OK && status != BIE_NOT_CONVERGED) return status;
     for (int64_t q = 0; q < nrhs; ++q) {
       if (niter) niter[q] = mo.inner_iters[q];
@@ -295,7 +295,8 @@ int solve_on_gpu(int kind, cdouble zk, cdouble alpha, cdouble beta, int64_t npat
     }
   } else {
     bie::GmresOut go;
-    status = bie::gmres(P, 0, 0, int(nrhs), zid, dr.p, nullptr, numit, eps_gmres, dx.p, go, stg.st);
+    status = bie::gmres(P, 0, 0, int(nrhs), zid.data(), dr.p, nullptr, numit, eps_gmres, dx.p, go,
+                        stg.st);
     if (status != BIE_OK && status != BIE_NOT_CONVERGED && status != BIE_BREAKDOWN) return status;
     for (int64_t q = 0; q < nrhs; ++q) {
       if (niter) niter[q] = go.niter[q];
@@ -853,11 +854,12 @@ int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
   if (!plan || (mode != 0 && mode != 1) || nd < 1 || nd > 256 || numit < 1) return BIE_ERR_ARG;
   return guarded([&] {
     bie::Plan& P = *static_cast<bie::Plan*>(plan);
-    const cdouble z(zid[0], P.cplx ? zid[1] : 0.0);
+    const std::vector<cdouble> z(size_t(nd), cdouble(zid[0], P.cplx ? zid[1] : 0.0));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (mode == 0) {
       bie::GmresOut go;
-      const int s = bie::gmres(P, 0, 0, int(nd), z, rhs_dev, x0_dev, numit, eps_gmres, soln_dev, go, st);
+      const int s = bie::gmres(P, 0, 0, int(nd), z.data(), rhs_dev, x0_dev, numit, eps_gmres,
+                               soln_dev, go, st);
       if (s == BIE_OK || s == BIE_NOT_CONVERGED || s == BIE_BREAKDOWN) {
         for (int64_t q = 0; q < nd; ++q) {
           if (niter) niter[q] = go.niter[q];
@@ -869,7 +871,7 @@ int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
       return s;
     }
     bie::MixedOut mo;
-    const int s = bie::solve_mixed(P, int(nd), z, rhs_dev, x0_dev, numit, eps_gmres, 1e-5, 6,
+    const int s = bie::solve_mixed(P, int(nd), z.data(), rhs_dev, x0_dev, numit, eps_gmres, 1e-5, 6,
                                    soln_dev, mo, st);
     if (s == BIE_OK || s == BIE_NOT_CONVERGED) {
       for (int64_t q = 0; q < nd; ++q) {

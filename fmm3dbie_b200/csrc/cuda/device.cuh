@@ -131,26 +131,39 @@ cudaError_t launch_source_consts(const Geometry& g, const KParams& kp, int preci
                                  cudaStream_t st);
 
 // ---- GMRES helpers --------------------------------------------------------
-// Vectors hold npts points x nd densities (point-major), n = npts*nd values
-// (2n doubles when complex); density d is independent system d, so inner
-// products are per density.  wts are per point.
-// out[2*(k*nd+d)] + i out[2*(k*nd+d)+1] = sum_pt wts * conj(V_k[pt,d]) w[pt,d]
-// for k < m, V_k = V + k*ldv; partial needs 2*m*nd*nblk doubles.
-cudaError_t launch_mdot(const double* V, int64_t ldv, int m, const double* w,
-                        const double* wts, int64_t npts, int nd, int cplx, double* partial,
-                        int nblk, double* out, cudaStream_t st);
-// w[pt,d] -= sum_k h[k,d] V_k[pt,d]   (h complex on device, layout as out)
+// Vectors hold npts nodes x nd densities (point-major).  The nodes form
+// nseg segments (the surfaces of a batch; one for a single plan); system
+// sys = segment * nd + density is one independent linear system.  Reductions
+// run over chunks: contiguous node ranges that lie inside one segment.
+struct Segs {
+  int nseg = 1;                         // segments
+  int nchunk = 1;                       // reduction chunks
+  const int64_t* chunk_lo = nullptr;    // device, nchunk: first node of each chunk
+  const int64_t* chunk_hi = nullptr;    // device, nchunk: one past its last node
+  const int32_t* seg_chunk0 = nullptr;  // device, nseg+1: first chunk of each segment
+  const int32_t* node_seg = nullptr;    // device, npts: segment of each node (null if nseg == 1)
+};
+// out[2*(k*nsys + sys)] + i out[2*(k*nsys + sys)+1] = sum over sys's nodes of
+// wts * conj(V_k) w, for k < m, V_k = V + k*ldv; partial needs
+// 2*m*nd*nchunk doubles.
+cudaError_t launch_mdot(const double* V, int64_t ldv, int m, const double* w, const double* wts,
+                        int nd, int cplx, const Segs& sg, double* partial, double* out,
+                        cudaStream_t st);
+// w[e] -= sum_k h[k, sys(e)] V_k[e]   (h complex on device, layout as out)
 cudaError_t launch_maxpy(const double* V, int64_t ldv, int m, const double* h, double* w,
-                         int64_t n, int nd, int cplx, cudaStream_t st);
-// y[pt,d] = s[d] x[pt,d], s complex on device (y may alias x)
+                         int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st);
+// y[e] = s[sys(e)] x[e], s complex on device (y may alias x)
 cudaError_t launch_dscale(const double* x, double* y, const double* s, int64_t n, int nd,
-                          int cplx, cudaStream_t st);
+                          int cplx, const Segs& sg, cudaStream_t st);
 // y = a x + b y with scalar complex a = (ar, ai), b = (br, bi)
 cudaError_t launch_axpby(const double* x, double* y, double ar, double ai, double br, double bi,
                          int64_t n, int cplx, cudaStream_t st);
-// y[pt,d] = sum_k c[k,d] V_k[pt,d]
+// y[e] = a[sys(e)] x[e] + b y[e], a complex per system on device
+cudaError_t launch_axpbys(const double* x, double* y, const double* a, double br, double bi,
+                          int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st);
+// y[e] = sum_k c[k, sys(e)] V_k[e]
 cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
-                         int64_t n, int nd, int cplx, cudaStream_t st);
+                         int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st);
 
 // Number of kernels this library has launched in the process.
 int64_t launch_count();

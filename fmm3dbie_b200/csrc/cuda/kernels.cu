@@ -875,22 +875,33 @@ __global__ void to_f32_kernel(const double* __restrict__ in, float* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// GMRES vector kernels.  Vectors hold npts points x nd densities
-// (point-major); the nd densities are nd independent systems, so every
-// inner product is segmented by density index.
+// GMRES vector kernels.  Vectors hold npts nodes x nd densities (point-major).
+// The nodes form segments (one per surface of a batch); system
+// sys = seg(node) * nd + density is one independent linear system, so every
+// inner product is taken per system and every coefficient is per system.
+// Reductions run over chunks: contiguous node ranges inside one segment.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ int sys_of(const Segs& sg, int64_t e, int nd) {
+  const int64_t pt = e / nd;
+  const int seg = sg.node_seg ? sg.node_seg[pt] : 0;
+  return seg * nd + int(e - pt * nd);
+}
+
+// partial[((k*nd + d)*nchunk + c)] = sum over chunk c of wts * conj(V_k) w
 template <int CPLX>
 __global__ void mdot_partial_kernel(const double* __restrict__ V, int64_t ldv, int m,
                                     const double* __restrict__ w, const double* __restrict__ wts,
-                                    int64_t npts, int nd, double* __restrict__ partial) {
+                                    int nd, Segs sg, double* __restrict__ partial) {
   __shared__ double2 red[256];
   const int tid = threadIdx.x;
   const int rows = blockDim.x / nd;  // blockDim.x is a multiple of nd
   const int dd = tid % nd, r = tid / nd;
+  const int c = blockIdx.x;
+  const int64_t lo = sg.chunk_lo[c], hi = sg.chunk_hi[c];
   for (int k = 0; k < m; ++k) {
     const double* v = V + size_t(k) * ldv;
     double sr = 0, si = 0;
-    for (int64_t pt = int64_t(blockIdx.x) * rows + r; pt < npts; pt += int64_t(gridDim.x) * rows) {
+    for (int64_t pt = lo + r; pt < hi; pt += rows) {
       const int64_t e = pt * nd + dd;
       const double wt = wts[pt];
       if (CPLX) {
@@ -909,7 +920,7 @@ __global__ void mdot_partial_kernel(const double* __restrict__ V, int64_t ldv, i
         ar += red[q * nd + tid].x;
         ai += red[q * nd + tid].y;
       }
-      const size_t o = (size_t(k) * nd + tid) * gridDim.x + blockIdx.x;
+      const size_t o = (size_t(k) * nd + tid) * sg.nchunk + c;
       partial[2 * o] = ar;
       partial[2 * o + 1] = ai;
     }
@@ -917,15 +928,21 @@ __global__ void mdot_partial_kernel(const double* __restrict__ V, int64_t ldv, i
   }
 }
 
-__global__ void mdot_final_kernel(const double* __restrict__ partial, int nblk,
+// out[2*(k*nsys + sys)] = sum of the partials of the chunks of sys's segment
+__global__ void mdot_final_kernel(const double* __restrict__ partial, int nd, Segs sg,
                                   double* __restrict__ out) {
   __shared__ double red[2][32];
-  const int k = blockIdx.x;  // flattened (k, density)
+  const int nsys = sg.nseg * nd;
+  const int b = blockIdx.x;  // flattened (k, sys)
+  const int k = b / nsys, sys = b - k * nsys;
+  const int seg = sys / nd, d = sys - seg * nd;
+  const int c0 = sg.seg_chunk0[seg], c1 = sg.seg_chunk0[seg + 1];
+  const size_t base = (size_t(k) * nd + d) * sg.nchunk;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   double sr = 0, si = 0;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-    sr += partial[2 * (size_t(k) * nblk + b)];
-    si += partial[2 * (size_t(k) * nblk + b) + 1];
+  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    sr += partial[2 * (base + c)];
+    si += partial[2 * (base + c) + 1];
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
@@ -946,24 +963,25 @@ __global__ void mdot_final_kernel(const double* __restrict__ partial, int nblk,
       si += __shfl_xor_sync(0xffffffffu, si, off);
     }
     if (lane == 0) {
-      out[2 * k] = sr;
-      out[2 * k + 1] = si;
+      out[2 * b] = sr;
+      out[2 * b + 1] = si;
     }
   }
 }
 
-// w[pt,d] -= sum_k h[k,d] V_k[pt,d]
+// w[e] -= sum_k h[k, sys(e)] V_k[e]
 template <int CPLX>
 __global__ void maxpy_kernel(const double* __restrict__ V, int64_t ldv, int m,
                              const double* __restrict__ h, double* __restrict__ w, int64_t n,
-                             int nd) {
+                             int nd, Segs sg) {
+  const int nsys = sg.nseg * nd;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
        e += int64_t(gridDim.x) * blockDim.x) {
-    const int dd = int(e % nd);
+    const int sy = sys_of(sg, e, nd);
     if (CPLX) {
       double xr = w[2 * e], xi = w[2 * e + 1];
       for (int k = 0; k < m; ++k) {
-        const double hr = h[2 * (k * nd + dd)], hi = h[2 * (k * nd + dd) + 1];
+        const double hr = h[2 * (k * nsys + sy)], hi = h[2 * (k * nsys + sy) + 1];
         const double vr = V[size_t(k) * ldv + 2 * e], vi = V[size_t(k) * ldv + 2 * e + 1];
         xr -= hr * vr - hi * vi;
         xi -= hr * vi + hi * vr;
@@ -972,23 +990,24 @@ __global__ void maxpy_kernel(const double* __restrict__ V, int64_t ldv, int m,
       w[2 * e + 1] = xi;
     } else {
       double x = w[e];
-      for (int k = 0; k < m; ++k) x -= h[2 * (k * nd + dd)] * V[size_t(k) * ldv + e];
+      for (int k = 0; k < m; ++k) x -= h[2 * (k * nsys + sy)] * V[size_t(k) * ldv + e];
       w[e] = x;
     }
   }
 }
 
-// y[pt,d] = sum_k c[k,d] V_k[pt,d]
+// y[e] = sum_k c[k, sys(e)] V_k[e]
 template <int CPLX>
 __global__ void combo_kernel(const double* __restrict__ V, int64_t ldv, int m,
                              const double* __restrict__ c, double* __restrict__ y, int64_t n,
-                             int nd) {
+                             int nd, Segs sg) {
+  const int nsys = sg.nseg * nd;
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
        e += int64_t(gridDim.x) * blockDim.x) {
-    const int dd = int(e % nd);
+    const int sy = sys_of(sg, e, nd);
     double xr = 0, xi = 0;
     for (int k = 0; k < m; ++k) {
-      const double cr = c[2 * (k * nd + dd)], ci = c[2 * (k * nd + dd) + 1];
+      const double cr = c[2 * (k * nsys + sy)], ci = c[2 * (k * nsys + sy) + 1];
       if (CPLX) {
         const double vr = V[size_t(k) * ldv + 2 * e], vi = V[size_t(k) * ldv + 2 * e + 1];
         xr += cr * vr - ci * vi;
@@ -1022,14 +1041,33 @@ __global__ void axpby_kernel(const double* __restrict__ x, double* __restrict__ 
   }
 }
 
-// y[pt,d] = s[d] * x[pt,d] with s complex, on device
+// y[e] = a[sys(e)] * x[e] + b * y[e], a complex per system (device)
 template <int CPLX>
-__global__ void dscale_kernel(const double* __restrict__ x, double* __restrict__ y,
-                              const double* __restrict__ s, int64_t n, int nd) {
+__global__ void axpbys_kernel(const double* __restrict__ x, double* __restrict__ y,
+                              const double* __restrict__ a, double br, double bi, int64_t n,
+                              int nd, Segs sg) {
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
        e += int64_t(gridDim.x) * blockDim.x) {
-    const int dd = int(e % nd);
-    const double sr = s[2 * dd], si = s[2 * dd + 1];
+    const int sy = sys_of(sg, e, nd);
+    const double ar = a[2 * sy], ai = a[2 * sy + 1];
+    if (CPLX) {
+      const double xr = x[2 * e], xi = x[2 * e + 1], yr = y[2 * e], yi = y[2 * e + 1];
+      y[2 * e] = ar * xr - ai * xi + br * yr - bi * yi;
+      y[2 * e + 1] = ar * xi + ai * xr + br * yi + bi * yr;
+    } else {
+      y[e] = ar * x[e] + br * y[e];
+    }
+  }
+}
+
+// y[e] = s[sys(e)] * x[e], s complex per system (device)
+template <int CPLX>
+__global__ void dscale_kernel(const double* __restrict__ x, double* __restrict__ y,
+                              const double* __restrict__ s, int64_t n, int nd, Segs sg) {
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int sy = sys_of(sg, e, nd);
+    const double sr = s[2 * sy], si = s[2 * sy + 1];
     if (CPLX) {
       const double xr = x[2 * e], xi = x[2 * e + 1];
       y[2 * e] = sr * xr - si * xi;
@@ -1425,37 +1463,37 @@ cudaError_t launch_reduce_partials(int kind, const double* partial, int nchunks,
 }
 
 cudaError_t launch_mdot(const double* V, int64_t ldv, int m, const double* w, const double* wts,
-                        int64_t npts, int nd, int cplx, double* partial, int nblk, double* out,
+                        int nd, int cplx, const Segs& sg, double* partial, double* out,
                         cudaStream_t st) {
   if (m <= 0) return cudaSuccess;
   if (nd < 1 || nd > 256) return cudaErrorInvalidValue;
   const int threads = (256 / nd) * nd;
   if (cplx)
-    mdot_partial_kernel<1><<<nblk, threads, 0, st>>>(V, ldv, m, w, wts, npts, nd, partial);
+    mdot_partial_kernel<1><<<sg.nchunk, threads, 0, st>>>(V, ldv, m, w, wts, nd, sg, partial);
   else
-    mdot_partial_kernel<0><<<nblk, threads, 0, st>>>(V, ldv, m, w, wts, npts, nd, partial);
-  mdot_final_kernel<<<m * nd, 256, 0, st>>>(partial, nblk, out);
+    mdot_partial_kernel<0><<<sg.nchunk, threads, 0, st>>>(V, ldv, m, w, wts, nd, sg, partial);
+  mdot_final_kernel<<<m * sg.nseg * nd, 256, 0, st>>>(partial, nd, sg, out);
   count(2);
   return cudaGetLastError();
 }
 
 cudaError_t launch_maxpy(const double* V, int64_t ldv, int m, const double* h, double* w,
-                         int64_t n, int nd, int cplx, cudaStream_t st) {
+                         int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st) {
   if (m <= 0) return cudaSuccess;
   if (cplx)
-    maxpy_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, h, w, n, nd);
+    maxpy_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, h, w, n, nd, sg);
   else
-    maxpy_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, h, w, n, nd);
+    maxpy_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, h, w, n, nd, sg);
   count();
   return cudaGetLastError();
 }
 
 cudaError_t launch_dscale(const double* x, double* y, const double* s, int64_t n, int nd, int cplx,
-                          cudaStream_t st) {
+                          const Segs& sg, cudaStream_t st) {
   if (cplx)
-    dscale_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(x, y, s, n, nd);
+    dscale_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(x, y, s, n, nd, sg);
   else
-    dscale_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(x, y, s, n, nd);
+    dscale_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(x, y, s, n, nd, sg);
   count();
   return cudaGetLastError();
 }
@@ -1470,12 +1508,22 @@ cudaError_t launch_axpby(const double* x, double* y, double ar, double ai, doubl
   return cudaGetLastError();
 }
 
-cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
-                         int64_t n, int nd, int cplx, cudaStream_t st) {
+cudaError_t launch_axpbys(const double* x, double* y, const double* a, double br, double bi,
+                          int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st) {
   if (cplx)
-    combo_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, c, y, n, nd);
+    axpbys_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(x, y, a, br, bi, n, nd, sg);
   else
-    combo_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, c, y, n, nd);
+    axpbys_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(x, y, a, br, bi, n, nd, sg);
+  count();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
+                         int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st) {
+  if (cplx)
+    combo_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, c, y, n, nd, sg);
+  else
+    combo_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(V, ldv, m, c, y, n, nd, sg);
   count();
   return cudaGetLastError();
 }

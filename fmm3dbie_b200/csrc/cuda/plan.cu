@@ -298,7 +298,11 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   for (auto& e : ev_) BIE_CUDA(cudaEventCreate(&e));
   // host vectors above are consumed by async copies: wait before they go
   BIE_CUDA(cudaStreamSynchronize(st));
-  return kOk;
+  // as a solver operator: one segment of npts nodes
+  nodes = npts;
+  d_node_wts = wts_.p;
+  seg_start = {0, npts};
+  return init_segments(st);
 }
 
 int Plan::nchunks_for(int precision, int nd) const { return far_config(precision, nd).nchunks; }
@@ -464,326 +468,6 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
     times.calls[precision] += 1;
   }
   return kOk;
-}
-
-// ---------------------------------------------------------------------------
-// GMRES
-// ---------------------------------------------------------------------------
-namespace {
-// zrotmat_gmres (rotmat_gmres.f:60-100)
-inline void rotmat(cdouble a, cdouble b, cdouble& c, cdouble& s) {
-  if (a == cdouble(0)) {
-    s = 1.0;
-    c = 0.0;
-  } else {
-    const cdouble t = b / a;
-    c = 1.0 / std::sqrt(1.0 + std::norm(t));
-    s = t * c;
-  }
-}
-
-}  // namespace
-
-int gmres(Plan& P, int precision, int rres_precision, int nd, cdouble zid, const double* d_rhs,
-          const double* d_x0, int64_t numit, double eps_gmres, double* d_soln, GmresOut& out,
-          cudaStream_t st) {
-  if (!P.targets_on_surface || P.ntarg != P.npts) {
-    set_last_error("GMRES needs a plan whose targets are the surface nodes");
-    return kErrArg;
-  }
-  if (numit < 1 || nd < 1 || nd > 256) return kErrArg;
-  const int cplx = P.cplx ? 1 : 0;
-  const int64_t npts = P.npts, n = npts * nd;
-  const int64_t ldv = n * (cplx ? 2 : 1);
-  const int nblk = std::min<int>(2 * P.num_sms, int((npts + 63) / 64) + 1);
-  GmresWorkspace& ws = P.gws;
-  BIE_CUDA(ws.V.alloc(size_t(ldv) * (numit + 1)));
-  BIE_CUDA(ws.w.alloc(size_t(ldv)));
-  BIE_CUDA(ws.partial.alloc(size_t(2) * (numit + 1) * nd * nblk));
-  BIE_CUDA(ws.dots.alloc(size_t(2) * 3 * (numit + 1) * nd));
-  BIE_CUDA(ws.coef.alloc(size_t(2) * (numit + 1) * nd));
-  BIE_CUDA(ws.scale.alloc(size_t(2) * nd));
-  double* d_h1 = ws.dots.p;
-  double* d_h2 = ws.dots.p + 2 * (numit + 1) * nd;
-  double* d_nrm = ws.dots.p + 4 * (numit + 1) * nd;
-  const double* wts = P.d_wts();
-  double* V = ws.V.p;
-  // residual start: r0 = rhs - (zid x0 + K x0)  (stored in V_0 before scaling)
-  if (d_x0) {
-    int ier = P.matvec(precision, nd, d_x0, V, st);
-    if (ier) return ier;
-    // V0 = -(zid x0 + K x0) + rhs
-    BIE_CUDA(dev::launch_axpby(d_x0, V, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
-    BIE_CUDA(dev::launch_axpby(d_rhs, V, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
-  } else {
-    BIE_CUDA(cudaMemcpyAsync(V, d_rhs, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  }
-  BIE_CUDA(dev::launch_mdot(V, ldv, 1, V, wts, npts, nd, cplx, ws.partial.p, nblk, d_nrm, st));
-  std::vector<double> hbuf(2 * (numit + 1) * nd * 2 + 2 * nd);
-  BIE_CUDA(cudaMemcpyAsync(hbuf.data(), d_nrm, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-  BIE_CUDA(cudaStreamSynchronize(st));
-  std::vector<double> rb(nd), bnorm(nd);
-  std::vector<double> hscale(2 * nd, 0.0);
-  for (int d = 0; d < nd; ++d) {
-    rb[d] = std::sqrt(std::max(hbuf[2 * d], 0.0));
-    hscale[2 * d] = rb[d] > 0 ? 1.0 / rb[d] : 0.0;
-    bnorm[d] = rb[d];
-  }
-  // With an initial guess the stopping test stays relative to ||rhs||_w, so a
-  // warm-started solve meets the same accuracy as one from zero.
-  if (d_x0) {
-    BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, npts, nd, cplx, ws.partial.p, nblk, d_nrm, st));
-    std::vector<double> hb(2 * nd);
-    BIE_CUDA(cudaMemcpyAsync(hb.data(), d_nrm, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaStreamSynchronize(st));
-    for (int d = 0; d < nd; ++d) bnorm[d] = std::sqrt(std::max(hb[2 * d], 0.0));
-  }
-  BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nd * sizeof(double), cudaMemcpyHostToDevice, st));
-  BIE_CUDA(dev::launch_dscale(V, V, ws.scale.p, n, nd, cplx, st));
-  // per-system Hessenberg columns, rotations and residual vector
-  const int64_t M = numit;
-  std::vector<cdouble> H(size_t(nd) * (M + 1) * M), cs(size_t(nd) * M), sn(size_t(nd) * M),
-      sv(size_t(nd) * (M + 1));
-  std::vector<int64_t> done(nd, 0);
-  out.niter.assign(nd, 0);
-  out.errs.assign(size_t(nd) * (M + 1), 0.0);
-  out.rres.assign(nd, 0.0);
-  out.status = kOk;
-  int nactive = 0;
-  for (int d = 0; d < nd; ++d) {
-    sv[size_t(d) * (M + 1)] = rb[d];
-    if (rb[d] == 0.0) done[d] = -1;  // zero right-hand side: solution 0
-    else ++nactive;
-  }
-  auto Hc = [&](int d, int64_t row, int64_t col) -> cdouble& {
-    return H[(size_t(d) * M + col) * (M + 1) + row];
-  };
-  std::vector<double> hh1(2 * (M + 1) * nd), hh2(2 * (M + 1) * nd), hn(2 * nd);
-  int64_t it = 0;
-  for (; it < M && nactive > 0; ++it) {
-    double* vit = V + size_t(it) * ldv;
-    double* vnext = V + size_t(it + 1) * ldv;
-    int ier = P.matvec(precision, nd, vit, ws.w.p, st);
-    if (ier) return ier;
-    const int m = int(it + 1);
-    BIE_CUDA(dev::launch_mdot(V, ldv, m, ws.w.p, wts, npts, nd, cplx, ws.partial.p, nblk, d_h1, st));
-    BIE_CUDA(dev::launch_maxpy(V, ldv, m, d_h1, ws.w.p, n, nd, cplx, st));
-    BIE_CUDA(dev::launch_mdot(V, ldv, m, ws.w.p, wts, npts, nd, cplx, ws.partial.p, nblk, d_h2, st));
-    BIE_CUDA(dev::launch_maxpy(V, ldv, m, d_h2, ws.w.p, n, nd, cplx, st));
-    BIE_CUDA(dev::launch_mdot(ws.w.p, ldv, 1, ws.w.p, wts, npts, nd, cplx, ws.partial.p, nblk, d_nrm, st));
-    BIE_CUDA(cudaMemcpyAsync(hh1.data(), d_h1, 2 * m * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaMemcpyAsync(hh2.data(), d_h2, 2 * m * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaMemcpyAsync(hn.data(), d_nrm, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaStreamSynchronize(st));
-    for (int d = 0; d < nd; ++d) {
-      hscale[2 * d] = 0.0;
-      hscale[2 * d + 1] = 0.0;
-      if (done[d] != 0) continue;
-      for (int k = 0; k < m; ++k)
-        Hc(d, k, it) = cdouble(hh1[2 * (k * nd + d)] + hh2[2 * (k * nd + d)],
-                               hh1[2 * (k * nd + d) + 1] + hh2[2 * (k * nd + d) + 1]);
-      Hc(d, it, it) += zid;
-      const double wnrm = std::sqrt(std::max(hn[2 * d], 0.0));
-      cdouble* c = cs.data() + size_t(d) * M;
-      cdouble* s = sn.data() + size_t(d) * M;
-      cdouble* svd = sv.data() + size_t(d) * (M + 1);
-      for (int64_t k = 0; k < it; ++k) {
-        const cdouble t = c[k] * Hc(d, k, it) + std::conj(s[k]) * Hc(d, k + 1, it);
-        Hc(d, k + 1, it) = -s[k] * Hc(d, k, it) + c[k] * Hc(d, k + 1, it);
-        Hc(d, k, it) = t;
-      }
-      rotmat(Hc(d, it, it), cdouble(wnrm), c[it], s[it]);
-      Hc(d, it, it) = c[it] * Hc(d, it, it) + std::conj(s[it]) * wnrm;
-      svd[it + 1] = -s[it] * svd[it];
-      svd[it] = c[it] * svd[it];
-      const double err = bnorm[d] > 0 ? std::abs(svd[it + 1]) / bnorm[d] : 0.0;
-      out.errs[size_t(d) * (M + 1) + it] = err;
-      if (!(err == err) || !(wnrm == wnrm)) {
-        out.status = kBreakdown;
-        done[d] = it + 1;
-        --nactive;
-        continue;
-      }
-      if (err <= eps_gmres || it == M - 1 || wnrm == 0.0) {
-        done[d] = it + 1;
-        --nactive;
-        continue;
-      }
-      hscale[2 * d] = 1.0 / wnrm;
-    }
-    BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nd * sizeof(double), cudaMemcpyHostToDevice, st));
-    BIE_CUDA(dev::launch_dscale(ws.w.p, vnext, ws.scale.p, n, nd, cplx, st));
-  }
-  // back-substitution per system: y = triu(H)\s, soln = V y (+ x0)
-  std::vector<double> hc(size_t(2) * (M + 1) * nd, 0.0);
-  for (int d = 0; d < nd; ++d) {
-    if (done[d] <= 0) continue;
-    const int64_t k = done[d];
-    std::vector<cdouble> y(k);
-    const cdouble* svd = sv.data() + size_t(d) * (M + 1);
-    for (int64_t j = k - 1; j >= 0; --j) {
-      cdouble acc = svd[j];
-      for (int64_t l = j + 1; l < k; ++l) acc -= Hc(d, j, l) * y[l];
-      y[j] = acc / Hc(d, j, j);
-    }
-    for (int64_t j = 0; j < k; ++j) {
-      hc[2 * (j * nd + d)] = y[j].real();
-      hc[2 * (j * nd + d) + 1] = y[j].imag();
-    }
-    out.niter[d] = k;
-    if (out.errs[size_t(d) * (M + 1) + k - 1] > eps_gmres && out.status == kOk) out.status = kNotConverged;
-  }
-  const int mused = int(std::max<int64_t>(it, 1));
-  BIE_CUDA(cudaMemcpyAsync(ws.coef.p, hc.data(), 2 * mused * nd * sizeof(double), cudaMemcpyHostToDevice, st));
-  BIE_CUDA(dev::launch_combo(V, ldv, mused, ws.coef.p, d_soln, n, nd, cplx, st));
-  if (d_x0) BIE_CUDA(dev::launch_axpby(d_x0, d_soln, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
-  // rres = || zid x + K x - rhs ||_w / ||rhs||_w   (one more matvec)
-  if (rres_precision >= 0) {
-    int ier = P.matvec(rres_precision, nd, d_soln, ws.w.p, st);
-    if (ier) return ier;
-    BIE_CUDA(dev::launch_axpby(d_soln, ws.w.p, zid.real(), zid.imag(), 1.0, 0.0, n, cplx, st));
-    BIE_CUDA(dev::launch_axpby(d_rhs, ws.w.p, -1.0, 0.0, 1.0, 0.0, n, cplx, st));
-    BIE_CUDA(dev::launch_mdot(ws.w.p, ldv, 1, ws.w.p, wts, npts, nd, cplx, ws.partial.p, nblk, d_nrm, st));
-    BIE_CUDA(cudaMemcpyAsync(hn.data(), d_nrm, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-    // ||rhs|| (the initial residual norm is ||rhs - A x0||, not ||rhs||)
-    BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, npts, nd, cplx, ws.partial.p, nblk, d_h1, st));
-    std::vector<double> hr(2 * nd);
-    BIE_CUDA(cudaMemcpyAsync(hr.data(), d_h1, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaStreamSynchronize(st));
-    for (int d = 0; d < nd; ++d) {
-      const double rn = std::sqrt(std::max(hr[2 * d], 0.0));
-      out.rres[d] = rn > 0 ? std::sqrt(std::max(hn[2 * d], 0.0)) / rn : 0.0;
-    }
-  }
-  return out.status;
-}
-
-int solve_mixed(Plan& P, int nd, cdouble zid, const double* d_rhs, const double* d_x0,
-                int64_t numit, double eps_target, double inner_floor, int max_outer,
-                double* d_soln, MixedOut& out, cudaStream_t st) {
-  const int cplx = P.cplx ? 1 : 0;
-  const int64_t npts = P.npts, n = npts * nd;
-  const int64_t ldv = n * (cplx ? 2 : 1);
-  const int nblk = std::min<int>(2 * P.num_sms, int((npts + 63) / 64) + 1);
-  // buffers live in the plan: after the first solve no call allocates (a
-  // cudaFree would synchronise the device and serialise concurrent solves)
-  DBuf<double>& r = P.mws.r;
-  DBuf<double>& d = P.mws.d;
-  DBuf<double>& partial = P.mws.partial;
-  DBuf<double>& nrm = P.mws.nrm;
-  BIE_CUDA(r.alloc(ldv));
-  BIE_CUDA(d.alloc(ldv));
-  BIE_CUDA(partial.alloc(size_t(2) * nd * nblk));
-  BIE_CUDA(nrm.alloc(size_t(4) * nd));
-  out.inner_iters.assign(nd, 0);
-  out.outer.assign(nd, 0);
-  out.rres.assign(nd, 1.0);
-  out.fp64_matvecs = out.fp32_matvecs = 0;
-  out.status = kOk;
-  const double* wts = P.d_wts();
-  // ||rhs||_w per system
-  std::vector<double> hb(2 * nd), hr(2 * nd);
-  BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, npts, nd, cplx, partial.p, nblk, nrm.p, st));
-  BIE_CUDA(cudaMemcpyAsync(hb.data(), nrm.p, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-  // x = x0 or 0; r = rhs - (zid x + K x).  The residual of a guess is taken
-  // with the FP32 operator: it only seeds the first correction, and every
-  // convergence decision below is made on an FP64 residual.
-  bool r_is_f64 = true;
-  std::vector<double> bn(nd);
-  if (d_x0) {
-    BIE_CUDA(cudaMemcpyAsync(d_soln, d_x0, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    int ier = P.matvec(1, nd, d_soln, r.p, st);
-    if (ier) return ier;
-    ++out.fp32_matvecs;
-    BIE_CUDA(dev::launch_axpby(d_soln, r.p, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
-    BIE_CUDA(dev::launch_axpby(d_rhs, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
-    r_is_f64 = false;
-    // fallback per system: a guess whose residual is not below ||rhs|| is
-    // replaced by zero (x = 0, r = rhs)
-    BIE_CUDA(dev::launch_mdot(r.p, ldv, 1, r.p, wts, npts, nd, cplx, partial.p, nblk, nrm.p, st));
-    BIE_CUDA(cudaMemcpyAsync(hr.data(), nrm.p, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaStreamSynchronize(st));
-    std::vector<double> keep(2 * nd, 0.0), drop(2 * nd, 0.0);
-    bool any_drop = false;
-    out.x0_dropped.assign(nd, 0);
-    for (int q = 0; q < nd; ++q) {
-      const double b = std::sqrt(std::max(hb[2 * q], 0.0));
-      const double rr = std::sqrt(std::max(hr[2 * q], 0.0));
-      const bool ok = rr < b;
-      keep[2 * q] = ok ? 1.0 : 0.0;
-      drop[2 * q] = ok ? 0.0 : 1.0;
-      if (!ok) {
-        any_drop = true;
-        out.x0_dropped[q] = 1;
-      }
-    }
-    if (any_drop) {
-      double* s = nrm.p + 2 * nd;
-      BIE_CUDA(cudaMemcpyAsync(s, keep.data(), 2 * nd * sizeof(double), cudaMemcpyHostToDevice, st));
-      BIE_CUDA(dev::launch_dscale(d_soln, d_soln, s, n, nd, cplx, st));
-      BIE_CUDA(dev::launch_dscale(r.p, r.p, s, n, nd, cplx, st));
-      BIE_CUDA(cudaStreamSynchronize(st));
-      BIE_CUDA(cudaMemcpyAsync(s, drop.data(), 2 * nd * sizeof(double), cudaMemcpyHostToDevice, st));
-      BIE_CUDA(dev::launch_dscale(d_rhs, d.p, s, n, nd, cplx, st));
-      BIE_CUDA(dev::launch_axpby(d.p, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
-    }
-  } else {
-    BIE_CUDA(cudaMemsetAsync(d_soln, 0, ldv * sizeof(double), st));
-    BIE_CUDA(cudaMemcpyAsync(r.p, d_rhs, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  }
-  BIE_CUDA(cudaStreamSynchronize(st));
-  for (int q = 0; q < nd; ++q) bn[q] = std::sqrt(std::max(hb[2 * q], 0.0));
-  for (int outer = 0; outer <= max_outer; ++outer) {
-    BIE_CUDA(dev::launch_mdot(r.p, ldv, 1, r.p, wts, npts, nd, cplx, partial.p, nblk, nrm.p, st));
-    BIE_CUDA(cudaMemcpyAsync(hr.data(), nrm.p, 2 * nd * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaStreamSynchronize(st));
-    double worst_ratio = 0.0;
-    bool all_done = true;
-    for (int q = 0; q < nd; ++q) {
-      const double rel = bn[q] > 0 ? std::sqrt(std::max(hr[2 * q], 0.0)) / bn[q] : 0.0;
-      out.rres[q] = rel;
-      if (rel > eps_target) {
-        all_done = false;
-        worst_ratio = std::max(worst_ratio, eps_target / rel);
-      }
-    }
-    if (!r_is_f64 && all_done) {
-      // the guess already meets the target in FP32: confirm it in FP64
-      int ier = P.matvec(0, nd, d_soln, r.p, st);
-      if (ier) return ier;
-      ++out.fp64_matvecs;
-      BIE_CUDA(dev::launch_axpby(d_soln, r.p, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
-      BIE_CUDA(dev::launch_axpby(d_rhs, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
-      r_is_f64 = true;
-      continue;
-    }
-    if (r_is_f64 && (all_done || outer == max_outer)) {
-      if (!all_done) out.status = kNotConverged;
-      break;
-    }
-    // inner relative tolerance: what this step must gain, not below the
-    // accuracy the f32 operator can deliver
-    const double tol = std::max(inner_floor, 0.5 * worst_ratio);
-    GmresOut go;
-    int ier = gmres(P, 1, -1, nd, zid, r.p, nullptr, numit, tol, d.p, go, st);
-    if (ier && ier != kNotConverged) return ier;
-    int64_t maxit = 0;
-    for (int q = 0; q < nd; ++q) {
-      out.inner_iters[q] += go.niter[q];
-      out.outer[q] += 1;
-      maxit = std::max(maxit, go.niter[q]);
-    }
-    out.fp32_matvecs += int(maxit);
-    // x += d ; r = rhs - (zid x + K x) in f64
-    BIE_CUDA(dev::launch_axpby(d.p, d_soln, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
-    ier = P.matvec(0, nd, d_soln, r.p, st);
-    if (ier) return ier;
-    ++out.fp64_matvecs;
-    BIE_CUDA(dev::launch_axpby(d_soln, r.p, -zid.real(), -zid.imag(), -1.0, 0.0, n, cplx, st));
-    BIE_CUDA(dev::launch_axpby(d_rhs, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
-    r_is_f64 = true;
-  }
-  return out.status;
 }
 
 }  // namespace bie

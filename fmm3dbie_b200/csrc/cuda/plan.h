@@ -127,11 +127,42 @@ struct StageTimes {
   int64_t calls[2] = {0, 0};
 };
 
-class Plan {
+// A linear operator K of the second-kind systems (zid I + K) x = b.
+// Vectors hold `nodes` nodes x nd densities (point-major).  The nodes form
+// segments (the surfaces of a batch, one for a single plan): system
+// (segment g, density d) is independent of the others, so the solvers run
+// nseg * nd systems with their own inner products, Hessenberg matrices and
+// stopping tests.
+class Operator {
  public:
-  int kind = 0;
+  virtual ~Operator() = default;
+  // y = K x for nd densities; precision 0 = f64, 1 = f32 far field + f32 W_eff.
+  virtual int apply(int precision, int nd, const double* x, double* y, cudaStream_t st) = 0;
+  // whether the operator maps node values to node values (GMRES needs it)
+  virtual bool square() const = 0;
+
   bool cplx = false;
   int device = 0, num_sms = 148;
+  int64_t nodes = 0;                      // rows per density
+  const double* d_node_wts = nullptr;     // smooth quadrature weight per node (device)
+  std::vector<int64_t> seg_start{0, 0};   // host, nseg + 1 node offsets
+  int nseg() const { return int(seg_start.size()) - 1; }
+  // device reduction tables for seg_start (chunks of about nodes/(2 SMs));
+  // call after seg_start and nodes are set
+  int init_segments(cudaStream_t st);
+  dev::Segs segs;
+
+  GmresWorkspace gws;  // reused across solves
+  MixedWorkspace mws;
+
+ private:
+  DBuf<int64_t> chunk_lo_, chunk_hi_;
+  DBuf<int32_t> seg_chunk0_, node_seg_;
+};
+
+class Plan : public Operator {
+ public:
+  int kind = 0;
   dev::KParams kp;
   dev::Geometry g;
   dev::Near nr;
@@ -142,6 +173,10 @@ class Plan {
   // pot = K sigma (principal value, no identity term), nd densities,
   // precision 0 = f64, 1 = f32 far field + f32 W_eff.
   int matvec(int precision, int nd, const double* d_sigma, double* d_pot, cudaStream_t st);
+  int apply(int precision, int nd, const double* x, double* y, cudaStream_t st) override {
+    return matvec(precision, nd, x, y, st);
+  }
+  bool square() const override { return targets_on_surface && ntarg == npts; }
   int nchunks_for(int precision, int nd) const;
 
   // Far-kernel launch shape: block-shape variant and number of source
@@ -154,9 +189,6 @@ class Plan {
   };
   FarConfig far_config(int precision, int nd) const;
   const double* d_wts() const { return wts_.p; }
-
-  GmresWorkspace gws;  // reused across solves on this plan
-  MixedWorkspace mws;
 
   // per-stage timing with CUDA events on the launch stream (off by default)
   bool timing = false;
@@ -186,14 +218,16 @@ struct GmresOut {
   int status = kOk;
 };
 
-// Unrestarted GMRES on (zid I + K) x = rhs for nd independent systems
-// (zgmres_guru / dgmres_guru semantics, gmres_routs.f90:13-375, with
-// classical Gram-Schmidt applied twice in place of modified Gram-Schmidt).
-// The inner matvec uses `precision`; the final relative residual rres uses
-// `rres_precision` (-1 skips it).  d_x0 (optional) is an initial guess.
-int gmres(Plan& P, int precision, int rres_precision, int nd, cdouble zid, const double* d_rhs,
-          const double* d_x0, int64_t numit, double eps_gmres, double* d_soln, GmresOut& out,
-          cudaStream_t st);
+// Unrestarted GMRES on (zid I + K) x = rhs for the operator's nseg * nd
+// independent systems (zgmres_guru / dgmres_guru semantics,
+// gmres_routs.f90:13-375, with classical Gram-Schmidt applied twice in
+// place of modified Gram-Schmidt).  zid has one value per system
+// (system = segment * nd + density).  The inner matvec uses `precision`;
+// the final relative residual rres uses `rres_precision` (-1 skips it).
+// d_x0 (optional) is an initial guess.
+int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble* zid,
+          const double* d_rhs, const double* d_x0, int64_t numit, double eps_gmres,
+          double* d_soln, GmresOut& out, cudaStream_t st);
 
 // Mixed-precision solve: FP64 residuals and iterative refinement around
 // FP32-matvec GMRES inner solves.  Stops when the FP64 relative residual
@@ -206,7 +240,7 @@ struct MixedOut {
   int fp64_matvecs = 0, fp32_matvecs = 0;
   int status = kOk;
 };
-int solve_mixed(Plan& P, int nd, cdouble zid, const double* d_rhs, const double* d_x0,
+int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, const double* d_x0,
                 int64_t numit, double eps_target, double inner_floor, int max_outer,
                 double* d_soln, MixedOut& out, cudaStream_t st);
 

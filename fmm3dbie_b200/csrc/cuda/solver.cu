@@ -1,0 +1,418 @@
+// GMRES and the mixed-precision refinement solver on an Operator: a single
+// plan (one segment) or a batch of surfaces (one segment per surface).  Every
+// system (segment, density) has its own inner products, Hessenberg matrix,
+// Givens rotations and stopping test; all systems share every launch.
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "plan.h"
+
+namespace bie {
+
+namespace {
+
+#define BIE_CUDA(call)                                                             \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));          \
+      return e_ == cudaErrorMemoryAllocation ? kErrNoMem : kErrCuda;               \
+    }                                                                              \
+  } while (0)
+
+// zrotmat_gmres (rotmat_gmres.f:60-100)
+inline void rotmat(cdouble a, cdouble b, cdouble& c, cdouble& s) {
+  if (a == cdouble(0)) {
+    s = 1.0;
+    c = 0.0;
+  } else {
+    const cdouble t = b / a;
+    c = 1.0 / std::sqrt(1.0 + std::norm(t));
+    s = t * c;
+  }
+}
+
+// host complex per system -> interleaved doubles
+std::vector<double> interleave(const std::vector<cdouble>& v) {
+  std::vector<double> o(2 * v.size());
+  for (size_t i = 0; i < v.size(); ++i) {
+    o[2 * i] = v[i].real();
+    o[2 * i + 1] = v[i].imag();
+  }
+  return o;
+}
+
+}  // namespace
+
+int Operator::init_segments(cudaStream_t st) {
+  const int ns = nseg();
+  if (ns < 1 || seg_start.front() != 0 || seg_start.back() != nodes) {
+    set_last_error("segment table inconsistent with the node count");
+    return kErrArg;
+  }
+  // chunks of about nodes / (2 SMs), at least 64 nodes, never across segments
+  const int64_t target = std::max<int64_t>(64, nodes / std::max(1, 2 * num_sms));
+  std::vector<int64_t> lo, hi;
+  std::vector<int32_t> c0(ns + 1, 0);
+  for (int g = 0; g < ns; ++g) {
+    c0[g] = int32_t(lo.size());
+    const int64_t a = seg_start[g], b = seg_start[g + 1];
+    const int64_t nc = std::max<int64_t>(1, (b - a + target - 1) / target);
+    for (int64_t c = 0; c < nc; ++c) {
+      lo.push_back(a + (b - a) * c / nc);
+      hi.push_back(a + (b - a) * (c + 1) / nc);
+    }
+  }
+  c0[ns] = int32_t(lo.size());
+  BIE_CUDA(chunk_lo_.alloc(lo.size()));
+  BIE_CUDA(chunk_hi_.alloc(hi.size()));
+  BIE_CUDA(seg_chunk0_.alloc(c0.size()));
+  BIE_CUDA(cudaMemcpyAsync(chunk_lo_.p, lo.data(), lo.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(cudaMemcpyAsync(chunk_hi_.p, hi.data(), hi.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(cudaMemcpyAsync(seg_chunk0_.p, c0.data(), c0.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  segs.nseg = ns;
+  segs.nchunk = int(lo.size());
+  segs.chunk_lo = chunk_lo_.p;
+  segs.chunk_hi = chunk_hi_.p;
+  segs.seg_chunk0 = seg_chunk0_.p;
+  segs.node_seg = nullptr;
+  if (ns > 1) {
+    std::vector<int32_t> ns_of(nodes);
+    for (int g = 0; g < ns; ++g)
+      for (int64_t i = seg_start[g]; i < seg_start[g + 1]; ++i) ns_of[i] = g;
+    BIE_CUDA(node_seg_.alloc(ns_of.size()));
+    BIE_CUDA(cudaMemcpyAsync(node_seg_.p, ns_of.data(), ns_of.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    segs.node_seg = node_seg_.p;
+  }
+  // the host vectors above are pageable: finish the copies before they go
+  BIE_CUDA(cudaStreamSynchronize(st));
+  return kOk;
+}
+
+int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble* zid,
+          const double* d_rhs, const double* d_x0, int64_t numit, double eps_gmres,
+          double* d_soln, GmresOut& out, cudaStream_t st) {
+  if (!P.square()) {
+    set_last_error("GMRES needs an operator whose targets are its nodes");
+    return kErrArg;
+  }
+  if (numit < 1 || nd < 1 || nd > 256) return kErrArg;
+  const int cplx = P.cplx ? 1 : 0;
+  const dev::Segs& sg = P.segs;
+  const int nsys = sg.nseg * nd;
+  const int64_t n = P.nodes * nd;
+  const int64_t ldv = n * (cplx ? 2 : 1);
+  GmresWorkspace& ws = P.gws;
+  BIE_CUDA(ws.V.alloc(size_t(ldv) * (numit + 1)));
+  BIE_CUDA(ws.w.alloc(size_t(ldv)));
+  BIE_CUDA(ws.partial.alloc(size_t(2) * (numit + 1) * nd * sg.nchunk));
+  BIE_CUDA(ws.dots.alloc(size_t(2) * 3 * (numit + 1) * nsys));
+  BIE_CUDA(ws.coef.alloc(size_t(2) * (numit + 1) * nsys));
+  BIE_CUDA(ws.scale.alloc(size_t(2) * 2 * nsys));
+  double* d_h1 = ws.dots.p;
+  double* d_h2 = ws.dots.p + 2 * (numit + 1) * nsys;
+  double* d_nrm = ws.dots.p + 4 * (numit + 1) * nsys;
+  double* d_zid = ws.scale.p + 2 * nsys;  // zid per system
+  const double* wts = P.d_node_wts;
+  double* V = ws.V.p;
+  std::vector<cdouble> zv(zid, zid + nsys);
+  {
+    const std::vector<double> zh = interleave(zv);
+    BIE_CUDA(cudaMemcpyAsync(d_zid, zh.data(), zh.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  // residual start: r0 = rhs - (zid x0 + K x0)  (stored in V_0 before scaling)
+  if (d_x0) {
+    int ier = P.apply(precision, nd, d_x0, V, st);
+    if (ier) return ier;
+    // V0 = zid x0 + K x0, then V0 = rhs - V0
+    BIE_CUDA(dev::launch_axpbys(d_x0, V, d_zid, 1.0, 0.0, n, nd, cplx, sg, st));
+    BIE_CUDA(dev::launch_axpby(d_rhs, V, 1.0, 0.0, -1.0, 0.0, n, cplx, st));
+  } else {
+    BIE_CUDA(cudaMemcpyAsync(V, d_rhs, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  BIE_CUDA(dev::launch_mdot(V, ldv, 1, V, wts, nd, cplx, sg, ws.partial.p, d_nrm, st));
+  std::vector<double> hbuf(2 * nsys);
+  BIE_CUDA(cudaMemcpyAsync(hbuf.data(), d_nrm, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+  BIE_CUDA(cudaStreamSynchronize(st));
+  std::vector<double> rb(nsys), bnorm(nsys);
+  std::vector<double> hscale(2 * nsys, 0.0);
+  for (int q = 0; q < nsys; ++q) {
+    rb[q] = std::sqrt(std::max(hbuf[2 * q], 0.0));
+    hscale[2 * q] = rb[q] > 0 ? 1.0 / rb[q] : 0.0;
+    bnorm[q] = rb[q];
+  }
+  // With an initial guess the stopping test stays relative to ||rhs||_w, so a
+  // warm-started solve meets the same accuracy as one from zero.
+  if (d_x0) {
+    BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, nd, cplx, sg, ws.partial.p, d_nrm, st));
+    std::vector<double> hb(2 * nsys);
+    BIE_CUDA(cudaMemcpyAsync(hb.data(), d_nrm, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    for (int q = 0; q < nsys; ++q) bnorm[q] = std::sqrt(std::max(hb[2 * q], 0.0));
+  }
+  BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(dev::launch_dscale(V, V, ws.scale.p, n, nd, cplx, sg, st));
+  // per-system Hessenberg columns, rotations and residual vector
+  const int64_t M = numit;
+  std::vector<cdouble> H(size_t(nsys) * (M + 1) * M), cs(size_t(nsys) * M), sn(size_t(nsys) * M),
+      sv(size_t(nsys) * (M + 1));
+  std::vector<int64_t> done(nsys, 0);
+  out.niter.assign(nsys, 0);
+  out.errs.assign(size_t(nsys) * (M + 1), 0.0);
+  out.rres.assign(nsys, 0.0);
+  out.status = kOk;
+  int nactive = 0;
+  for (int q = 0; q < nsys; ++q) {
+    sv[size_t(q) * (M + 1)] = rb[q];
+    if (rb[q] == 0.0) done[q] = -1;  // zero right-hand side: solution 0
+    else ++nactive;
+  }
+  auto Hc = [&](int q, int64_t row, int64_t col) -> cdouble& {
+    return H[(size_t(q) * M + col) * (M + 1) + row];
+  };
+  std::vector<double> hh1(2 * (M + 1) * nsys), hh2(2 * (M + 1) * nsys), hn(2 * nsys);
+  int64_t it = 0;
+  for (; it < M && nactive > 0; ++it) {
+    double* vit = V + size_t(it) * ldv;
+    double* vnext = V + size_t(it + 1) * ldv;
+    int ier = P.apply(precision, nd, vit, ws.w.p, st);
+    if (ier) return ier;
+    const int m = int(it + 1);
+    BIE_CUDA(dev::launch_mdot(V, ldv, m, ws.w.p, wts, nd, cplx, sg, ws.partial.p, d_h1, st));
+    BIE_CUDA(dev::launch_maxpy(V, ldv, m, d_h1, ws.w.p, n, nd, cplx, sg, st));
+    BIE_CUDA(dev::launch_mdot(V, ldv, m, ws.w.p, wts, nd, cplx, sg, ws.partial.p, d_h2, st));
+    BIE_CUDA(dev::launch_maxpy(V, ldv, m, d_h2, ws.w.p, n, nd, cplx, sg, st));
+    BIE_CUDA(dev::launch_mdot(ws.w.p, ldv, 1, ws.w.p, wts, nd, cplx, sg, ws.partial.p, d_nrm, st));
+    BIE_CUDA(cudaMemcpyAsync(hh1.data(), d_h1, 2 * m * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaMemcpyAsync(hh2.data(), d_h2, 2 * m * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaMemcpyAsync(hn.data(), d_nrm, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    for (int q = 0; q < nsys; ++q) {
+      hscale[2 * q] = 0.0;
+      hscale[2 * q + 1] = 0.0;
+      if (done[q] != 0) continue;
+      for (int k = 0; k < m; ++k)
+        Hc(q, k, it) = cdouble(hh1[2 * (k * nsys + q)] + hh2[2 * (k * nsys + q)],
+                               hh1[2 * (k * nsys + q) + 1] + hh2[2 * (k * nsys + q) + 1]);
+      Hc(q, it, it) += zv[q];
+      const double wnrm = std::sqrt(std::max(hn[2 * q], 0.0));
+      cdouble* c = cs.data() + size_t(q) * M;
+      cdouble* s = sn.data() + size_t(q) * M;
+      cdouble* svq = sv.data() + size_t(q) * (M + 1);
+      for (int64_t k = 0; k < it; ++k) {
+        const cdouble t = c[k] * Hc(q, k, it) + std::conj(s[k]) * Hc(q, k + 1, it);
+        Hc(q, k + 1, it) = -s[k] * Hc(q, k, it) + c[k] * Hc(q, k + 1, it);
+        Hc(q, k, it) = t;
+      }
+      rotmat(Hc(q, it, it), cdouble(wnrm), c[it], s[it]);
+      Hc(q, it, it) = c[it] * Hc(q, it, it) + std::conj(s[it]) * wnrm;
+      svq[it + 1] = -s[it] * svq[it];
+      svq[it] = c[it] * svq[it];
+      const double err = bnorm[q] > 0 ? std::abs(svq[it + 1]) / bnorm[q] : 0.0;
+      out.errs[size_t(q) * (M + 1) + it] = err;
+      if (!(err == err) || !(wnrm == wnrm)) {
+        out.status = kBreakdown;
+        done[q] = it + 1;
+        --nactive;
+        continue;
+      }
+      if (err <= eps_gmres || it == M - 1 || wnrm == 0.0) {
+        done[q] = it + 1;
+        --nactive;
+        continue;
+      }
+      hscale[2 * q] = 1.0 / wnrm;
+    }
+    BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
+    BIE_CUDA(dev::launch_dscale(ws.w.p, vnext, ws.scale.p, n, nd, cplx, sg, st));
+  }
+  // back-substitution per system: y = triu(H)\s, soln = V y (+ x0)
+  std::vector<double> hc(size_t(2) * (M + 1) * nsys, 0.0);
+  for (int q = 0; q < nsys; ++q) {
+    if (done[q] <= 0) continue;
+    const int64_t k = done[q];
+    std::vector<cdouble> y(k);
+    const cdouble* svq = sv.data() + size_t(q) * (M + 1);
+    for (int64_t j = k - 1; j >= 0; --j) {
+      cdouble acc = svq[j];
+      for (int64_t l = j + 1; l < k; ++l) acc -= Hc(q, j, l) * y[l];
+      y[j] = acc / Hc(q, j, j);
+    }
+    for (int64_t j = 0; j < k; ++j) {
+      hc[2 * (j * nsys + q)] = y[j].real();
+      hc[2 * (j * nsys + q) + 1] = y[j].imag();
+    }
+    out.niter[q] = k;
+    if (out.errs[size_t(q) * (M + 1) + k - 1] > eps_gmres && out.status == kOk) out.status = kNotConverged;
+  }
+  const int mused = int(std::max<int64_t>(it, 1));
+  BIE_CUDA(cudaMemcpyAsync(ws.coef.p, hc.data(), 2 * mused * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(dev::launch_combo(V, ldv, mused, ws.coef.p, d_soln, n, nd, cplx, sg, st));
+  if (d_x0) BIE_CUDA(dev::launch_axpby(d_x0, d_soln, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+  // rres = || zid x + K x - rhs ||_w / ||rhs||_w   (one more matvec)
+  if (rres_precision >= 0) {
+    int ier = P.apply(rres_precision, nd, d_soln, ws.w.p, st);
+    if (ier) return ier;
+    BIE_CUDA(dev::launch_axpbys(d_soln, ws.w.p, d_zid, 1.0, 0.0, n, nd, cplx, sg, st));
+    BIE_CUDA(dev::launch_axpby(d_rhs, ws.w.p, -1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    BIE_CUDA(dev::launch_mdot(ws.w.p, ldv, 1, ws.w.p, wts, nd, cplx, sg, ws.partial.p, d_nrm, st));
+    BIE_CUDA(cudaMemcpyAsync(hn.data(), d_nrm, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+    // ||rhs|| (the initial residual norm is ||rhs - A x0||, not ||rhs||)
+    BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, nd, cplx, sg, ws.partial.p, d_h1, st));
+    std::vector<double> hr(2 * nsys);
+    BIE_CUDA(cudaMemcpyAsync(hr.data(), d_h1, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    for (int q = 0; q < nsys; ++q) {
+      const double rn = std::sqrt(std::max(hr[2 * q], 0.0));
+      out.rres[q] = rn > 0 ? std::sqrt(std::max(hn[2 * q], 0.0)) / rn : 0.0;
+    }
+  }
+  return out.status;
+}
+
+int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, const double* d_x0,
+                int64_t numit, double eps_target, double inner_floor, int max_outer,
+                double* d_soln, MixedOut& out, cudaStream_t st) {
+  if (!P.square()) {
+    set_last_error("the solver needs an operator whose targets are its nodes");
+    return kErrArg;
+  }
+  if (nd < 1 || nd > 256) return kErrArg;
+  const int cplx = P.cplx ? 1 : 0;
+  const dev::Segs& sg = P.segs;
+  const int nsys = sg.nseg * nd;
+  const int64_t n = P.nodes * nd;
+  const int64_t ldv = n * (cplx ? 2 : 1);
+  // buffers live in the operator: after the first solve no call allocates (a
+  // cudaFree would synchronise the device and serialise concurrent solves)
+  DBuf<double>& r = P.mws.r;
+  DBuf<double>& d = P.mws.d;
+  DBuf<double>& partial = P.mws.partial;
+  DBuf<double>& nrm = P.mws.nrm;
+  BIE_CUDA(r.alloc(ldv));
+  BIE_CUDA(d.alloc(ldv));
+  BIE_CUDA(partial.alloc(size_t(2) * nd * sg.nchunk));
+  BIE_CUDA(nrm.alloc(size_t(6) * nsys));
+  double* d_zid = nrm.p + 4 * nsys;  // zid per system
+  {
+    std::vector<cdouble> zv(zid, zid + nsys);
+    const std::vector<double> zh = interleave(zv);
+    BIE_CUDA(cudaMemcpyAsync(d_zid, zh.data(), zh.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  out.inner_iters.assign(nsys, 0);
+  out.outer.assign(nsys, 0);
+  out.rres.assign(nsys, 1.0);
+  out.fp64_matvecs = out.fp32_matvecs = 0;
+  out.status = kOk;
+  const double* wts = P.d_node_wts;
+  // r = rhs - (zid x + K x) from K x already in r
+  auto finish_residual = [&]() -> int {
+    BIE_CUDA(dev::launch_axpbys(d_soln, r.p, d_zid, 1.0, 0.0, n, nd, cplx, sg, st));
+    BIE_CUDA(dev::launch_axpby(d_rhs, r.p, 1.0, 0.0, -1.0, 0.0, n, cplx, st));
+    return kOk;
+  };
+  // ||rhs||_w per system
+  std::vector<double> hb(2 * nsys), hr(2 * nsys);
+  BIE_CUDA(dev::launch_mdot(d_rhs, ldv, 1, d_rhs, wts, nd, cplx, sg, partial.p, nrm.p, st));
+  BIE_CUDA(cudaMemcpyAsync(hb.data(), nrm.p, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+  // x = x0 or 0; r = rhs - (zid x + K x).  The residual of a guess is taken
+  // with the FP32 operator: it only seeds the first correction, and every
+  // convergence decision below is made on an FP64 residual.
+  bool r_is_f64 = true;
+  std::vector<double> bn(nsys);
+  out.x0_dropped.assign(nsys, 0);
+  if (d_x0) {
+    BIE_CUDA(cudaMemcpyAsync(d_soln, d_x0, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    int ier = P.apply(1, nd, d_soln, r.p, st);
+    if (ier) return ier;
+    ++out.fp32_matvecs;
+    if ((ier = finish_residual())) return ier;
+    r_is_f64 = false;
+    // fallback per system: a guess whose residual is not below ||rhs|| is
+    // replaced by zero (x = 0, r = rhs)
+    BIE_CUDA(dev::launch_mdot(r.p, ldv, 1, r.p, wts, nd, cplx, sg, partial.p, nrm.p, st));
+    BIE_CUDA(cudaMemcpyAsync(hr.data(), nrm.p, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    std::vector<double> keep(2 * nsys, 0.0), drop(2 * nsys, 0.0);
+    bool any_drop = false;
+    for (int q = 0; q < nsys; ++q) {
+      const double b = std::sqrt(std::max(hb[2 * q], 0.0));
+      const double rr = std::sqrt(std::max(hr[2 * q], 0.0));
+      const bool ok = rr < b;
+      keep[2 * q] = ok ? 1.0 : 0.0;
+      drop[2 * q] = ok ? 0.0 : 1.0;
+      if (!ok) {
+        any_drop = true;
+        out.x0_dropped[q] = 1;
+      }
+    }
+    if (any_drop) {
+      double* s = nrm.p + 2 * nsys;
+      BIE_CUDA(cudaMemcpyAsync(s, keep.data(), 2 * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
+      BIE_CUDA(dev::launch_dscale(d_soln, d_soln, s, n, nd, cplx, sg, st));
+      BIE_CUDA(dev::launch_dscale(r.p, r.p, s, n, nd, cplx, sg, st));
+      BIE_CUDA(cudaStreamSynchronize(st));
+      BIE_CUDA(cudaMemcpyAsync(s, drop.data(), 2 * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
+      BIE_CUDA(dev::launch_dscale(d_rhs, d.p, s, n, nd, cplx, sg, st));
+      BIE_CUDA(dev::launch_axpby(d.p, r.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    }
+  } else {
+    BIE_CUDA(cudaMemsetAsync(d_soln, 0, ldv * sizeof(double), st));
+    BIE_CUDA(cudaMemcpyAsync(r.p, d_rhs, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  BIE_CUDA(cudaStreamSynchronize(st));
+  for (int q = 0; q < nsys; ++q) bn[q] = std::sqrt(std::max(hb[2 * q], 0.0));
+  for (int outer = 0; outer <= max_outer; ++outer) {
+    BIE_CUDA(dev::launch_mdot(r.p, ldv, 1, r.p, wts, nd, cplx, sg, partial.p, nrm.p, st));
+    BIE_CUDA(cudaMemcpyAsync(hr.data(), nrm.p, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    double worst_ratio = 0.0;
+    bool all_done = true;
+    for (int q = 0; q < nsys; ++q) {
+      const double rel = bn[q] > 0 ? std::sqrt(std::max(hr[2 * q], 0.0)) / bn[q] : 0.0;
+      out.rres[q] = rel;
+      if (rel > eps_target) {
+        all_done = false;
+        worst_ratio = std::max(worst_ratio, eps_target / rel);
+      }
+    }
+    if (!r_is_f64 && all_done) {
+      // the guess already meets the target in FP32: confirm it in FP64
+      int ier = P.apply(0, nd, d_soln, r.p, st);
+      if (ier) return ier;
+      ++out.fp64_matvecs;
+      if ((ier = finish_residual())) return ier;
+      r_is_f64 = true;
+      continue;
+    }
+    if (r_is_f64 && (all_done || outer == max_outer)) {
+      if (!all_done) out.status = kNotConverged;
+      break;
+    }
+    // inner relative tolerance: what this step must gain, not below the
+    // accuracy the f32 operator can deliver
+    const double tol = std::max(inner_floor, 0.5 * worst_ratio);
+    GmresOut go;
+    int ier = gmres(P, 1, -1, nd, zid, r.p, nullptr, numit, tol, d.p, go, st);
+    if (ier && ier != kNotConverged) return ier;
+    int64_t maxit = 0;
+    for (int q = 0; q < nsys; ++q) {
+      out.inner_iters[q] += go.niter[q];
+      out.outer[q] += 1;
+      maxit = std::max(maxit, go.niter[q]);
+    }
+    out.fp32_matvecs += int(maxit);
+    // x += d ; r = rhs - (zid x + K x) in f64
+    BIE_CUDA(dev::launch_axpby(d.p, d_soln, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    ier = P.apply(0, nd, d_soln, r.p, st);
+    if (ier) return ier;
+    ++out.fp64_matvecs;
+    if ((ier = finish_residual())) return ier;
+    r_is_f64 = true;
+  }
+  return out.status;
+}
+
+}  // namespace bie
