@@ -619,32 +619,42 @@ def torus_leg(dev, nd=16, weights=WARMSTART_WEIGHTS):
 
 
 def uneven_leg(dev, kinds=(0, 1)):
-    """32 ellipsoids (semi-axes U(0.5,3), 80/320/1280 patches,
-    orders {4,6,8}, zk U(1,6)), 4 interior point sources each, Laplace and
-    Helmholtz batches.  Every surface solves its 4 systems as one
-    multi-density batch on its own stream; all surfaces run concurrently.
-    Reports systems solved per second for the mixed and FP64 paths and for
-    the mixed path run surface after surface."""
+    """32 ellipsoids (semi-axes U(0.5,3), 80/320/1280 patches, orders {4,6,8},
+    zk U(1,6)), 4 interior point sources each, Laplace and Helmholtz batches.
+    The graph engine runs every matvec stage of all surfaces as one
+    persistent launch replayed from a CUDA graph (each surface's 4 systems
+    share the launches); the streams engine solves each surface on its own
+    stream.  Reports systems solved per second."""
     import torch
     from fmm3dbie_b200.batch import SurfaceBatch, uneven_ellipsoids
+    from fmm3dbie_b200.surface import setup
     out = {"workload": "32 ellipsoids, npts 1200-57600, 4 point-source rhs each"}
     for kind in kinds:
         t0 = time.time()
         items, rhs, _ = uneven_ellipsoids(kind)
-        B = SurfaceBatch(items, EPS)
+        setups = [setup(it.surf, it.kind, EPS, it.params) for it in items]
         t_setup = time.time() - t0
         R = [torch.tensor(np.ascontiguousarray(r), device=dev) for r in rhs]
         nsys = sum(r.shape[1] for r in rhs)
         res = {"setup_s": round(t_setup, 1), "npts_total": int(sum(it.surf.npts for it in items)),
                "systems": nsys}
-        for mode, tag, conc in ((1, "mixed", True), (0, "fp64", True), (1, "mixed_sequential", False)):
-            B.solve(R, mode=mode, eps_gmres=TOL_RES, concurrent=conc)  # warm-up / tuning
-            _, infos, ms = B.solve(R, mode=mode, eps_gmres=TOL_RES, concurrent=conc)
+        G = SurfaceBatch(items, EPS, engine="graph", setups=setups)
+        for mode, tag in ((1, "mixed"), (0, "fp64")):
+            G.solve(R, mode=mode, eps_gmres=TOL_RES)  # warm-up / tuning / graph capture
+            _, infos, ms = G.solve(R, mode=mode, eps_gmres=TOL_RES)
             res[tag] = {"solves_per_s": nsys * 1000.0 / ms, "ms": ms,
                         "max_rres": float(max(np.max(i["rres"]) for i in infos))}
+        info = G.info()
+        res["far_variant_chunk_f32_nd1"] = [int(info[4]), int(info[5])]
+        G.close()
+        S = SurfaceBatch(items, EPS, engine="streams", setups=setups)
+        S.solve(R, mode=1, eps_gmres=TOL_RES)
+        _, infos, ms = S.solve(R, mode=1, eps_gmres=TOL_RES)
+        res["mixed_streams"] = {"solves_per_s": nsys * 1000.0 / ms, "ms": ms,
+                                "max_rres": float(max(np.max(i["rres"]) for i in infos))}
+        S.close()
         res["speedup_vs_fp64"] = res["fp64"]["ms"] / res["mixed"]["ms"]
         out["laplace" if kind == 0 else "helmholtz"] = res
-        B.close()
     return out
 
 

@@ -107,6 +107,14 @@ _SIGS = {
     "bie_farfield_dev": (C.c_int, [I64, PDBL, I64, VP, VP, VP, VP, I64, VP, DBL, I64, VP, VP]),
     "bie_farfield_dev_noalloc": (C.c_int, [I64, PDBL, I64, VP, VP, VP, VP, I64, VP, DBL, I64, VP,
                                            VP]),
+    "bie_batch_create": (C.c_int, [C.POINTER(VP)]),
+    "bie_batch_destroy": (C.c_int, [VP]),
+    "bie_batch_add": (C.c_int, [VP, VP]),
+    "bie_batch_finalize": (C.c_int, [VP, VP]),
+    "bie_batch_info": (C.c_int, [VP, PI64]),
+    "bie_batch_set_graph": (C.c_int, [VP, I64]),
+    "bie_batch_matvec": (C.c_int, [VP, I64, I64, VP, VP, VP]),
+    "bie_batch_solve": (C.c_int, [VP, I64, I64, PDBL, VP, VP, I64, DBL, VP, PI64, PDBL, PDBL, VP]),
     "bie_mlp_create": (C.c_int, [I64, C.POINTER(VP)]),
     "bie_mlp_destroy": (C.c_int, [VP]),
     "bie_mlp_info": (C.c_int, [VP, PI64]),

@@ -1,20 +1,24 @@
 """Batches of independent surfaces (uneven sizes, orders and wavenumbers).
 
-``SurfaceBatch`` keeps one device plan per surface and solves all of them
-together: every surface's GMRES runs on its own CUDA stream from its own host
-thread (the ctypes calls release the GIL), so small and large surfaces share
-the GPU concurrently instead of queueing behind each other.  Each surface may
-carry several right-hand sides, which its plan solves as one multi-density
-batch.  After the first solve of a plan no call allocates device memory, so
-the streams never serialise on a cudaFree.
+``SurfaceBatch`` solves many surfaces together.  With ``engine="graph"``
+(default) the surfaces form one device operator (``bie_batch_*``): every
+matvec stage -- strengths or oversampling, far field, near correction -- is
+one persistent launch walking a work list that spans all surfaces, the three
+launches are captured once in a CUDA graph, and GMRES runs all (surface,
+density) systems in the same launches.  With ``engine="streams"`` each surface
+keeps its own plan and solves on its own CUDA stream from its own host thread
+(the ctypes calls release the GIL).  Each surface may carry several
+right-hand sides.
 """
 from __future__ import annotations
 
+import ctypes as C
 import threading
 from dataclasses import dataclass
 
 import numpy as np
 
+from . import _lib as L
 from .plan import Plan
 from .surface import Surface, setup
 
@@ -28,26 +32,130 @@ class BatchItem:
 
 
 class SurfaceBatch:
-    def __init__(self, items, eps: float):
+    def __init__(self, items, eps: float, engine: str = "graph", setups=None):
         import torch
+        if engine not in ("graph", "streams"):
+            raise ValueError("engine must be 'graph' or 'streams'")
         self.torch = torch
+        self.engine = engine
         self.items = list(items)
-        self.setups = [setup(it.surf, it.kind, eps, it.params) for it in self.items]
+        if engine == "graph" and len({it.kind for it in self.items}) != 1:
+            raise ValueError("a graph batch needs one kernel kind for all surfaces")
+        self.setups = (list(setups) if setups is not None else
+                       [setup(it.surf, it.kind, eps, it.params) for it in self.items])
         self.plans = [Plan(it.kind, it.params, it.surf, st.near, st.over)
                       for it, st in zip(self.items, self.setups)]
         dev = torch.device("cuda", torch.cuda.current_device())
         self.device = dev
-        self.streams = [torch.cuda.Stream(dev) for _ in self.items]
+        self.npts = [it.surf.npts for it in self.items]
+        self.offsets = np.concatenate([[0], np.cumsum(self.npts)]).astype(np.int64)
+        self._b = None
+        if engine == "graph":
+            lib = L.lib()
+            h = C.c_void_p()
+            L.check(lib.bie_batch_create(C.byref(h)), "bie_batch_create")
+            self._b = h
+            for p in self.plans:
+                L.check(lib.bie_batch_add(h, p._h), "bie_batch_add")
+                p._h = None  # the batch owns it now
+            L.check(lib.bie_batch_finalize(h, self._stream()), "bie_batch_finalize")
+            self.plans = []
+        else:
+            self.streams = [torch.cuda.Stream(dev) for _ in self.items]
+
+    def _stream(self):
+        return C.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)
 
     def close(self):
+        if self._b is not None:
+            L.lib().bie_batch_destroy(self._b)
+            self._b = None
         for p in self.plans:
             p.close()
 
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        """surfaces, nodes, kind, reduction chunks, far variant and chunk
+        length kept for (f32, nd = 1)."""
+        out = np.zeros(6, np.int64)
+        L.check(L.lib().bie_batch_info(self._b, L.ptr(out)), "bie_batch_info")
+        return out
+
+    def set_graph(self, enable: bool):
+        L.check(L.lib().bie_batch_set_graph(self._b, int(enable)), "bie_batch_set_graph")
+
+    def concat(self, parts):
+        """Per-surface (npts_q, nd) tensors -> one (nodes, nd) batch vector."""
+        return self.torch.cat([p.reshape(p.shape[0], -1) for p in parts], 0).contiguous()
+
+    def split(self, x):
+        return [x[self.offsets[q]:self.offsets[q + 1]] for q in range(len(self.items))]
+
+    def matvec(self, x, iprec: int = 0, out=None):
+        """K x for the batch vector x (nodes, nd) (graph engine)."""
+        if self._b is None:
+            raise RuntimeError("matvec is available with engine='graph'")
+        nd = 1 if x.dim() == 1 else x.shape[1]
+        if out is None:
+            out = self.torch.empty_like(x)
+        L.check(L.lib().bie_batch_matvec(self._b, iprec, nd, C.c_void_p(x.data_ptr()),
+                                         C.c_void_p(out.data_ptr()), self._stream()),
+                "bie_batch_matvec")
+        return out
+
     def solve(self, rhs, mode: int = 1, numit: int = 200, eps_gmres: float = 1e-7,
-              concurrent: bool = True):
-        """rhs[q]: (npts_q, nrhs_q) device tensors.  Returns (solutions,
-        infos, device milliseconds from the first launch to the last
-        completion)."""
+              concurrent: bool = True, x0=None):
+        """rhs[q]: (npts_q, nrhs) device tensors.  Returns (solutions, infos,
+        device milliseconds from the first launch to the last completion)."""
+        if self.engine == "graph":
+            return self._solve_graph(rhs, mode, numit, eps_gmres, x0)
+        return self._solve_streams(rhs, mode, numit, eps_gmres, concurrent)
+
+    def _solve_graph(self, rhs, mode, numit, eps_gmres, x0):
+        torch = self.torch
+        nd = {r.shape[1] if r.dim() == 2 else 1 for r in rhs}
+        if len(nd) != 1:
+            raise ValueError("a graph batch needs the same number of right-hand sides per surface")
+        nd = nd.pop()
+        b = self.concat(rhs)
+        xb = torch.empty_like(b)
+        x0b = self.concat(x0) if x0 is not None else None
+        ns = len(self.items)
+        z = np.zeros(2 * ns)
+        for q, it in enumerate(self.items):
+            z[2 * q], z[2 * q + 1] = complex(it.zid).real, complex(it.zid).imag
+        niter = np.zeros(ns * nd, np.int64)
+        rres = np.zeros(ns * nd)
+        stats = np.zeros(2)
+        main = torch.cuda.current_stream(self.device)
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(main)
+        st = L.lib().bie_batch_solve(self._b, mode, nd, L.ptr(z), C.c_void_p(b.data_ptr()),
+                                     C.c_void_p(x0b.data_ptr()) if x0b is not None else None,
+                                     numit, eps_gmres, C.c_void_p(xb.data_ptr()), L.ptr(niter),
+                                     L.ptr(rres), L.ptr(stats), self._stream())
+        stop.record(main)
+        stop.synchronize()
+        if st not in (0, 3, 4):
+            L.check(st, "bie_batch_solve")
+        sols = [x.reshape(r.shape) for x, r in zip(self.split(xb), rhs)]
+        infos = []
+        for q in range(ns):
+            info = {"status": int(st), "niter": niter[q * nd:(q + 1) * nd],
+                    "rres": rres[q * nd:(q + 1) * nd]}
+            if mode == 1:
+                info["fp64_matvecs"] = int(stats[0])
+                info["fp32_matvecs"] = int(stats[1])
+            infos.append(info)
+        return sols, infos, start.elapsed_time(stop)
+
+    def _solve_streams(self, rhs, mode, numit, eps_gmres, concurrent):
         torch = self.torch
         main = torch.cuda.current_stream(self.device)
         start = torch.cuda.Event(enable_timing=True)

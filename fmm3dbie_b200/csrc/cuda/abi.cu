@@ -818,6 +818,101 @@ int bie_plan_create(int64_t kind, const double* params, int64_t npatches,
   });
 }
 
+// ---- batches of surfaces (no reference counterpart) --------------------------
+int bie_batch_create(void** batch) {
+  if (!batch) return BIE_ERR_ARG;
+  *batch = new bie::BatchPlan();
+  return BIE_OK;
+}
+
+int bie_batch_destroy(void* batch) {
+  delete static_cast<bie::BatchPlan*>(batch);
+  return BIE_OK;
+}
+
+int bie_batch_add(void* batch, void* plan) {
+  if (!batch || !plan) return BIE_ERR_ARG;
+  // on failure the caller keeps the plan
+  return static_cast<bie::BatchPlan*>(batch)->add(static_cast<bie::Plan*>(plan));
+}
+
+int bie_batch_finalize(void* batch, void* stream) {
+  if (!batch) return BIE_ERR_ARG;
+  return guarded([&] {
+    return static_cast<bie::BatchPlan*>(batch)->finalize(static_cast<cudaStream_t>(stream));
+  });
+}
+
+int bie_batch_info(void* batch, int64_t* info) {
+  if (!batch || !info) return BIE_ERR_ARG;
+  const auto* B = static_cast<const bie::BatchPlan*>(batch);
+  info[0] = int64_t(B->plans.size());
+  info[1] = B->nodes;
+  info[2] = B->kind;
+  info[3] = B->segs.nchunk;
+  int v = -1;
+  int64_t ch = 0;
+  info[4] = B->far_choice(1, 1, &v, &ch) ? v : -1;
+  info[5] = ch;
+  return BIE_OK;
+}
+
+int bie_batch_set_graph(void* batch, int64_t enable) {
+  if (!batch) return BIE_ERR_ARG;
+  static_cast<bie::BatchPlan*>(batch)->use_graph = enable != 0;
+  return BIE_OK;
+}
+
+int bie_batch_matvec(void* batch, int64_t iprec, int64_t nd, const double* x_dev, double* y_dev,
+                     void* stream) {
+  if (!batch || (iprec != 0 && iprec != 1) || nd < 1) return BIE_ERR_ARG;
+  return guarded([&] {
+    return static_cast<bie::BatchPlan*>(batch)->apply(int(iprec), int(nd), x_dev, y_dev,
+                                                      static_cast<cudaStream_t>(stream));
+  });
+}
+
+int bie_batch_solve(void* batch, int64_t mode, int64_t nd, const double* zid,
+                    const double* rhs_dev, const double* x0_dev, int64_t numit, double eps_gmres,
+                    double* soln_dev, int64_t* niter, double* rres, double* stats, void* stream) {
+  if (!batch || (mode != 0 && mode != 1) || nd < 1 || nd > 256 || numit < 1 || !zid)
+    return BIE_ERR_ARG;
+  return guarded([&] {
+    bie::BatchPlan& B = *static_cast<bie::BatchPlan*>(batch);
+    const int ns = B.nseg();
+    std::vector<cdouble> z(size_t(ns) * nd);
+    for (int g = 0; g < ns; ++g)
+      for (int64_t d = 0; d < nd; ++d) z[size_t(g) * nd + d] = cdouble(zid[2 * g], zid[2 * g + 1]);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t nsys = z.size();
+    if (mode == 0) {
+      bie::GmresOut go;
+      const int s = bie::gmres(B, 0, 0, int(nd), z.data(), rhs_dev, x0_dev, numit, eps_gmres,
+                               soln_dev, go, st);
+      if (s == BIE_OK || s == BIE_NOT_CONVERGED || s == BIE_BREAKDOWN)
+        for (size_t q = 0; q < nsys; ++q) {
+          if (niter) niter[q] = go.niter[q];
+          if (rres) rres[q] = go.rres[q];
+        }
+      return s;
+    }
+    bie::MixedOut mo;
+    const int s = bie::solve_mixed(B, int(nd), z.data(), rhs_dev, x0_dev, numit, eps_gmres, 1e-5, 6,
+                                   soln_dev, mo, st);
+    if (s == BIE_OK || s == BIE_NOT_CONVERGED) {
+      for (size_t q = 0; q < nsys; ++q) {
+        if (niter) niter[q] = mo.inner_iters[q];
+        if (rres) rres[q] = mo.rres[q];
+      }
+      if (stats) {
+        stats[0] = mo.fp64_matvecs;
+        stats[1] = mo.fp32_matvecs;
+      }
+    }
+    return s;
+  });
+}
+
 int bie_plan_destroy(void* plan) {
   delete static_cast<bie::Plan*>(plan);
   return BIE_OK;

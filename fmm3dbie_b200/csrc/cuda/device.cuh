@@ -165,6 +165,50 @@ cudaError_t launch_axpbys(const double* x, double* y, const double* a, double br
 cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
                          int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st);
 
+// ---- batched matvec: the surfaces of a batch in one launch per stage -------
+// One surface as the batched kernels see it.  Vector slices of the surface
+// start at node vofs (input and output: the targets are the nodes), its
+// oversampled sources at sofs in the batch strength array, its far partial
+// sums at pofs[precision] (doubles) with nchunks[precision] chunks of
+// chunk_len[precision] sources.
+struct BatchSurf {
+  Geometry g;
+  Near nr;
+  KParams kp;
+  const void* weff[2] = {nullptr, nullptr};  // W_eff: double* (f64), float* (f32)
+  const void* ab[2] = {nullptr, nullptr};    // per-source (a, b) per precision
+  int64_t vofs = 0, sofs = 0;
+  int64_t pofs[2] = {0, 0};
+  int64_t chunk_len[2] = {0, 0};
+  int nchunks[2] = {0, 0};
+};
+
+struct BatchArgs {
+  int kind = 0, precision = 0, nd = 1, variant = 0;
+  bool ck = false;                         // some surface has a complex wavenumber
+  const BatchSurf* surfs = nullptr;        // device table
+  const int2* patch_items = nullptr;       // (surface, patch)
+  const int4* far_items = nullptr;         // (surface, target block, source chunk, density group)
+  const int2* row_items = nullptr;         // (surface, group of 8 target rows)
+  int npatch_items = 0, nfar_items = 0, nrow_items = 0;
+  const double* const* xref = nullptr;     // device slot holding the input vector pointer
+  double* const* yref = nullptr;           // device slot holding the output vector pointer
+  void* str = nullptr;                     // strengths (nd == 1) or oversampled densities
+  double* partial = nullptr;
+  int grid_patch = 1, grid_far = 1, grid_row = 1;  // persistent grid sizes
+  int max_np = 0;
+};
+// Strengths/oversampling, far field and combine of every surface: three
+// persistent launches, each walking its work list.  Reads the vector
+// pointers from xref/yref when it runs (so the launches can be captured in
+// a CUDA graph once and replayed for any vectors).
+cudaError_t launch_batch_matvec(const BatchArgs& a, cudaStream_t st);
+// Far-kernel shape used by the batch: targets per block and densities per
+// block group for (precision, variant, nd); blocks per SM of the kernel.
+void batch_far_shape(int precision, int variant, int nd, int* targets_per_block, int* group);
+int batch_far_blocks_per_sm(int kind, int precision, int variant, int nd, bool ck);
+int batch_far_variants(int precision, int nd);
+
 // Number of kernels this library has launched in the process.
 int64_t launch_count();
 // Adds n launches made by kernels defined outside kernels.cu to that count.

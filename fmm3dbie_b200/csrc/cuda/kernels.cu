@@ -47,10 +47,9 @@ struct Vec<double> {
 // (a) strengths
 // ---------------------------------------------------------------------------
 template <typename R, int CPLX>
-__global__ void strengths_kernel(Geometry g, KParams kp, const double* __restrict__ sigma,
-                                 R* __restrict__ str, int nd) {
-  extern __shared__ double sh[];
-  const int p = blockIdx.x;
+__device__ __forceinline__ void strengths_body(const Geometry& g, const KParams& kp,
+                                               const double* __restrict__ sigma,
+                                               R* __restrict__ str, int nd, int p, double* sh) {
   const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
   const int os = g.ostart[p], nf = g.ostart[p + 1] - os;
   const double* M = g.imat + g.cmoff[g.pclass[p]];
@@ -83,6 +82,13 @@ __global__ void strengths_kernel(Geometry g, KParams kp, const double* __restric
       str[2 * o + 1] = R(kp.br * sr * f);
     }
   }
+}
+
+template <typename R, int CPLX>
+__global__ void strengths_kernel(Geometry g, KParams kp, const double* __restrict__ sigma,
+                                 R* __restrict__ str, int nd) {
+  extern __shared__ double sh[];
+  strengths_body<R, CPLX>(g, kp, sigma, str, nd, blockIdx.x, sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -208,25 +214,21 @@ __device__ __forceinline__ void pair_lap(R tx, R ty, R tz, const typename Vec<R>
   p = fma(e, rinv, p);
 }
 
+// One block's work of the far field: target block bx (NT*TPT targets),
+// source chunk by (chunk_len sources), density bz.  Shared tiles and the
+// FP64 trig table come from the calling kernel.
 template <int KIND, typename R, int NT, int TPT, int TILE, bool CK>
-__global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R* __restrict__ str,
-                                                 double* __restrict__ partial, int64_t chunk_len,
-                                                 int nd) {
+__device__ __forceinline__ void far_block(const Geometry& g, const KParams& kp,
+                                          const R* __restrict__ str, double* __restrict__ partial,
+                                          int64_t chunk_len, int nd, int64_t bx, int64_t by, int bz,
+                                          const double2* tab, typename Vec<R>::T4* sg0,
+                                          typename Vec<R>::T2* sg1, R* sst) {
   using R2 = typename Vec<R>::T2;
   using R4 = typename Vec<R>::T4;
   constexpr int SW = (KIND == 1) ? 4 : 2;  // strength reals per source
-  __shared__ R4 sg0[TILE];
-  __shared__ R2 sg1[TILE];
-  __shared__ R sst[TILE * SW];
-  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
-  const double2* tab = nullptr;
-  if constexpr (sizeof(R) == 8 && KIND == 1) {
-    fill_trig_table(stab);  // published by the first __syncthreads of the tile loop
-    tab = stab;
-  }
   const int64_t ntarg = g.ntarg, nptso = g.nptso;
-  const int64_t tbase = int64_t(blockIdx.x) * NT * TPT;
-  const int m = blockIdx.z;  // density index
+  const int64_t tbase = int64_t(bx) * NT * TPT;
+  const int m = bz;  // density index
   // Coordinates are shifted by the block's first target so that nearby
   // pairs keep their relative accuracy in single precision.
   const int64_t tc = tbase < ntarg ? tbase : ntarg - 1;
@@ -250,8 +252,8 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
   const bool boxes = sizeof(R) == 4 && NT * TPT == kFarBlockTargets32 && g.sbox && g.tbox;
   if (boxes)
 #pragma unroll
-    for (int c = 0; c < 6; ++c) tbx[c] = g.tbox[6 * blockIdx.x + c];
-  const int64_t s0 = int64_t(blockIdx.y) * chunk_len;
+    for (int c = 0; c < 6; ++c) tbx[c] = g.tbox[6 * bx + c];
+  const int64_t s0 = int64_t(by) * chunk_len;
   const int64_t s1 = min(s0 + chunk_len, nptso);
   for (int64_t sb = s0; sb < s1; sb += TILE) {
     const int ns = int((s1 - sb) < TILE ? (s1 - sb) : TILE);
@@ -332,7 +334,7 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
   for (int t = 0; t < TPT; ++t) {
     const int64_t it = tbase + threadIdx.x + int64_t(t) * NT;
     if (it >= ntarg) continue;
-    const size_t o = (size_t(blockIdx.y) * ntarg + it) * nd + m;
+    const size_t o = (size_t(by) * ntarg + it) * nd + m;
     if (KIND == 1) {
       partial[2 * o] = accr[t];
       partial[2 * o + 1] = acci[t];
@@ -340,6 +342,25 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
       partial[o] = accr[t];
     }
   }
+}
+
+
+template <int KIND, typename R, int NT, int TPT, int TILE, bool CK>
+__global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R* __restrict__ str,
+                                                 double* __restrict__ partial, int64_t chunk_len,
+                                                 int nd) {
+  constexpr int SW = (KIND == 1) ? 4 : 2;
+  __shared__ typename Vec<R>::T4 sg0[TILE];
+  __shared__ typename Vec<R>::T2 sg1[TILE];
+  __shared__ R sst[TILE * SW];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  const double2* tab = nullptr;
+  if constexpr (sizeof(R) == 8 && KIND == 1) {
+    fill_trig_table(stab);  // published by the first __syncthreads of the tile loop
+    tab = stab;
+  }
+  far_block<KIND, R, NT, TPT, TILE, CK>(g, kp, str, partial, chunk_len, nd, blockIdx.x, blockIdx.y,
+                                        blockIdx.z, tab, sg0, sg1, sst);
 }
 
 // ---------------------------------------------------------------------------
@@ -356,29 +377,23 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
 // ---------------------------------------------------------------------------
 constexpr int kMdCentre = 512;
 
+// One block's work of the multi-density far field: target block bx, source
+// chunk by, density group bz (MD densities).  Shared tiles and the FP64 trig
+// table come from the calling kernel.
 template <int KIND, typename R, int NT, int TPT, int MD, int TILE, bool CK>
-__global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
-                                                    const R* __restrict__ ab,
-                                                    const R* __restrict__ sig, int nd,
-                                                    double* __restrict__ partial,
-                                                    int64_t chunk_len) {
+__device__ __forceinline__ void far_md_block(const Geometry& g, const KParams& kp,
+                                             const R* __restrict__ ab, const R* __restrict__ sig,
+                                             int nd, double* __restrict__ partial,
+                                             int64_t chunk_len, int64_t bx, int64_t by, int bz,
+                                             const double2* tab, typename Vec<R>::T4* sg0,
+                                             typename Vec<R>::T2* sg1, R* sab, R* ssig) {
   using R2 = typename Vec<R>::T2;
   using R4 = typename Vec<R>::T4;
   constexpr int C = (KIND == 1) ? 2 : 1;  // reals per complex value
   static_assert(MD % 2 == 0, "densities are read from shared memory two at a time");
-  __shared__ R4 sg0[TILE];
-  __shared__ R2 sg1[TILE];
-  __shared__ __align__(16) R sab[TILE * 2 * C];
-  __shared__ __align__(16) R ssig[TILE * MD * C];
-  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
-  const double2* tab = nullptr;
-  if constexpr (sizeof(R) == 8 && KIND == 1) {
-    fill_trig_table(stab);  // published by the first __syncthreads of the tile loop
-    tab = stab;
-  }
   const int64_t ntarg = g.ntarg, nptso = g.nptso;
-  const int64_t tbase = int64_t(blockIdx.x) * NT * TPT;
-  const int m0 = blockIdx.z * MD;
+  const int64_t tbase = int64_t(bx) * NT * TPT;
+  const int m0 = bz * MD;
   const int64_t tcen = (tbase / kMdCentre) * kMdCentre;
   const int64_t tc = tcen < ntarg ? tcen : ntarg - 1;
   const double cx = g.tx[tc], cy = g.ty[tc], cz = g.tz[tc];
@@ -398,7 +413,7 @@ __global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
   }
   const R thr2 = R(kp.thresh * kp.thresh);
   const R k = R(kp.kr), kim = R(kp.ki);
-  const int64_t s0 = int64_t(blockIdx.y) * chunk_len;
+  const int64_t s0 = int64_t(by) * chunk_len;
   const int64_t s1 = min(s0 + chunk_len, nptso);
   for (int64_t sb = s0; sb < s1; sb += TILE) {
     const int ns = int((s1 - sb) < TILE ? (s1 - sb) : TILE);
@@ -473,20 +488,39 @@ __global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
 #pragma unroll
     for (int m = 0; m < MD; ++m) {
       if (m0 + m >= nd) continue;
-      const size_t o = (size_t(blockIdx.y) * ntarg + it) * nd + m0 + m;
+      const size_t o = (size_t(by) * ntarg + it) * nd + m0 + m;
 #pragma unroll
       for (int c = 0; c < C; ++c) partial[C * o + c] = acc[t][m][c];
     }
   }
 }
 
+template <int KIND, typename R, int NT, int TPT, int MD, int TILE, bool CK>
+__global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
+                                                    const R* __restrict__ ab,
+                                                    const R* __restrict__ sig, int nd,
+                                                    double* __restrict__ partial,
+                                                    int64_t chunk_len) {
+  constexpr int C = (KIND == 1) ? 2 : 1;
+  __shared__ typename Vec<R>::T4 sg0[TILE];
+  __shared__ typename Vec<R>::T2 sg1[TILE];
+  __shared__ __align__(16) R sab[TILE * 2 * C];
+  __shared__ __align__(16) R ssig[TILE * MD * C];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  const double2* tab = nullptr;
+  if constexpr (sizeof(R) == 8 && KIND == 1) {
+    fill_trig_table(stab);  // published by the first __syncthreads of the tile loop
+    tab = stab;
+  }
+  far_md_block<KIND, R, NT, TPT, MD, TILE, CK>(g, kp, ab, sig, nd, partial, chunk_len, blockIdx.x,
+                                               blockIdx.y, blockIdx.z, tab, sg0, sg1, sab, ssig);
+}
+
 // sigma_over[s][m] = (imat sigma_patch)[s][m] without scaling (several
 // densities); feeds far_md_kernel.
 template <typename R, int CPLX>
-__global__ void oversample_kernel(Geometry g, const double* __restrict__ sigma,
-                                  R* __restrict__ sover, int nd) {
-  extern __shared__ double sh[];
-  const int p = blockIdx.x;
+__device__ __forceinline__ void oversample_body(const Geometry& g, const double* __restrict__ sigma,
+                                                R* __restrict__ sover, int nd, int p, double* sh) {
   const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
   const int os = g.ostart[p], nf = g.ostart[p + 1] - os;
   const double* M = g.imat + g.cmoff[g.pclass[p]];
@@ -506,6 +540,13 @@ __global__ void oversample_kernel(Geometry g, const double* __restrict__ sigma,
     sover[C * o] = R(sr);
     if (CPLX) sover[C * o + 1] = R(si);
   }
+}
+
+template <typename R, int CPLX>
+__global__ void oversample_kernel(Geometry g, const double* __restrict__ sigma,
+                                  R* __restrict__ sover, int nd) {
+  extern __shared__ double sh[];
+  oversample_body<R, CPLX>(g, sigma, sover, nd, blockIdx.x, sh);
 }
 
 // Per-source constants a_s = alpha w_s/(4pi), b_s = beta w_s/(4pi).
@@ -544,13 +585,16 @@ constexpr int kCombineThreads = 256;  // 8 warps = 8 consecutive target rows per
 constexpr int kCombineUnroll = 4;     // W_eff entries per lane in flight
 
 
+// Rows 8*bx .. 8*bx+7 (one warp each) of the near correction plus the far
+// partial sums.
 template <int CPLX, typename W>
-__global__ void __launch_bounds__(kCombineThreads)
-    combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
-                   const double* __restrict__ sigma, const double* __restrict__ partial,
-                   int nchunks, double* __restrict__ pot, int nd) {
+__device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
+                                             const W* __restrict__ weff,
+                                             const double* __restrict__ sigma,
+                                             const double* __restrict__ partial, int nchunks,
+                                             double* __restrict__ pot, int nd, int64_t bx) {
   const int lane = threadIdx.x & 31;
-  const int64_t i = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t i = (int64_t(bx) * blockDim.x + threadIdx.x) >> 5;
   const int64_t ntarg = g.ntarg;
   if (nd == 1) {
     __shared__ double sred[32][8][2];
@@ -559,7 +603,7 @@ __global__ void __launch_bounds__(kCombineThreads)
     // covers four whole 8-row segments
     {
       const int r = threadIdx.x & 7, c0 = threadIdx.x >> 3;
-      const int64_t row = int64_t(blockIdx.x) * 8 + r;
+      const int64_t row = int64_t(bx) * 8 + r;
       double pr = 0, pi = 0;
       if (row < ntarg)
         for (int c = c0; c < nchunks; c += 32) {
@@ -710,6 +754,14 @@ __global__ void __launch_bounds__(kCombineThreads)
       pot[o] = ar;
     }
   }
+}
+
+template <int CPLX, typename W>
+__global__ void __launch_bounds__(kCombineThreads)
+    combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
+                   const double* __restrict__ sigma, const double* __restrict__ partial,
+                   int nchunks, double* __restrict__ pot, int nd) {
+  combine_rows<CPLX, W>(g, nr, weff, sigma, partial, nchunks, pot, nd, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1281,6 +1333,232 @@ cudaError_t far_any(const Geometry& g, const KParams& kp, const MatvecArgs& a, c
   return far_variant<0, double, false>(v, g, kp, a, st, occ);
 }
 }  // namespace
+
+namespace {
+// ---- batched matvec kernels ----------------------------------------------------
+template <typename R, int CPLX>
+__global__ void batch_strengths_kernel(const BatchSurf* __restrict__ bs,
+                                       const int2* __restrict__ items, int nitems,
+                                       const double* const* __restrict__ xref,
+                                       R* __restrict__ str, int nd, int over) {
+  extern __shared__ double sh[];
+  const double* x = *xref;
+  constexpr int C = CPLX ? 2 : 1;
+  for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    const int2 it = items[w];
+    const BatchSurf& S = bs[it.x];
+    const Geometry g = S.g;
+    if (over)
+      oversample_body<R, CPLX>(g, x + S.vofs * nd * C, str + S.sofs * nd * C, nd, it.y, sh);
+    else
+      strengths_body<R, CPLX>(g, S.kp, x + S.vofs * nd * C, str + S.sofs * nd * 2 * C, nd, it.y,
+                              sh);
+    __syncthreads();
+  }
+}
+
+template <int KIND, typename R, int NT, int TPT, int TILE, bool CK>
+__global__ void __launch_bounds__(NT)
+    batch_far_kernel(const BatchSurf* __restrict__ bs, const int4* __restrict__ items, int nitems,
+                     const R* __restrict__ str, double* __restrict__ partial, int nd, int prec) {
+  constexpr int SW = (KIND == 1) ? 4 : 2;
+  __shared__ typename Vec<R>::T4 sg0[TILE];
+  __shared__ typename Vec<R>::T2 sg1[TILE];
+  __shared__ R sst[TILE * SW];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  const double2* tab = nullptr;
+  if constexpr (sizeof(R) == 8 && KIND == 1) {
+    fill_trig_table(stab);
+    tab = stab;
+  }
+  __syncthreads();
+  for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    const int4 it = items[w];
+    const BatchSurf& S = bs[it.x];
+    const Geometry g = S.g;
+    const KParams kp = S.kp;
+    far_block<KIND, R, NT, TPT, TILE, CK>(g, kp, str + S.sofs * nd * SW, partial + S.pofs[prec],
+                                          S.chunk_len[prec], nd, it.y, it.z, it.w, tab, sg0, sg1,
+                                          sst);
+    __syncthreads();
+  }
+}
+
+template <int KIND, typename R, int NT, int TPT, int MD, int TILE, bool CK>
+__global__ void __launch_bounds__(NT)
+    batch_far_md_kernel(const BatchSurf* __restrict__ bs, const int4* __restrict__ items,
+                        int nitems, const R* __restrict__ sig, double* __restrict__ partial,
+                        int nd, int prec) {
+  constexpr int C = (KIND == 1) ? 2 : 1;
+  __shared__ typename Vec<R>::T4 sg0[TILE];
+  __shared__ typename Vec<R>::T2 sg1[TILE];
+  __shared__ __align__(16) R sab[TILE * 2 * C];
+  __shared__ __align__(16) R ssig[TILE * MD * C];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  const double2* tab = nullptr;
+  if constexpr (sizeof(R) == 8 && KIND == 1) {
+    fill_trig_table(stab);
+    tab = stab;
+  }
+  __syncthreads();
+  for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    const int4 it = items[w];
+    const BatchSurf& S = bs[it.x];
+    const Geometry g = S.g;
+    const KParams kp = S.kp;
+    far_md_block<KIND, R, NT, TPT, MD, TILE, CK>(
+        g, kp, static_cast<const R*>(S.ab[prec]), sig + S.sofs * nd * C, nd,
+        partial + S.pofs[prec], S.chunk_len[prec], it.y, it.z, it.w, tab, sg0, sg1, sab, ssig);
+    __syncthreads();
+  }
+}
+
+template <int CPLX, typename W>
+__global__ void __launch_bounds__(kCombineThreads)
+    batch_combine_kernel(const BatchSurf* __restrict__ bs, const int2* __restrict__ items,
+                         int nitems, const double* const* __restrict__ xref,
+                         double* const* __restrict__ yref, const double* __restrict__ partial,
+                         int nd, int prec) {
+  const double* x = *xref;
+  double* y = *yref;
+  constexpr int C = CPLX ? 2 : 1;
+  for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    const int2 it = items[w];
+    const BatchSurf& S = bs[it.x];
+    const Geometry g = S.g;
+    const Near nr = S.nr;
+    combine_rows<CPLX, W>(g, nr, static_cast<const W*>(S.weff[prec]), x + S.vofs * nd * C,
+                          partial + S.pofs[prec], S.nchunks[prec], y + S.vofs * nd * C, nd, it.y);
+    __syncthreads();
+  }
+}
+
+template <int KIND, typename R, bool CK, int V>
+cudaError_t batch_far_dispatch(const BatchArgs& a, cudaStream_t st, int* occ) {
+  constexpr bool F32 = sizeof(R) == 4;
+  constexpr int NT = F32 ? kF32Shapes[V][0] : kF64Shapes[V][0];
+  constexpr int TPT = F32 ? kF32Shapes[V][1] : kF64Shapes[V][1];
+  auto kern = batch_far_kernel<KIND, R, NT, TPT, kFarTile, CK>;
+  if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, NT, 0);
+  kern<<<a.grid_far, NT, 0, st>>>(a.surfs, a.far_items, a.nfar_items,
+                                  static_cast<const R*>(a.str), a.partial, a.nd, a.precision);
+  return cudaGetLastError();
+}
+
+template <int KIND, typename R, bool CK, int CL, int V>
+cudaError_t batch_far_md_dispatch(const BatchArgs& a, cudaStream_t st, int* occ) {
+  constexpr int NT = kMdShapes[CL][V][0], TPT = kMdShapes[CL][V][1], MD = kMdShapes[CL][V][2];
+  auto kern = batch_far_md_kernel<KIND, R, NT, TPT, MD, kFarTile, CK>;
+  if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, NT, 0);
+  kern<<<a.grid_far, NT, 0, st>>>(a.surfs, a.far_items, a.nfar_items,
+                                  static_cast<const R*>(a.str), a.partial, a.nd, a.precision);
+  return cudaGetLastError();
+}
+
+template <int KIND, typename R, bool CK>
+cudaError_t batch_far_t(const BatchArgs& a, cudaStream_t st, int* occ) {
+  const int v = a.variant;
+  if (a.nd == 1) {
+    switch (v) {
+      case 1: return batch_far_dispatch<KIND, R, CK, 1>(a, st, occ);
+      case 2: return batch_far_dispatch<KIND, R, CK, 2>(a, st, occ);
+      default: return batch_far_dispatch<KIND, R, CK, 0>(a, st, occ);
+    }
+  }
+  switch (md_class(a.nd) * 3 + (v < 0 || v > 2 ? 0 : v)) {
+    case 0: return batch_far_md_dispatch<KIND, R, CK, 0, 0>(a, st, occ);
+    case 1: return batch_far_md_dispatch<KIND, R, CK, 0, 1>(a, st, occ);
+    case 2: return batch_far_md_dispatch<KIND, R, CK, 0, 2>(a, st, occ);
+    case 3: return batch_far_md_dispatch<KIND, R, CK, 1, 0>(a, st, occ);
+    case 4: return batch_far_md_dispatch<KIND, R, CK, 1, 1>(a, st, occ);
+    case 5: return batch_far_md_dispatch<KIND, R, CK, 1, 2>(a, st, occ);
+    case 6: return batch_far_md_dispatch<KIND, R, CK, 2, 0>(a, st, occ);
+    case 7: return batch_far_md_dispatch<KIND, R, CK, 2, 1>(a, st, occ);
+    default: return batch_far_md_dispatch<KIND, R, CK, 2, 2>(a, st, occ);
+  }
+}
+
+cudaError_t batch_far_any(const BatchArgs& a, cudaStream_t st, int* occ) {
+  if (a.precision == 1) {
+    if (a.kind == 1) return a.ck ? batch_far_t<1, float, true>(a, st, occ) : batch_far_t<1, float, false>(a, st, occ);
+    return batch_far_t<0, float, false>(a, st, occ);
+  }
+  if (a.kind == 1) return a.ck ? batch_far_t<1, double, true>(a, st, occ) : batch_far_t<1, double, false>(a, st, occ);
+  return batch_far_t<0, double, false>(a, st, occ);
+}
+}  // namespace
+
+void batch_far_shape(int precision, int variant, int nd, int* targets_per_block, int* group) {
+  const int v = variant < 0 || variant > 2 ? 0 : variant;
+  if (nd == 1) {
+    const int(*sh)[2] = precision == 1 ? kF32Shapes : kF64Shapes;
+    *targets_per_block = sh[v][0] * sh[v][1];
+    *group = 1;
+    return;
+  }
+  const int cl = md_class(nd);
+  *targets_per_block = kMdShapes[cl][v][0] * kMdShapes[cl][v][1];
+  *group = kMdShapes[cl][v][2];
+}
+
+int batch_far_variants(int precision, int nd) {
+  (void)precision;
+  (void)nd;
+  return 3;
+}
+
+int batch_far_blocks_per_sm(int kind, int precision, int variant, int nd, bool ck) {
+  BatchArgs a;
+  a.kind = kind;
+  a.precision = precision;
+  a.variant = variant;
+  a.nd = nd;
+  a.ck = ck;
+  int occ = 0;
+  batch_far_any(a, nullptr, &occ);
+  return occ;
+}
+
+cudaError_t launch_batch_matvec(const BatchArgs& a, cudaStream_t st) {
+  const int cplx = a.kind == 1;
+  const size_t sh = size_t(a.max_np) * a.nd * (cplx ? 2 : 1) * sizeof(double);
+  if (sh > 200 * 1024) return cudaErrorInvalidValue;
+  const int over = a.nd > 1 ? 1 : 0;
+  auto strengths = [&](auto kern, auto* out) -> cudaError_t {
+    if (sh > 48 * 1024)
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
+    kern<<<a.grid_patch, 128, sh, st>>>(a.surfs, a.patch_items, a.npatch_items, a.xref, out, a.nd,
+                                        over);
+    return cudaGetLastError();
+  };
+  cudaError_t e;
+  if (a.precision == 1)
+    e = cplx ? strengths(batch_strengths_kernel<float, 1>, static_cast<float*>(a.str))
+             : strengths(batch_strengths_kernel<float, 0>, static_cast<float*>(a.str));
+  else
+    e = cplx ? strengths(batch_strengths_kernel<double, 1>, static_cast<double*>(a.str))
+             : strengths(batch_strengths_kernel<double, 0>, static_cast<double*>(a.str));
+  if (e != cudaSuccess) return e;
+  e = batch_far_any(a, st, nullptr);
+  if (e != cudaSuccess) return e;
+  if (cplx) {
+    if (a.precision == 1)
+      batch_combine_kernel<1, float><<<a.grid_row, kCombineThreads, 0, st>>>(
+          a.surfs, a.row_items, a.nrow_items, a.xref, a.yref, a.partial, a.nd, a.precision);
+    else
+      batch_combine_kernel<1, double><<<a.grid_row, kCombineThreads, 0, st>>>(
+          a.surfs, a.row_items, a.nrow_items, a.xref, a.yref, a.partial, a.nd, a.precision);
+  } else {
+    if (a.precision == 1)
+      batch_combine_kernel<0, float><<<a.grid_row, kCombineThreads, 0, st>>>(
+          a.surfs, a.row_items, a.nrow_items, a.xref, a.yref, a.partial, a.nd, a.precision);
+    else
+      batch_combine_kernel<0, double><<<a.grid_row, kCombineThreads, 0, st>>>(
+          a.surfs, a.row_items, a.nrow_items, a.xref, a.yref, a.partial, a.nd, a.precision);
+  }
+  count(3);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_far(const Geometry& g, const KParams& kp, const MatvecArgs& a, cudaStream_t st) {
   if (g.ntarg == 0) return cudaSuccess;

@@ -4,6 +4,7 @@
 #include <complex>
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <string>
 #include <utility>
 #include <vector>
@@ -189,6 +190,13 @@ class Plan : public Operator {
   };
   FarConfig far_config(int precision, int nd) const;
   const double* d_wts() const { return wts_.p; }
+  // W_eff and the per-source (a, b) constants for precision 0 (f64) / 1 (f32)
+  const void* weff_ptr(int precision) const {
+    return precision == 1 ? static_cast<const void*>(weff32_.p) : static_cast<const void*>(weff64_.p);
+  }
+  const void* ab_ptr(int precision) const {
+    return precision == 1 ? static_cast<const void*>(ab32_.p) : static_cast<const void*>(ab64_.p);
+  }
 
   // per-stage timing with CUDA events on the launch stream (off by default)
   bool timing = false;
@@ -209,6 +217,48 @@ class Plan : public Operator {
   DBuf<char> str_;
   DBuf<double> partial_;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+// A batch of surfaces solved together: one operator whose nodes are the
+// surfaces' nodes back to back (segment = surface).  Each surface keeps its
+// own plan (geometry, near quadrature folded into W_eff); the batch adds a
+// device table of surface descriptors and work lists, so each matvec stage
+// is one persistent launch over all surfaces, and captures the three
+// launches once per (precision, nd) in a CUDA graph that is replayed for
+// every matvec (the kernels read the vector pointers from device memory).
+class BatchPlan : public Operator {
+ public:
+  int kind = -1;
+  bool ck = false;               // some surface has a complex wavenumber
+  bool use_graph = true;
+  std::vector<std::unique_ptr<Plan>> plans;
+  ~BatchPlan() override;
+  int add(Plan* p);  // an on-surface plan; on success the batch owns it
+  int finalize(cudaStream_t st);         // node table, weights, reduction segments
+  int apply(int precision, int nd, const double* x, double* y, cudaStream_t st) override;
+  bool square() const override;
+  // far shape kept by the autotuner for (precision, nd): variant, chunk length
+  bool far_choice(int precision, int nd, int* variant, int64_t* chunk) const;
+
+ private:
+  struct Config {
+    int variant = 0;
+    int64_t chunk = 0;
+    DBuf<dev::BatchSurf> surfs;
+    DBuf<int2> patch_items, row_items;
+    DBuf<int4> far_items;
+    DBuf<char> str;
+    DBuf<double> partial;
+    DBuf<void*> refs;  // [0] input vector, [1] output vector (device pointer slots)
+    dev::BatchArgs args;
+    cudaGraphExec_t graph = nullptr;
+  };
+  int build_config(int precision, int nd, int variant, int64_t chunk, Config& c, cudaStream_t st);
+  int tune(int precision, int nd, cudaStream_t st, std::unique_ptr<Config>& out);
+  std::map<std::pair<int, int>, std::unique_ptr<Config>> cfg_;
+  DBuf<double> wts_;
+  int64_t nptso_total_ = 0;
+  int max_np_ = 0;
 };
 
 struct GmresOut {

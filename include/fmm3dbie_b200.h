@@ -329,6 +329,36 @@ int bie_farfield_dev_noalloc(int64_t kind, const double* zk, int64_t ns, const d
                              const double* dipstr_dev, int64_t nt, const double* targ_dev,
                              double thresh, int64_t iprec, double* pot_dev, void* stream);
 
+/* ---- batches of surfaces (no reference counterpart) ---------------------
+ * Many surfaces of uneven size solved together as one operator whose nodes
+ * are the surfaces' nodes back to back (vectors: all nodes of surface 0,
+ * then surface 1, ...; nd densities per node, point-major).  Each matvec
+ * stage runs as one persistent launch over all surfaces (work lists of
+ * patches, target-block x source-chunk items and row groups), captured once
+ * per (precision, nd) in a CUDA graph; the far-field shape is autotuned on
+ * the first matvec of each (precision, nd).  Every (surface, density) is an
+ * independent system of the solvers. */
+int bie_batch_create(void** batch);
+int bie_batch_destroy(void* batch);
+/* Adds an on-surface plan (bie_plan_create with ntarg = 0).  On success the
+ * batch owns the plan (do not destroy it); on failure the caller keeps it.
+ * All plans share one kernel kind and one device. */
+int bie_batch_add(void* batch, void* plan);
+int bie_batch_finalize(void* batch, void* stream);
+/* info[6]: surfaces, nodes, kind, reduction chunks, far-kernel variant and
+ * source chunk length kept for (f32, nd = 1) (-1 / 0 before the first use). */
+int bie_batch_info(void* batch, int64_t* info);
+/* 1 (default): replay the captured graph; 0: launch the three kernels. */
+int bie_batch_set_graph(void* batch, int64_t enable);
+int bie_batch_matvec(void* batch, int64_t iprec, int64_t nd, const double* x_dev, double* y_dev,
+                     void* stream);
+/* bie_plan_solve for a batch: zid per surface (complex, 2 doubles each);
+ * niter(nsurf*nd), rres(nsurf*nd) per system (surface-major); mode 1:
+ * stats[0] = FP64 matvecs, stats[1] = FP32 matvecs. */
+int bie_batch_solve(void* batch, int64_t mode, int64_t nd, const double* zid,
+                    const double* rhs_dev, const double* x0_dev, int64_t numit, double eps_gmres,
+                    double* soln_dev, int64_t* niter, double* rres, double* stats, void* stream);
+
 /* ---- learned warm start (no reference counterpart) ----------------------
  * The reference solvers always start GMRES from zero
  * (helm_comb_dir_solver_guru, helm_comb_dir.f:2071, calls zgmres_guru at
