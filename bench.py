@@ -643,7 +643,11 @@ def uneven_leg(dev, kinds=(0, 1)):
             G.solve(R, mode=mode, eps_gmres=TOL_RES)  # warm-up / tuning / graph capture
             _, infos, ms = G.solve(R, mode=mode, eps_gmres=TOL_RES)
             res[tag] = {"solves_per_s": nsys * 1000.0 / ms, "ms": ms,
-                        "max_rres": float(max(np.max(i["rres"]) for i in infos))}
+                        "max_rres": float(max(np.max(i["rres"]) for i in infos)),
+                        "max_niter": int(max(np.max(i["niter"]) for i in infos))}
+            if mode == 1:
+                res[tag]["batch_matvecs_fp32_fp64"] = [infos[0]["fp32_matvecs"],
+                                                       infos[0]["fp64_matvecs"]]
         info = G.info()
         res["far_variant_chunk_f32_nd1"] = [int(info[4]), int(info[5])]
         G.close()

@@ -87,7 +87,23 @@ int BatchPlan::finalize(cudaStream_t st) {
     BIE_CUDA(cudaMemcpyAsync(wts_.p + seg_start[s], plans[s]->d_wts(),
                              size_t(plans[s]->npts) * sizeof(double), cudaMemcpyDeviceToDevice, st));
   d_node_wts = wts_.p;
-  return init_segments(st);
+  live_host_.assign(plans.size(), 1);
+  std::vector<int> ones(plans.size(), 1);
+  BIE_CUDA(upload_vec(live_, ones, st));
+  return init_segments(st);  // synchronises st before `ones` goes
+}
+
+int BatchPlan::set_active(const std::vector<uint8_t>& active, cudaStream_t st) {
+  if (active.size() != plans.size()) {
+    set_last_error("active mask size differs from the number of surfaces");
+    return kErrArg;
+  }
+  if (active == live_host_) return kOk;
+  live_host_ = active;
+  std::vector<int> h(active.begin(), active.end());
+  // pageable source: staged before cudaMemcpyAsync returns
+  BIE_CUDA(cudaMemcpyAsync(live_.p, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  return kOk;
 }
 
 int BatchPlan::build_config(int precision, int nd, int variant, int64_t chunk, Config& c,
@@ -112,6 +128,7 @@ int BatchPlan::build_config(int precision, int nd, int variant, int64_t chunk, C
     d.ab[1] = p.ab_ptr(1);
     d.vofs = vofs;
     d.sofs = sofs;
+    d.live = live_.p + s;
     const int64_t nch = std::max<int64_t>(1, (p.nptso + chunk - 1) / chunk);
     d.chunk_len[precision] = chunk;
     d.nchunks[precision] = int(nch);

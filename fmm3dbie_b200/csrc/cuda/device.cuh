@@ -181,6 +181,9 @@ struct BatchSurf {
   int64_t pofs[2] = {0, 0};
   int64_t chunk_len[2] = {0, 0};
   int nchunks[2] = {0, 0};
+  // device flag: 0 while every system of the surface has converged; its
+  // strengths and far-field items are then skipped and its output rows zeroed
+  const int* live = nullptr;
 };
 
 struct BatchArgs {

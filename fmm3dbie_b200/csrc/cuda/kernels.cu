@@ -1347,6 +1347,7 @@ __global__ void batch_strengths_kernel(const BatchSurf* __restrict__ bs,
   for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const int2 it = items[w];
     const BatchSurf& S = bs[it.x];
+    if (S.live && *S.live == 0) continue;  // uniform over the block
     const Geometry g = S.g;
     if (over)
       oversample_body<R, CPLX>(g, x + S.vofs * nd * C, str + S.sofs * nd * C, nd, it.y, sh);
@@ -1375,6 +1376,7 @@ __global__ void __launch_bounds__(NT)
   for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const int4 it = items[w];
     const BatchSurf& S = bs[it.x];
+    if (S.live && *S.live == 0) continue;  // uniform over the block
     const Geometry g = S.g;
     const KParams kp = S.kp;
     far_block<KIND, R, NT, TPT, TILE, CK>(g, kp, str + S.sofs * nd * SW, partial + S.pofs[prec],
@@ -1404,6 +1406,7 @@ __global__ void __launch_bounds__(NT)
   for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const int4 it = items[w];
     const BatchSurf& S = bs[it.x];
+    if (S.live && *S.live == 0) continue;  // uniform over the block
     const Geometry g = S.g;
     const KParams kp = S.kp;
     far_md_block<KIND, R, NT, TPT, MD, TILE, CK>(
@@ -1425,6 +1428,16 @@ __global__ void __launch_bounds__(kCombineThreads)
   for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const int2 it = items[w];
     const BatchSurf& S = bs[it.x];
+    if (S.live && *S.live == 0) {
+      // converged surface: zero rows, so no stale value enters the solver
+      const int64_t row = int64_t(it.y) * 8 + (threadIdx.x >> 5);
+      if (row < S.g.ntarg) {
+        double* yr = y + (S.vofs + row) * nd * C;
+        for (int j = threadIdx.x & 31; j < nd * C; j += 32) yr[j] = 0.0;
+      }
+      __syncthreads();
+      continue;
+    }
     const Geometry g = S.g;
     const Near nr = S.nr;
     combine_rows<CPLX, W>(g, nr, static_cast<const W*>(S.weff[prec]), x + S.vofs * nd * C,

@@ -141,6 +141,14 @@ class Operator {
   virtual int apply(int precision, int nd, const double* x, double* y, cudaStream_t st) = 0;
   // whether the operator maps node values to node values (GMRES needs it)
   virtual bool square() const = 0;
+  // Segments whose systems have all converged (active[g] == 0) may skip
+  // their work in later apply() calls; their output is then zero.  The
+  // default does the full work.
+  virtual int set_active(const std::vector<uint8_t>& active, cudaStream_t st) {
+    (void)active;
+    (void)st;
+    return 0;
+  }
 
   bool cplx = false;
   int device = 0, num_sms = 148;
@@ -237,6 +245,7 @@ class BatchPlan : public Operator {
   int finalize(cudaStream_t st);         // node table, weights, reduction segments
   int apply(int precision, int nd, const double* x, double* y, cudaStream_t st) override;
   bool square() const override;
+  int set_active(const std::vector<uint8_t>& active, cudaStream_t st) override;
   // far shape kept by the autotuner for (precision, nd): variant, chunk length
   bool far_choice(int precision, int nd, int* variant, int64_t* chunk) const;
 
@@ -257,6 +266,8 @@ class BatchPlan : public Operator {
   int tune(int precision, int nd, cudaStream_t st, std::unique_ptr<Config>& out);
   std::map<std::pair<int, int>, std::unique_ptr<Config>> cfg_;
   DBuf<double> wts_;
+  DBuf<int> live_;                 // per surface, read by the batched kernels
+  std::vector<uint8_t> live_host_;
   int64_t nptso_total_ = 0;
   int max_np_ = 0;
 };
@@ -275,9 +286,10 @@ struct GmresOut {
 // (system = segment * nd + density).  The inner matvec uses `precision`;
 // the final relative residual rres uses `rres_precision` (-1 skips it).
 // d_x0 (optional) is an initial guess.
+// eps_sys (optional): a relative tolerance per system in place of eps_gmres.
 int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble* zid,
           const double* d_rhs, const double* d_x0, int64_t numit, double eps_gmres,
-          double* d_soln, GmresOut& out, cudaStream_t st);
+          double* d_soln, GmresOut& out, cudaStream_t st, const double* eps_sys = nullptr);
 
 // Mixed-precision solve: FP64 residuals and iterative refinement around
 // FP32-matvec GMRES inner solves.  Stops when the FP64 relative residual

@@ -93,7 +93,7 @@ int Operator::init_segments(cudaStream_t st) {
 
 int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble* zid,
           const double* d_rhs, const double* d_x0, int64_t numit, double eps_gmres,
-          double* d_soln, GmresOut& out, cudaStream_t st) {
+          double* d_soln, GmresOut& out, cudaStream_t st, const double* eps_sys) {
   if (!P.square()) {
     set_last_error("GMRES needs an operator whose targets are its nodes");
     return kErrArg;
@@ -177,7 +177,13 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
   for (; it < M && nactive > 0; ++it) {
     double* vit = V + size_t(it) * ldv;
     double* vnext = V + size_t(it + 1) * ldv;
-    int ier = P.apply(precision, nd, vit, ws.w.p, st);
+    // segments whose systems have all converged skip their matvec work
+    std::vector<uint8_t> act(sg.nseg, 0);
+    for (int q = 0; q < nsys; ++q)
+      if (done[q] == 0) act[q / nd] = 1;
+    int ier = P.set_active(act, st);
+    if (ier) return ier;
+    ier = P.apply(precision, nd, vit, ws.w.p, st);
     if (ier) return ier;
     const int m = int(it + 1);
     BIE_CUDA(dev::launch_mdot(V, ldv, m, ws.w.p, wts, nd, cplx, sg, ws.partial.p, d_h1, st));
@@ -218,7 +224,7 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
         --nactive;
         continue;
       }
-      if (err <= eps_gmres || it == M - 1 || wnrm == 0.0) {
+      if (err <= (eps_sys ? eps_sys[q] : eps_gmres) || it == M - 1 || wnrm == 0.0) {
         done[q] = it + 1;
         --nactive;
         continue;
@@ -227,6 +233,10 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
     }
     BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
     BIE_CUDA(dev::launch_dscale(ws.w.p, vnext, ws.scale.p, n, nd, cplx, sg, st));
+  }
+  {
+    int ier = P.set_active(std::vector<uint8_t>(sg.nseg, 1), st);
+    if (ier) return ier;
   }
   // back-substitution per system: y = triu(H)\s, soln = V y (+ x0)
   std::vector<double> hc(size_t(2) * (M + 1) * nsys, 0.0);
@@ -245,7 +255,8 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
       hc[2 * (j * nsys + q) + 1] = y[j].imag();
     }
     out.niter[q] = k;
-    if (out.errs[size_t(q) * (M + 1) + k - 1] > eps_gmres && out.status == kOk) out.status = kNotConverged;
+    if (out.errs[size_t(q) * (M + 1) + k - 1] > (eps_sys ? eps_sys[q] : eps_gmres) && out.status == kOk)
+      out.status = kNotConverged;
   }
   const int mused = int(std::max<int64_t>(it, 1));
   BIE_CUDA(cudaMemcpyAsync(ws.coef.p, hc.data(), 2 * mused * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -364,6 +375,17 @@ int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, co
   }
   BIE_CUDA(cudaStreamSynchronize(st));
   for (int q = 0; q < nsys; ++q) bn[q] = std::sqrt(std::max(hb[2 * q], 0.0));
+  // frozen[q]: an FP64 residual has shown system q at the target; it sits
+  // out the remaining refinement steps (zero inner residual, and in a batch
+  // its surface skips the FP64 residual matvecs once all its systems froze)
+  std::vector<uint8_t> frozen(nsys, 0);
+  auto seg_mask = [&]() {
+    std::vector<uint8_t> act(sg.nseg, 0);
+    for (int q = 0; q < nsys; ++q)
+      if (!frozen[q]) act[q / nd] = 1;
+    return act;
+  };
+  int ier = kOk;
   for (int outer = 0; outer <= max_outer; ++outer) {
     BIE_CUDA(dev::launch_mdot(r.p, ldv, 1, r.p, wts, nd, cplx, sg, partial.p, nrm.p, st));
     BIE_CUDA(cudaMemcpyAsync(hr.data(), nrm.p, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -371,17 +393,20 @@ int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, co
     double worst_ratio = 0.0;
     bool all_done = true;
     for (int q = 0; q < nsys; ++q) {
+      if (frozen[q]) continue;  // keeps its last FP64 relative residual
       const double rel = bn[q] > 0 ? std::sqrt(std::max(hr[2 * q], 0.0)) / bn[q] : 0.0;
       out.rres[q] = rel;
       if (rel > eps_target) {
         all_done = false;
         worst_ratio = std::max(worst_ratio, eps_target / rel);
+      } else if (r_is_f64) {
+        frozen[q] = 1;
       }
     }
     if (!r_is_f64 && all_done) {
       // the guess already meets the target in FP32: confirm it in FP64
-      int ier = P.apply(0, nd, d_soln, r.p, st);
-      if (ier) return ier;
+      if ((ier = P.set_active(std::vector<uint8_t>(sg.nseg, 1), st))) return ier;
+      if ((ier = P.apply(0, nd, d_soln, r.p, st))) return ier;
       ++out.fp64_matvecs;
       if ((ier = finish_residual())) return ier;
       r_is_f64 = true;
@@ -391,27 +416,50 @@ int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, co
       if (!all_done) out.status = kNotConverged;
       break;
     }
-    // inner relative tolerance: what this step must gain, not below the
-    // accuracy the f32 operator can deliver
+    // inner relative tolerance per system: what this step must gain for that
+    // system, not below the accuracy the f32 operator can deliver
     const double tol = std::max(inner_floor, 0.5 * worst_ratio);
+    std::vector<double> tol_sys(nsys, tol);
+    for (int q = 0; q < nsys; ++q)
+      if (out.rres[q] > eps_target) tol_sys[q] = std::max(inner_floor, 0.5 * eps_target / out.rres[q]);
+    // systems at the target (frozen, or below it in an FP32 residual) sit
+    // this inner solve out: a zero residual makes GMRES skip them
+    {
+      std::vector<double> keep(2 * nsys, 0.0);
+      bool any = false;
+      for (int q = 0; q < nsys; ++q) {
+        keep[2 * q] = (!frozen[q] && out.rres[q] > eps_target) ? 1.0 : 0.0;
+        any = any || keep[2 * q] == 0.0;
+      }
+      if (any) {
+        double* sk = nrm.p + 2 * nsys;
+        BIE_CUDA(cudaMemcpyAsync(sk, keep.data(), 2 * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
+        BIE_CUDA(dev::launch_dscale(r.p, r.p, sk, n, nd, cplx, sg, st));
+      }
+    }
     GmresOut go;
-    int ier = gmres(P, 1, -1, nd, zid, r.p, nullptr, numit, tol, d.p, go, st);
+    ier = gmres(P, 1, -1, nd, zid, r.p, nullptr, numit, tol, d.p, go, st, tol_sys.data());
     if (ier && ier != kNotConverged) return ier;
     int64_t maxit = 0;
     for (int q = 0; q < nsys; ++q) {
+      if (frozen[q]) continue;
       out.inner_iters[q] += go.niter[q];
       out.outer[q] += 1;
       maxit = std::max(maxit, go.niter[q]);
     }
     out.fp32_matvecs += int(maxit);
-    // x += d ; r = rhs - (zid x + K x) in f64
+    // x += d ; r = rhs - (zid x + K x) in f64 for the systems still refined
+    // (frozen surfaces of a batch skip the matvec; their r is not read again)
     BIE_CUDA(dev::launch_axpby(d.p, d_soln, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    if ((ier = P.set_active(seg_mask(), st))) return ier;
     ier = P.apply(0, nd, d_soln, r.p, st);
     if (ier) return ier;
+    if ((ier = P.set_active(std::vector<uint8_t>(sg.nseg, 1), st))) return ier;
     ++out.fp64_matvecs;
     if ((ier = finish_residual())) return ier;
     r_is_f64 = true;
   }
+  if ((ier = P.set_active(std::vector<uint8_t>(sg.nseg, 1), st))) return ier;
   return out.status;
 }
 
