@@ -62,14 +62,38 @@ def env_rank():
         int(os.environ.get("LOCAL_RANK", 0))
 
 
-def build_problem(nref=3, norder=6):
+def build_problem(nref=3, norder=6, nq_stats=None):
+    """The ellipsoid, its setup (near quadrature on the device when one is
+    visible; nq_stats receives the generator's counters) and the rhs."""
     from fmm3dbie_b200 import surface as S
     s = S.icosa_ellipsoid(nref, norder, (1.0, 2.0, 3.0))
     t = time.time()
-    st = S.setup(s, 1, EPS, ZPARS)
+    st = S.setup(s, 1, EPS, ZPARS, stats=nq_stats)
     r = np.linalg.norm(s.xyz - X0, axis=1)
     rhs = np.exp(1j * ZK * r) / (4 * np.pi * r)
     return s, st, rhs, time.time() - t
+
+
+def nearquad_compare(s, st):
+    """Near quadrature of the bench ellipsoid by the host generator (all host
+    cores) and the device generator, on the same near list."""
+    from fmm3dbie_b200 import surface as S
+    targs = s.srcvals
+    ipatch_id, uvs = s.patch_id_uvs()
+    nf = st.near
+    args = (s, 1, EPS, ZPARS, targs, ipatch_id, uvs, nf.row_ptr, nf.col_ind, nf.iquad, st.rfac0)
+    t0 = time.time()
+    wc = S.getnearquad(*args, engine="cpu")
+    t_cpu = time.time() - t0
+    gs = np.zeros(4, np.int64)
+    t0 = time.time()
+    wg = S.getnearquad(*args, engine="gpu", stats=gs)
+    t_gpu = time.time() - t0
+    diff = float(np.max(np.abs(wg - wc)) / np.max(np.abs(wc)))
+    return {"host_generator_s": round(t_cpu, 3), "host_cores": len(os.sched_getaffinity(0)),
+            "device_call_s": round(t_gpu, 3), "device_kernel_ms": gs[3] / 1e3,
+            "kernel_evals": int(gs[0]), "pairs": int(gs[1] + gs[2]),
+            "max_abs_diff_over_max": diff}
 
 
 def gpu_uuid(dev_index):
@@ -266,6 +290,8 @@ def main():
                     help="skip the batched leg (64 plane-wave right-hand sides)")
     ap.add_argument("--torus", action="store_true",
                     help="also run the torus warm-start leg (trained warm start; ~1-2 min host setup)")
+    ap.add_argument("--no-nearquad", action="store_true",
+                    help="skip the near-quadrature generator comparison (host vs device)")
     ap.add_argument("--uneven", action="store_true",
                     help="add the uneven batch leg (32 ellipsoids; ~2 min of CPU setup)")
     args = ap.parse_args()
@@ -286,7 +312,8 @@ def main():
     from fmm3dbie_b200 import _lib as L
     lib = L.lib()
 
-    s, st, rhs, t_setup = build_problem()
+    nq_stats = np.zeros(4, np.int64)
+    s, st, rhs, t_setup = build_problem(nq_stats=nq_stats)
     P = Plan(1, ZPARS, s, st.near, st.over)
     stream = torch.cuda.current_stream(dev)
     r_d = torch.tensor(rhs, device=dev)
@@ -403,6 +430,9 @@ def main():
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(s, st, int(info64["niter"][0]))
+    nearquad = None
+    if rank == 0 and world == 1 and not args.no_nearquad:
+        nearquad = nearquad_compare(s, st)
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         P.close()
@@ -434,6 +464,8 @@ def main():
                       "fp32_matvecs": infom["fp32_matvecs"]},
             "problem": {"npts": P.npts, "nptso": P.nptso, "nnz": P.nnz, "nquad": P.nquad,
                         "setup_s": round(t_setup, 2),
+                        "nearquad_device_kernel_ms": nq_stats[3] / 1e3,
+                        "nearquad_kernel_evals": int(nq_stats[0]),
                         "far_shape_variant_chunks": {"f64": [int(pinfo[8]), int(pinfo[5])],
                                                      "f32": [int(pinfo[9]), int(pinfo[6])]}},
             "roofline": {"kernel": "far_kernel<helm,f32>", "bound": "fp32", "achieved": achieved,
@@ -453,6 +485,7 @@ def main():
             "clocks": ck,
             "e2e": e2e,
             "cpu_baseline": base,
+            "nearquad": nearquad,
             "batched": batched,
             "uneven": uneven,
             "torus_warm_start": torus,

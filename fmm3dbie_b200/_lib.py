@@ -62,6 +62,16 @@ _SIGS = {
     "bie_getnearquad_helm_comb_dir_eval": (C.c_int, [I64, PI64, PI64, PI64, I64, PDBL, PDBL, I64,
                                                      I64, PDBL, PI64, PDBL, DBL, PDBL, I64, I64,
                                                      PI64, PI64, PI64, DBL, I64, PDBL]),
+    "bie_getnearquad_lap_comb_dir_eval_gpu": (C.c_int, [I64, PI64, PI64, PI64, I64, PDBL, PDBL,
+                                                        I64, I64, PDBL, PI64, PDBL, DBL, PDBL,
+                                                        I64, I64, PI64, PI64, PI64, DBL, I64,
+                                                        PDBL, PI64]),
+    "bie_getnearquad_helm_comb_dir_eval_gpu": (C.c_int, [I64, PI64, PI64, PI64, I64, PDBL, PDBL,
+                                                         I64, I64, PDBL, PI64, PDBL, DBL, PDBL,
+                                                         I64, I64, PI64, PI64, PI64, DBL, I64,
+                                                         PDBL, PI64]),
+    "bie_set_nearquad_engine": (C.c_int, [I64]),
+    "bie_get_nearquad_engine": (I64, []),
     "bie_lpcomp_lap_comb_dir_addsub": (C.c_int, [I64, PI64, PI64, PI64, I64, PDBL, PDBL, DBL, I64,
                                                  PDBL, I64, PDBL, I64, PI64, I64, PI64, PI64, PI64,
                                                  I64, I64, PDBL, PI64, I64, PI64, PDBL, PDBL, I64,

@@ -5,6 +5,7 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstdlib>
@@ -18,6 +19,7 @@
 #include "../host/basis.h"
 #include "../host/nearquad.h"
 #include "../host/setup.h"
+#include "nearquad_gpu.h"
 #include "plan.h"
 
 using bie::cdouble;
@@ -84,6 +86,15 @@ int check_surf(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
   return BIE_OK;
 }
 
+// Stream-ordered host<->device staging of one host-buffer call.
+struct Stage {
+  cudaStream_t st = nullptr;
+  Stage() { cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking); }
+  ~Stage() {
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
 // Everything the simple interfaces derive from the geometry (the setup part
 // of lap_comb_dir_eval / helm_comb_dir_solver).
 struct Setup {
@@ -93,6 +104,17 @@ struct Setup {
   int64_t nnz = 0, nquad = 0, nptso = 0;
   double rfac = 0, rfac0 = 0;
 };
+
+// Near quadrature engine of the setup: 1 = device generator (default),
+// 0 = host generator.  Surfaces with patches above the device generator's
+// basis limit use the host generator.
+std::atomic<int> g_nearquad_engine{1};
+
+int64_t max_npols(const bie::Surf& s) {
+  int64_t m = 0;
+  for (int64_t p = 0; p < s.npatches; ++p) m = std::max(m, s.npols(p));
+  return m;
+}
 
 int run_setup(const bie::Surf& s, int kind, cdouble zk, cdouble alpha, cdouble beta, double eps,
               int ndtarg, int64_t ntarg, const double* targs, const int64_t* ipatch_id,
@@ -135,6 +157,26 @@ int run_setup(const bie::Surf& s, int kind, cdouble zk, cdouble alpha, cdouble b
   bie::qwts(so, o.wover.data());
   const size_t wl = size_t(o.nquad) * (kind == 1 ? 2 : 1);
   o.wnear.assign(wl, 0.0);
+  if (g_nearquad_engine.load() == 1 && o.nnz > 0 && max_npols(s) <= bie::kNearQuadMaxNp) {
+    Stage stg;
+    bie::AllocStreamScope alloc_scope(stg.st);
+    bie::DBuf<double> d_w;
+    if (d_w.alloc(wl) != cudaSuccess) {
+      bie::set_last_error("near quadrature: device allocation failed");
+      return BIE_ERR_NOMEM;
+    }
+    ier = bie::getnearquad_gpu(s, ndtarg, ntarg, targs, ipatch_id, uvs_targ, eps, kind, zk, alpha,
+                               beta, o.nnz, o.row_ptr.data(), o.col_ind.data(), o.iquad.data(),
+                               o.nquad, d_w.p, stg.st);
+    if (ier) return ier;
+    if (cudaMemcpyAsync(o.wnear.data(), d_w.p, wl * sizeof(double), cudaMemcpyDeviceToHost,
+                        stg.st) != cudaSuccess ||
+        cudaStreamSynchronize(stg.st) != cudaSuccess) {
+      bie::set_last_error("near quadrature: copy to host failed");
+      return BIE_ERR_CUDA;
+    }
+    return BIE_OK;
+  }
   std::vector<double> wre(o.nquad), wim(kind == 1 ? o.nquad : 0);
   ier = bie::getnearquad(s, ndtarg, ntarg, targs, ipatch_id, uvs_targ, eps, kind, zk, alpha, beta,
                          o.nnz, o.row_ptr.data(), o.col_ind.data(), o.iquad.data(), o.rfac0,
@@ -153,15 +195,6 @@ int run_setup(const bie::Surf& s, int kind, cdouble zk, cdouble alpha, cdouble b
   }
   return BIE_OK;
 }
-
-// Stream-ordered host<->device staging of one host-buffer call.
-struct Stage {
-  cudaStream_t st = nullptr;
-  Stage() { cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking); }
-  ~Stage() {
-    if (st) cudaStreamDestroy(st);
-  }
-};
 
 int plan_from_arrays(bie::Plan& P, int kind, cdouble zk, cdouble alpha, cdouble beta,
                      int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
@@ -558,6 +591,91 @@ int bie_getnearquad_helm_comb_dir_eval(int64_t npatches, const int64_t* norders,
     return ier ? BIE_ERR_ARG : BIE_OK;
   });
 }
+
+namespace {
+int nearquad_gpu_call(int kind, cdouble zk, cdouble alpha, cdouble beta, int64_t npatches,
+                      const int64_t* norders, const int64_t* ixyzs, const int64_t* iptype,
+                      int64_t npts, const double* srccoefs, const double* srcvals,
+                      int64_t ndtarg, int64_t ntarg, const double* targs,
+                      const int64_t* ipatch_id, const double* uvs_targ, double eps, int64_t nnz,
+                      const int64_t* row_ptr, const int64_t* col_ind, const int64_t* iquad,
+                      int64_t nquad, double* wnear, int64_t* stats) {
+  int ier = ensure_tables();
+  if (ier) return ier;
+  ier = check_surf(npatches, norders, ixyzs, iptype, npts);
+  if (ier) return ier;
+  if (nquad < 0 || (nquad > 0 && !wnear)) {
+    bie::set_last_error("getnearquad: missing output");
+    return BIE_ERR_ARG;
+  }
+  const size_t wl = size_t(nquad) * (kind == 1 ? 2 : 1);
+  Stage stg;
+  bie::AllocStreamScope alloc_scope(stg.st);
+  bie::DBuf<double> d_w;
+  if (d_w.alloc(std::max<size_t>(wl, 1)) != cudaSuccess) {
+    bie::set_last_error("getnearquad: device allocation failed");
+    return BIE_ERR_NOMEM;
+  }
+  bie::NearQuadStats st;
+  ier = bie::getnearquad_gpu(make_surf(npatches, norders, ixyzs, iptype, npts, srccoefs, srcvals),
+                             int(ndtarg), ntarg, targs, ipatch_id, uvs_targ, eps, kind, zk, alpha,
+                             beta, nnz, row_ptr, col_ind, iquad, nquad, d_w.p, stg.st, &st);
+  if (ier) return ier;
+  if (wl && (cudaMemcpyAsync(wnear, d_w.p, wl * sizeof(double), cudaMemcpyDeviceToHost,
+                             stg.st) != cudaSuccess ||
+             cudaStreamSynchronize(stg.st) != cudaSuccess)) {
+    bie::set_last_error("getnearquad: copy to host failed");
+    return BIE_ERR_CUDA;
+  }
+  if (stats) {
+    stats[0] = st.kernel_evals;
+    stats[1] = st.self_targets;
+    stats[2] = st.near_targets;
+    stats[3] = int64_t(st.device_ms * 1e3);
+  }
+  return BIE_OK;
+}
+}  // namespace
+
+int bie_getnearquad_lap_comb_dir_eval_gpu(
+    int64_t npatches, const int64_t* norders, const int64_t* ixyzs, const int64_t* iptype,
+    int64_t npts, const double* srccoefs, const double* srcvals, int64_t ndtarg, int64_t ntarg,
+    const double* targs, const int64_t* ipatch_id, const double* uvs_targ, double eps,
+    const double* dpars, int64_t /*iquadtype*/, int64_t nnz, const int64_t* row_ptr,
+    const int64_t* col_ind, const int64_t* iquad, double /*rfac0*/, int64_t nquad, double* wnear,
+    int64_t* stats) {
+  return guarded([&] {
+    return nearquad_gpu_call(0, 0.0, dpars[0], dpars[1], npatches, norders, ixyzs, iptype, npts,
+                             srccoefs, srcvals, ndtarg, ntarg, targs, ipatch_id, uvs_targ, eps,
+                             nnz, row_ptr, col_ind, iquad, nquad, wnear, stats);
+  });
+}
+
+int bie_getnearquad_helm_comb_dir_eval_gpu(
+    int64_t npatches, const int64_t* norders, const int64_t* ixyzs, const int64_t* iptype,
+    int64_t npts, const double* srccoefs, const double* srcvals, int64_t ndtarg, int64_t ntarg,
+    const double* targs, const int64_t* ipatch_id, const double* uvs_targ, double eps,
+    const double* zpars, int64_t /*iquadtype*/, int64_t nnz, const int64_t* row_ptr,
+    const int64_t* col_ind, const int64_t* iquad, double /*rfac0*/, int64_t nquad, double* wnear,
+    int64_t* stats) {
+  return guarded([&] {
+    return nearquad_gpu_call(1, zpar(zpars, 0), zpar(zpars, 1), zpar(zpars, 2), npatches, norders,
+                             ixyzs, iptype, npts, srccoefs, srcvals, ndtarg, ntarg, targs,
+                             ipatch_id, uvs_targ, eps, nnz, row_ptr, col_ind, iquad, nquad, wnear,
+                             stats);
+  });
+}
+
+int bie_set_nearquad_engine(int64_t engine) {
+  if (engine != 0 && engine != 1) {
+    bie::set_last_error("nearquad engine must be 0 (host) or 1 (device)");
+    return BIE_ERR_ARG;
+  }
+  g_nearquad_engine.store(int(engine));
+  return BIE_OK;
+}
+
+int64_t bie_get_nearquad_engine(void) { return g_nearquad_engine.load(); }
 
 int bie_lpcomp_lap_comb_dir_addsub(int64_t npatches, const int64_t* norders,
                                    const int64_t* ixyzs, const int64_t* iptype, int64_t npts,

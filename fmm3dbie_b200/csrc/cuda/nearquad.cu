@@ -1,0 +1,759 @@
+// Device near-field quadrature generator (see nearquad_gpu.h).
+//
+// One warp per (target, patch) pair of the row-sparse near list, taken from
+// a global work counter (self pairs first: they cost the most).  A warp
+// integrates one parameter-space triangle at a time: each lane evaluates
+// one rule node -- the patch basis (Koornwinder on triangles, tensor
+// Legendre/Chebyshev on quads), the geometry sum over the patch
+// coefficients and the kernel -- and writes the basis row to shared
+// memory; the lanes then switch to one basis index each and accumulate
+// sum_q K_q w_q P_l(y_q) over the chunk.  The refinement stack of the
+// adaptive rule (vertices, level and the integral vector of every pending
+// triangle) lives in a per-warp slice of global scratch; DFS order and the
+// acceptance test follow the host generator (host/nearquad.cpp:190-247).
+// The self rule (host/nearquad.cpp:251-311) flattens (sub-triangle, sinh
+// node, Duffy node) into one index the lanes stride over.
+#include "nearquad_gpu.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../host/basis.h"
+#include "plan.h"
+
+namespace bie {
+namespace {
+
+constexpr int kNqMaxLevel = 18;
+// Integral vectors per warp: at most 1 + 3 * 17 + 4 = 56 pending triangles
+// (one other root, three siblings per level, four at the deepest level) and
+// four children computed above the top.
+constexpr int kNqSlots = 64;
+constexpr int kNqStackDoubles = 8;  // per pending triangle: 6 vertex coordinates, level
+constexpr int kNqMaxSteps = 1 << 16;
+constexpr int kNqTriOrder = kMaxOrder;  // Koornwinder tables up to order 20
+constexpr int kNqLeg = 41;              // tensor bases up to order 40
+constexpr int kNqJac = kNqTriOrder + 1;
+constexpr int kNqSubDoubles = 8 * 8 + 8;  // 8 self sub-triangles x 8, then the count
+constexpr double kNqOver4Pi = 0.07957747154594767;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Recurrence constants of the bases (uniform across a warp, so constant
+// memory broadcasts them):
+//   Koornwinder normalisation sqrt((2k+1)(2n+2)) at n(n+1)/2 + k;
+//   Jacobi P_m^{(0,2k+1)}: P_{m+1} = (cJacP x - cJacQ) P_m - cJacR P_{m-1} at k*21+m;
+//   Legendre: P_{k+1} = cLegA x P_k - cLegB P_{k-1}.
+__constant__ double cKoornNorm[(kNqTriOrder + 1) * (kNqTriOrder + 2) / 2];
+__constant__ double cJacP[kNqJac * kNqJac];
+__constant__ double cJacQ[kNqJac * kNqJac];
+__constant__ double cJacR[kNqJac * kNqJac];
+__constant__ double cLegA[kNqLeg];
+__constant__ double cLegB[kNqLeg];
+
+struct NqType {
+  int iptype, norder, np, nv;
+  int rule;            // 0..2: 8, 10 or 12 points per direction
+  int uvs, wts, umat;  // arena offsets of nodes (2 np), weights (np), umat (np x np)
+  double vert[8];      // corners of the reference domain
+};
+
+struct NqArgs {
+  double zr, zi, ar, ai, br, bi, eps;
+  const double* coefs;  // srccoefs, 9 per node
+  const NqType* types;
+  const int* ptype;
+  const int64_t* pstart;  // first node of each patch, 0-based
+  double* ptol;           // per-patch refinement tolerance
+  const double* arena;
+  int rule_off[3], rule_nq[3];  // xi[nq], eta[nq], w[nq] consecutive
+  int self_off, nself;          // Gauss-Legendre x[nself], w[nself]
+  const double* targ;           // 3 x nt
+  const double* uvt;            // 2 x nt
+  const longlong2* items;       // (pair, target); self pairs first
+  int64_t nitems, nself_items, npatches;
+  const int64_t* col_ind;
+  const int64_t* iquad;
+  double* wout;
+  double* scratch;
+  int64_t scratch_per_warp;
+  int np_max, stride, warp_doubles;
+  unsigned long long* counter;  // [0] next item, [1] kernel evaluations, [2] capped pairs
+};
+
+// Basis values at (u, v) -> prow[0..np) (when STORE) and the geometry
+// g = sum_l coefs_l P_l: xyz, d/du, d/dv.  Same bases as basis_pols.
+template <bool STORE>
+__device__ void basis_geom(int iptype, int n, double u, double v, const double* __restrict__ c,
+                           double* prow, double* g) {
+#pragma unroll
+  for (int k = 0; k < 9; ++k) g[k] = 0.0;
+  auto emit = [&](int idx, double p) {
+    if (STORE) prow[idx] = p;
+    const double* ci = c + 9 * idx;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) g[k] = fma(__ldg(ci + k), p, g[k]);
+  };
+  if (iptype == 1) {
+    double leg[kNqTriOrder + 1];
+    const double z = 2.0 * u + v - 1.0, y = 1.0 - v, y2 = y * y, x = 1.0 - 2.0 * v;
+    leg[0] = 1.0;
+    if (n >= 1) leg[1] = z;
+    for (int k = 1; k < n; ++k) leg[k + 1] = cLegA[k] * z * leg[k] - cLegB[k] * y2 * leg[k - 1];
+    for (int k = 0; k <= n; ++k) {
+      const double lk = leg[k];
+      const double b = 2.0 * k + 1.0;
+      int idx = k * (k + 1) / 2 + k;
+      emit(idx, lk * cKoornNorm[idx]);
+      if (n - k < 1) continue;
+      double jp = 1.0, jc = 0.5 * ((b + 2.0) * x - b);
+      idx = (k + 1) * (k + 2) / 2 + k;
+      emit(idx, lk * jc * cKoornNorm[idx]);
+      for (int m = 1; m < n - k; ++m) {
+        const int t = k * kNqJac + m;
+        const double jn = (cJacP[t] * x - cJacQ[t]) * jc - cJacR[t] * jp;
+        jp = jc;
+        jc = jn;
+        const int nn = m + 1 + k;
+        idx = nn * (nn + 1) / 2 + k;
+        emit(idx, lk * jc * cKoornNorm[idx]);
+      }
+    }
+  } else {
+    const bool leg = iptype == 11;
+    double pu[kNqLeg];
+    pu[0] = 1.0;
+    if (n >= 1) pu[1] = u;
+    for (int k = 1; k < n; ++k)
+      pu[k + 1] = leg ? cLegA[k] * u * pu[k] - cLegB[k] * pu[k - 1] : 2.0 * u * pu[k] - pu[k - 1];
+    double pvm = 0.0, pvc = 1.0;
+    for (int i = 0; i <= n; ++i) {
+      for (int j = 0; j <= n; ++j) emit(j + (n + 1) * i, pu[j] * pvc);
+      const double nx = i == 0 ? v : (leg ? cLegA[i] * v * pvc - cLegB[i] * pvm : 2.0 * v * pvc - pvm);
+      pvm = pvc;
+      pvc = nx;
+    }
+  }
+}
+
+// Combined-field kernel (alpha G + beta dG/dn_y) / 4pi at target x of the
+// source y with unit normal nr (host/nearquad.cpp LapComb / HelmComb).
+template <bool CPLX>
+__device__ __forceinline__ void kernel_val(const NqArgs& a, const double* y, const double* nr,
+                                           const double* x, double& re, double& im) {
+  const double dx = x[0] - y[0], dy = x[1] - y[1], dz = x[2] - y[2];
+  const double d = dx * nr[0] + dy * nr[1] + dz * nr[2];
+  const double r2 = dx * dx + dy * dy + dz * dz;
+  const double r = sqrt(r2);
+  const double ir = 1.0 / r;
+  const double dr3 = d * ir / r2;
+  if (!CPLX) {
+    re = (a.br * dr3 + a.ar * ir) * kNqOver4Pi;
+    im = 0.0;
+    return;
+  }
+  // (beta d (1 - ikr) / r^3 + alpha / r) e^{ikr},  1 - ikr = (1 + zi r) - i zr r
+  const double omr = 1.0 + a.zi * r, omi = -a.zr * r;
+  const double tr = (a.br * omr - a.bi * omi) * dr3 + a.ar * ir;
+  const double ti = (a.br * omi + a.bi * omr) * dr3 + a.ai * ir;
+  double s, c;
+  sincos(a.zr * r, &s, &c);
+  const double m = exp(-a.zi * r) * kNqOver4Pi;
+  re = (tr * c - ti * s) * m;
+  im = (tr * s + ti * c) * m;
+}
+
+// One rule node: basis row -> prow, kernel value -> (kr, ki); returns |J|.
+template <bool CPLX>
+__device__ double node_val(const NqArgs& a, const NqType* T, const double* c, double u, double v,
+                           double* prow, const double* x, double& kr, double& ki) {
+  double g[9];
+  basis_geom<true>(T->iptype, T->norder, u, v, c, prow, g);
+  const double n0 = g[4] * g[8] - g[5] * g[7];
+  const double n1 = g[5] * g[6] - g[3] * g[8];
+  const double n2 = g[3] * g[7] - g[4] * g[6];
+  const double jn = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+  const double inv = 1.0 / jn;
+  const double nr[3] = {n0 * inv, n1 * inv, n2 * inv};
+  kernel_val<CPLX>(a, g, nr, x, kr, ki);
+  return jn;
+}
+
+// Lanes own basis indices l = lane, lane + 32, ...: acc_l += sum over the
+// chunk's nodes of kv_q P_q,l.
+template <bool CPLX>
+__device__ __forceinline__ void accumulate(const double* P, const double* kv, int nv, int np,
+                                           int stride, double* acc, int lane) {
+  for (int l = lane; l < np; l += 32) {
+    double sr = 0.0, si = 0.0;
+    for (int q = 0; q < nv; ++q) {
+      const double p = P[q * stride + l];
+      sr = fma(kv[2 * q], p, sr);
+      if (CPLX) si = fma(kv[2 * q + 1], p, si);
+    }
+    acc[2 * l] += sr;
+    acc[2 * l + 1] += si;
+  }
+}
+
+// Integral vector over the parameter triangle v6 of K(x, y) P_l(y) dA -> dst.
+template <bool CPLX>
+__device__ void tri_integral(const NqArgs& a, const NqType* T, const double* c, const double* v6,
+                             const double* x, double* P, double* kv, double* acc, double* dst,
+                             int lane) {
+  const int np = T->np, stride = a.stride;
+  const int nq = a.rule_nq[T->rule];
+  const double* rule = a.arena + a.rule_off[T->rule];
+  const double ax = v6[2] - v6[0], ay = v6[3] - v6[1];
+  const double bx = v6[4] - v6[0], by = v6[5] - v6[1];
+  const double area2 = fabs(ax * by - ay * bx);
+  for (int l = lane; l < np; l += 32) acc[2 * l] = acc[2 * l + 1] = 0.0;
+  for (int q0 = 0; q0 < nq; q0 += 32) {
+    const int q = q0 + lane;
+    if (q < nq) {
+      const double xi = rule[q], eta = rule[nq + q], w = rule[2 * nq + q];
+      double kr, ki;
+      const double jn = node_val<CPLX>(a, T, c, v6[0] + xi * ax + eta * bx,
+                                       v6[1] + xi * ay + eta * by, P + lane * stride, x, kr, ki);
+      const double s = jn * w * area2;
+      kv[2 * lane] = kr * s;
+      kv[2 * lane + 1] = ki * s;
+    }
+    __syncwarp();
+    accumulate<CPLX>(P, kv, min(32, nq - q0), np, stride, acc, lane);
+    __syncwarp();
+  }
+  for (int l = lane; l < np; l += 32) {
+    dst[2 * l] = acc[2 * l];
+    dst[2 * l + 1] = acc[2 * l + 1];
+  }
+}
+
+// Adaptive integral for a target off the patch (host/nearquad.cpp:190-247):
+// pop a triangle, integrate its four children, accept their sum when it
+// agrees with the parent to tol (max over l) or at level 18, else push them.
+template <bool CPLX>
+__device__ void near_integral(const NqArgs& a, const NqType* T, const double* c, const double* x,
+                              double tol, double* P, double* kv, double* acc, double* out,
+                              double* vec, double* stk, int lane, unsigned long long& nev,
+                              int& capped) {
+  const int np = T->np, vs = 2 * a.np_max;
+  const int nq = a.rule_nq[T->rule];
+  for (int l = lane; l < np; l += 32) out[2 * l] = out[2 * l + 1] = 0.0;
+  const double* V = T->vert;
+  const int nroots = T->nv == 3 ? 1 : 2;
+  int sp = 0;
+  for (int r = 0; r < nroots; ++r) {
+    const double v6[6] = {V[0], V[1], V[2 + 2 * r], V[3 + 2 * r], V[4 + 2 * r], V[5 + 2 * r]};
+    if (lane == 0) {
+      for (int i = 0; i < 6; ++i) stk[kNqStackDoubles * sp + i] = v6[i];
+      stk[kNqStackDoubles * sp + 6] = 0.0;
+    }
+    tri_integral<CPLX>(a, T, c, v6, x, P, kv, acc, vec + size_t(sp) * vs, lane);
+    nev += nq;
+    ++sp;
+  }
+  __syncwarp();
+  int steps = 0;
+  while (sp > 0) {
+    if (++steps > kNqMaxSteps) {
+      capped = 1;
+      break;
+    }
+    const int top = sp - 1;
+    const double* e = stk + kNqStackDoubles * top;
+    const double v[6] = {e[0], e[1], e[2], e[3], e[4], e[5]};
+    const int lev = int(e[6]);
+    const double m01[2] = {0.5 * (v[0] + v[2]), 0.5 * (v[1] + v[3])};
+    const double m12[2] = {0.5 * (v[2] + v[4]), 0.5 * (v[3] + v[5])};
+    const double m20[2] = {0.5 * (v[4] + v[0]), 0.5 * (v[5] + v[1])};
+    const double ch[4][6] = {{v[0], v[1], m01[0], m01[1], m20[0], m20[1]},
+                             {m01[0], m01[1], v[2], v[3], m12[0], m12[1]},
+                             {m20[0], m20[1], m12[0], m12[1], v[4], v[5]},
+                             {m01[0], m01[1], m12[0], m12[1], m20[0], m20[1]}};
+    for (int q = 0; q < 4; ++q)
+      tri_integral<CPLX>(a, T, c, ch[q], x, P, kv, acc, vec + size_t(sp + q) * vs, lane);
+    nev += 4 * nq;
+    double err = 0.0;
+    const double* par = vec + size_t(top) * vs;
+    for (int l = lane; l < np; l += 32) {
+      double sr = 0.0, si = 0.0;
+      for (int q = 0; q < 4; ++q) {
+        sr += vec[size_t(sp + q) * vs + 2 * l];
+        si += vec[size_t(sp + q) * vs + 2 * l + 1];
+      }
+      acc[2 * l] = sr;
+      acc[2 * l + 1] = si;
+      const double dr = sr - par[2 * l], di = si - par[2 * l + 1];
+      err = fmax(err, CPLX ? sqrt(dr * dr + di * di) : fabs(dr));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) err = fmax(err, __shfl_xor_sync(kFull, err, o));
+    if (err <= tol || lev >= kNqMaxLevel) {
+      for (int l = lane; l < np; l += 32) {
+        out[2 * l] += acc[2 * l];
+        out[2 * l + 1] += acc[2 * l + 1];
+      }
+      sp = top;
+    } else {
+      for (int q = 0; q < 4; ++q)
+        for (int l = lane; l < np; l += 32) {
+          vec[size_t(top + q) * vs + 2 * l] = vec[size_t(sp + q) * vs + 2 * l];
+          vec[size_t(top + q) * vs + 2 * l + 1] = vec[size_t(sp + q) * vs + 2 * l + 1];
+        }
+      if (lane == 0)
+        for (int q = 0; q < 4; ++q) {
+          for (int i = 0; i < 6; ++i) stk[kNqStackDoubles * (top + q) + i] = ch[q][i];
+          stk[kNqStackDoubles * (top + q) + 6] = double(lev + 1);
+        }
+      sp = top + 4;
+    }
+    __syncwarp();
+  }
+}
+
+// Singular integral for a target at (u0, v0) on the patch
+// (host/nearquad.cpp:251-311): the patch split at the target's foot points
+// on the edges into triangles, each with a Duffy map in s and a sinh map in
+// the angle-like variable anchored at the closest edge point.
+template <bool CPLX>
+__device__ void self_integral(const NqArgs& a, const NqType* T, const double* c, double u0,
+                              double v0, double* P, double* kv, double* acc, double* sub,
+                              int lane, unsigned long long& nev) {
+  const int np = T->np, nself = a.nself;
+  double g[9];
+  basis_geom<false>(T->iptype, T->norder, u0, v0, c, nullptr, g);
+  const double x0[3] = {g[0], g[1], g[2]};
+  const double g11 = g[3] * g[3] + g[4] * g[4] + g[5] * g[5];
+  const double g12 = g[3] * g[6] + g[4] * g[7] + g[5] * g[8];
+  const double g22 = g[6] * g[6] + g[7] * g[7] + g[8] * g[8];
+  auto gdot = [&](double ax, double ay, double bx, double by) {
+    return ax * (g11 * bx + g12 * by) + ay * (g12 * bx + g22 * by);
+  };
+  if (lane == 0) {
+    int ns = 0;
+    const int nv = T->nv;
+    for (int e = 0; e < nv; ++e) {
+      const double ax = T->vert[2 * e], ay = T->vert[2 * e + 1];
+      const double bx = T->vert[2 * ((e + 1) % nv)], by = T->vert[2 * ((e + 1) % nv) + 1];
+      const double dx = bx - ax, dy = by - ay;
+      const double tau = gdot(u0 - ax, v0 - ay, dx, dy) / gdot(dx, dy, dx, dy);
+      double Pp[2][2], Qp[2][2];
+      int nsub;
+      if (tau <= 0.0) {
+        Pp[0][0] = ax, Pp[0][1] = ay, Qp[0][0] = bx, Qp[0][1] = by, nsub = 1;
+      } else if (tau >= 1.0) {
+        Pp[0][0] = bx, Pp[0][1] = by, Qp[0][0] = ax, Qp[0][1] = ay, nsub = 1;
+      } else {
+        const double fx = ax + tau * dx, fy = ay + tau * dy;
+        Pp[0][0] = fx, Pp[0][1] = fy, Qp[0][0] = ax, Qp[0][1] = ay;
+        Pp[1][0] = fx, Pp[1][1] = fy, Qp[1][0] = bx, Qp[1][1] = by;
+        nsub = 2;
+      }
+      for (int sb = 0; sb < nsub; ++sb) {
+        const double a0 = Pp[sb][0] - u0, a1 = Pp[sb][1] - v0;
+        const double b0 = Qp[sb][0] - Pp[sb][0], b1 = Qp[sb][1] - Pp[sb][1];
+        const double det = fabs(a0 * b1 - a1 * b0);
+        if (det <= 1e-300) continue;
+        const double h = sqrt(gdot(a0, a1, a0, a1));
+        const double L = sqrt(gdot(b0, b1, b0, b1));
+        double* o = sub + 8 * ns;
+        o[0] = a0, o[1] = a1, o[2] = b0, o[3] = b1, o[4] = det, o[5] = h / L;
+        o[6] = asinh(L / h);
+        ++ns;
+      }
+    }
+    sub[64] = double(ns);
+  }
+  __syncwarp();
+  const int nsub = int(sub[64]);
+  const double* xs = a.arena + a.self_off;
+  const double* ws = xs + nself;
+  for (int l = lane; l < np; l += 32) acc[2 * l] = acc[2 * l + 1] = 0.0;
+  const int per = nself * nself, total = nsub * per;
+  for (int q0 = 0; q0 < total; q0 += 32) {
+    const int q = q0 + lane;
+    if (q < total) {
+      const int si = q / per, rem = q - si * per;
+      const int iw = rem / nself, is = rem - iw * nself;
+      const double* o = sub + 8 * si;
+      const double W = o[6];
+      const double w = 0.5 * W * (xs[iw] + 1.0);
+      const double t = o[5] * sinh(w);
+      const double dtw = o[5] * cosh(w) * 0.5 * W * ws[iw];
+      const double ex = o[0] + t * o[2], ey = o[1] + t * o[3];
+      const double s = 0.5 * (xs[is] + 1.0);
+      const double jac = s * o[4] * dtw * 0.5 * ws[is];
+      double kr, ki;
+      const double jn =
+          node_val<CPLX>(a, T, c, u0 + s * ex, v0 + s * ey, P + lane * a.stride, x0, kr, ki);
+      kv[2 * lane] = kr * jn * jac;
+      kv[2 * lane + 1] = ki * jn * jac;
+    }
+    __syncwarp();
+    accumulate<CPLX>(P, kv, min(32, total - q0), np, a.stride, acc, lane);
+    __syncwarp();
+  }
+  nev += total;
+}
+
+// Per-patch tolerance 0.1 * eps * sqrt(min_j |J(u_j, v_j)| w_j); one warp
+// per patch.
+__global__ void __launch_bounds__(256) nq_tol_kernel(NqArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t p = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (p >= a.npatches) return;
+  const NqType* T = a.types + a.ptype[p];
+  const double* c = a.coefs + 9 * a.pstart[p];
+  double jw = 1e300;
+  for (int j = lane; j < T->np; j += 32) {
+    double g[9];
+    basis_geom<false>(T->iptype, T->norder, a.arena[T->uvs + 2 * j], a.arena[T->uvs + 2 * j + 1],
+                      c, nullptr, g);
+    const double n0 = g[4] * g[8] - g[5] * g[7];
+    const double n1 = g[5] * g[6] - g[3] * g[8];
+    const double n2 = g[3] * g[7] - g[4] * g[6];
+    jw = fmin(jw, sqrt(n0 * n0 + n1 * n1 + n2 * n2) * a.arena[T->wts + j]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) jw = fmin(jw, __shfl_xor_sync(kFull, jw, o));
+  if (lane == 0) a.ptol[p] = 0.1 * a.eps * sqrt(jw);
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(256) nq_pair_kernel(NqArgs a) {
+  extern __shared__ double nq_smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* P = nq_smem + size_t(wib) * a.warp_doubles;
+  double* kv = P + 32 * a.stride;
+  double* acc = kv + 64;
+  double* out = acc + 2 * a.np_max;
+  double* sub = out + 2 * a.np_max;
+  const int64_t gw = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  double* vec = a.scratch + gw * a.scratch_per_warp;
+  double* stk = vec + size_t(kNqSlots) * 2 * a.np_max;
+  unsigned long long nev = 0;
+  int capped = 0;
+  for (;;) {
+    long long idx = 0;
+    if (lane == 0) idx = (long long)atomicAdd(a.counter, 1ull);
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= a.nitems) break;
+    const longlong2 it = a.items[idx];
+    const int64_t k = it.x, t = it.y;
+    const int64_t p = a.col_ind[k] - 1;
+    const NqType* T = a.types + a.ptype[p];
+    const double* c = a.coefs + 9 * a.pstart[p];
+    const int np = T->np;
+    double* res;
+    if (idx < a.nself_items) {
+      self_integral<CPLX>(a, T, c, a.uvt[2 * t], a.uvt[2 * t + 1], P, kv, acc, sub, lane, nev);
+      res = acc;
+    } else {
+      near_integral<CPLX>(a, T, c, a.targ + 3 * t, a.ptol[p], P, kv, acc, out, vec, stk, lane,
+                          nev, capped);
+      res = out;
+    }
+    __syncwarp();
+    // nodal weights: w_j = sum_l I_l umat(l, j)
+    const double* U = a.arena + T->umat;
+    const int64_t base = a.iquad[k] - 1;
+    for (int j = lane; j < np; j += 32) {
+      double re = 0.0, im = 0.0;
+      for (int l = 0; l < np; ++l) {
+        const double u = U[l * np + j];
+        re = fma(res[2 * l], u, re);
+        if (CPLX) im = fma(res[2 * l + 1], u, im);
+      }
+      if (CPLX) {
+        a.wout[2 * (base + j)] = re;
+        a.wout[2 * (base + j) + 1] = im;
+      } else {
+        a.wout[base + j] = re;
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    atomicAdd(a.counter + 1, nev);
+    if (capped) atomicAdd(a.counter + 2, 1ull);
+  }
+}
+
+void fill_constants(cudaStream_t st) {
+  static thread_local std::vector<double> host;
+  if (host.empty()) {
+    host.assign((kNqTriOrder + 1) * (kNqTriOrder + 2) / 2 + 3 * kNqJac * kNqJac + 2 * kNqLeg, 0.0);
+    double* norm = host.data();
+    double* jp = norm + (kNqTriOrder + 1) * (kNqTriOrder + 2) / 2;
+    double* jq = jp + kNqJac * kNqJac;
+    double* jr = jq + kNqJac * kNqJac;
+    double* la = jr + kNqJac * kNqJac;
+    double* lb = la + kNqLeg;
+    for (int n = 0; n <= kNqTriOrder; ++n)
+      for (int k = 0; k <= n; ++k) norm[n * (n + 1) / 2 + k] = std::sqrt((2.0 * k + 1.0) * (2.0 * n + 2.0));
+    for (int k = 0; k < kNqJac; ++k) {
+      const double b = 2.0 * k + 1.0;
+      for (int m = 1; m < kNqJac; ++m) {
+        const double c0 = 2.0 * (m + 1.0) * (m + b + 1.0) * (2.0 * m + b);
+        jp[k * kNqJac + m] = (2.0 * m + b + 1.0) * (2.0 * m + b + 2.0) * (2.0 * m + b) / c0;
+        jq[k * kNqJac + m] = (2.0 * m + b + 1.0) * b * b / c0;
+        jr[k * kNqJac + m] = 2.0 * m * (m + b) * (2.0 * m + b + 2.0) / c0;
+      }
+    }
+    for (int k = 0; k < kNqLeg; ++k) {
+      la[k] = (2.0 * k + 1.0) / (k + 1.0);
+      lb[k] = k / (k + 1.0);
+    }
+  }
+  const double* h = host.data();
+  size_t off = 0;
+  auto put = [&](const void* sym, size_t n) {
+    cudaMemcpyToSymbolAsync(sym, h + off, n * sizeof(double), 0, cudaMemcpyHostToDevice, st);
+    off += n;
+  };
+  put(cKoornNorm, (kNqTriOrder + 1) * (kNqTriOrder + 2) / 2);
+  put(cJacP, kNqJac * kNqJac);
+  put(cJacQ, kNqJac * kNqJac);
+  put(cJacR, kNqJac * kNqJac);
+  put(cLegA, kNqLeg);
+  put(cLegB, kNqLeg);
+}
+
+template <class T>
+cudaError_t upload(DBuf<T>& d, const T* h, size_t n, cudaStream_t st) {
+  cudaError_t e = d.alloc(std::max<size_t>(n, 1));
+  if (e != cudaSuccess || n == 0) return e;
+  return cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+}  // namespace
+
+int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
+                    const int64_t* ipatch_id, const double* uvs_targ, double eps, int kind,
+                    cdouble zk, cdouble alpha, cdouble beta, int64_t nnz, const int64_t* row_ptr,
+                    const int64_t* col_ind, const int64_t* iquad, int64_t nquad,
+                    double* wnear_dev, cudaStream_t st, NearQuadStats* stats) {
+  if (stats) *stats = NearQuadStats{};
+  if (nnz == 0) return kOk;
+  if (nnz < 0 || nt <= 0 || ndt < 3 || !targs || !row_ptr || !col_ind || !iquad || !wnear_dev ||
+      s.npatches <= 0 || !s.srccoefs) {
+    set_last_error("getnearquad_gpu: invalid arguments");
+    return kErrArg;
+  }
+  if (row_ptr[0] != 1 || row_ptr[nt] - 1 != nnz || iquad[nnz] - 1 != nquad) {
+    set_last_error("getnearquad_gpu: row_ptr / iquad inconsistent with nnz / nquad");
+    return kErrArg;
+  }
+  // patch types, their node/weight/umat tables and the rules
+  std::map<std::pair<int, int>, int> tmap;
+  std::vector<NqType> types;
+  std::vector<double> arena;
+  std::vector<int> ptype(s.npatches);
+  std::vector<int64_t> pstart(s.npatches);
+  int np_max = 0;
+  for (int64_t p = 0; p < s.npatches; ++p) {
+    const int ip = int(s.iptype[p]), no = int(s.norders[p]);
+    const int np = int(s.npols(p));
+    if (!valid_patch(ip, no) || npols_of(ip, no) != np) {
+      set_last_error("getnearquad_gpu: patch " + std::to_string(p + 1) + " has an invalid type/order");
+      return kErrArg;
+    }
+    if (np > kNearQuadMaxNp) {
+      set_last_error("getnearquad_gpu: patch " + std::to_string(p + 1) + " has " +
+                     std::to_string(np) + " basis functions (device limit " +
+                     std::to_string(kNearQuadMaxNp) + ")");
+      return kErrArg;
+    }
+    auto key = std::make_pair(ip, no);
+    auto f = tmap.find(key);
+    if (f == tmap.end()) {
+      NqType T{};
+      T.iptype = ip;
+      T.norder = no;
+      T.np = np;
+      T.nv = boundary_vertices(ip, T.vert);
+      const int ng = nearquad_tri_ng(no);
+      T.rule = ng == 8 ? 0 : (ng == 10 ? 1 : 2);
+      std::vector<double> uvs(2 * np), umat(size_t(np) * np), vmat(size_t(np) * np), w(np);
+      if (disc_exps(ip, no, uvs.data(), umat.data(), vmat.data(), w.data())) {
+        set_last_error("getnearquad_gpu: no discretisation tables for a patch type");
+        return kErrTables;
+      }
+      T.uvs = int(arena.size());
+      arena.insert(arena.end(), uvs.begin(), uvs.end());
+      T.wts = int(arena.size());
+      arena.insert(arena.end(), w.begin(), w.end());
+      T.umat = int(arena.size());
+      arena.insert(arena.end(), umat.begin(), umat.end());
+      f = tmap.emplace(key, int(types.size())).first;
+      types.push_back(T);
+    }
+    ptype[p] = f->second;
+    pstart[p] = s.start(p);
+    np_max = std::max(np_max, np);
+  }
+  NqArgs a{};
+  const int ngs[3] = {8, 10, 12};
+  for (int r = 0; r < 3; ++r) {
+    std::vector<double> xi, eta, w;
+    nearquad_tri_rule(ngs[r], xi, eta, w);
+    a.rule_off[r] = int(arena.size());
+    a.rule_nq[r] = int(xi.size());
+    arena.insert(arena.end(), xi.begin(), xi.end());
+    arena.insert(arena.end(), eta.begin(), eta.end());
+    arena.insert(arena.end(), w.begin(), w.end());
+  }
+  a.nself = nearquad_self_order(eps);
+  {
+    std::vector<double> x(a.nself), w(a.nself);
+    gauss_legendre(a.nself, x.data(), w.data());
+    a.self_off = int(arena.size());
+    arena.insert(arena.end(), x.begin(), x.end());
+    arena.insert(arena.end(), w.begin(), w.end());
+  }
+  // work items, self pairs first, with the checks that keep every device
+  // access in bounds: patch index, row of wnear, self parameters
+  std::vector<longlong2> items, near_items;
+  items.reserve(nt);
+  near_items.reserve(nnz);
+  for (int64_t t = 0; t < nt; ++t) {
+    if (row_ptr[t + 1] < row_ptr[t]) {
+      set_last_error("getnearquad_gpu: row_ptr not monotone");
+      return kErrArg;
+    }
+    for (int64_t k = row_ptr[t] - 1; k < row_ptr[t + 1] - 1; ++k) {
+      const int64_t p = col_ind[k] - 1;
+      if (p < 0 || p >= s.npatches || iquad[k + 1] - iquad[k] != s.npols(p) || iquad[k] < 1) {
+        set_last_error("getnearquad_gpu: col_ind / iquad entry " + std::to_string(k + 1) +
+                       " out of range");
+        return kErrArg;
+      }
+      const bool self = ipatch_id && ipatch_id[t] == p + 1;
+      if (self && !uvs_targ) {
+        set_last_error("getnearquad_gpu: on-surface targets need uvs_targ");
+        return kErrArg;
+      }
+      (self ? items : near_items).push_back(make_longlong2(k, t));
+    }
+  }
+  const int64_t nself_items = int64_t(items.size());
+  items.insert(items.end(), near_items.begin(), near_items.end());
+  near_items.clear();
+  near_items.shrink_to_fit();
+  std::vector<double> targ3(3 * size_t(nt)), uvt(uvs_targ ? 2 * size_t(nt) : 0);
+  for (int64_t t = 0; t < nt; ++t)
+    for (int i = 0; i < 3; ++i) targ3[3 * t + i] = targs[size_t(ndt) * t + i];
+  if (uvs_targ) std::copy(uvs_targ, uvs_targ + 2 * size_t(nt), uvt.begin());
+
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int stride = np_max | 1;
+  const int warp_doubles = 32 * stride + 64 + 4 * np_max + kNqSubDoubles;
+  const size_t warp_bytes = sizeof(double) * size_t(warp_doubles);
+  const int wpb = int(std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / warp_bytes)));
+  const size_t smem = warp_bytes * wpb;
+  auto kern = kind == 1 ? nq_pair_kernel<true> : nq_pair_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  int bps = 0;
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 32 * wpb, smem);
+  if (e != cudaSuccess || bps < 1) {
+    set_last_error(std::string("getnearquad_gpu: launch configuration: ") + cudaGetErrorString(e));
+    return kErrCuda;
+  }
+  const int64_t want = (int64_t(items.size()) + wpb - 1) / wpb;
+  const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(nsm) * bps, want)));
+  const int64_t nwarps = int64_t(blocks) * wpb;
+
+  DBuf<double> d_coefs, d_arena, d_targ, d_uvt, d_tol, d_scratch;
+  DBuf<NqType> d_types;
+  DBuf<int> d_ptype;
+  DBuf<int64_t> d_pstart, d_col, d_iq;
+  DBuf<longlong2> d_items;
+  DBuf<unsigned long long> d_cnt;
+  const size_t per_warp = size_t(kNqSlots) * 2 * np_max + size_t(kNqSlots) * kNqStackDoubles;
+  if ((e = upload(d_coefs, s.srccoefs, 9 * size_t(s.npts), st)) != cudaSuccess ||
+      (e = upload(d_arena, arena.data(), arena.size(), st)) != cudaSuccess ||
+      (e = upload(d_targ, targ3.data(), targ3.size(), st)) != cudaSuccess ||
+      (e = upload(d_uvt, uvt.data(), uvt.size(), st)) != cudaSuccess ||
+      (e = d_tol.alloc(s.npatches)) != cudaSuccess ||
+      (e = d_scratch.alloc(per_warp * nwarps)) != cudaSuccess ||
+      (e = upload(d_types, types.data(), types.size(), st)) != cudaSuccess ||
+      (e = upload(d_ptype, ptype.data(), ptype.size(), st)) != cudaSuccess ||
+      (e = upload(d_pstart, pstart.data(), pstart.size(), st)) != cudaSuccess ||
+      (e = upload(d_col, col_ind, size_t(nnz), st)) != cudaSuccess ||
+      (e = upload(d_iq, iquad, size_t(nnz) + 1, st)) != cudaSuccess ||
+      (e = upload(d_items, items.data(), items.size(), st)) != cudaSuccess ||
+      (e = d_cnt.alloc(3)) != cudaSuccess ||
+      (e = cudaMemsetAsync(d_cnt.p, 0, 3 * sizeof(unsigned long long), st)) != cudaSuccess) {
+    set_last_error(std::string("getnearquad_gpu: device buffers: ") + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? kErrNoMem : kErrCuda;
+  }
+  fill_constants(st);
+  a.zr = zk.real();
+  a.zi = zk.imag();
+  a.ar = alpha.real();
+  a.ai = kind == 1 ? alpha.imag() : 0.0;
+  a.br = beta.real();
+  a.bi = kind == 1 ? beta.imag() : 0.0;
+  a.eps = eps;
+  a.coefs = d_coefs.p;
+  a.types = d_types.p;
+  a.ptype = d_ptype.p;
+  a.pstart = d_pstart.p;
+  a.ptol = d_tol.p;
+  a.arena = d_arena.p;
+  a.targ = d_targ.p;
+  a.uvt = d_uvt.p;
+  a.items = d_items.p;
+  a.nitems = int64_t(items.size());
+  a.nself_items = nself_items;
+  a.npatches = s.npatches;
+  a.col_ind = d_col.p;
+  a.iquad = d_iq.p;
+  a.wout = wnear_dev;
+  a.scratch = d_scratch.p;
+  a.scratch_per_warp = int64_t(per_warp);
+  a.np_max = np_max;
+  a.stride = stride;
+  a.warp_doubles = warp_doubles;
+  a.counter = d_cnt.p;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaEventCreate(&ev[0]);
+  cudaEventCreate(&ev[1]);
+  nq_tol_kernel<<<unsigned((s.npatches * 32 + 255) / 256), 256, 0, st>>>(a);
+  cudaEventRecord(ev[0], st);
+  kern<<<blocks, 32 * wpb, smem, st>>>(a);
+  cudaEventRecord(ev[1], st);
+  dev::note_launches(2);
+  unsigned long long cnt[3] = {0, 0, 0};
+  cudaMemcpyAsync(cnt, d_cnt.p, sizeof cnt, cudaMemcpyDeviceToHost, st);
+  e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  float ms = 0.f;
+  if (e == cudaSuccess) cudaEventElapsedTime(&ms, ev[0], ev[1]);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (e != cudaSuccess) {
+    set_last_error(std::string("getnearquad_gpu: ") + cudaGetErrorString(e));
+    return kErrCuda;
+  }
+  if (stats) {
+    stats->device_ms = ms;
+    stats->kernel_evals = int64_t(cnt[1]);
+    stats->self_targets = nself_items;
+    stats->near_targets = int64_t(items.size()) - nself_items;
+  }
+  if (cnt[2]) {
+    set_last_error("getnearquad_gpu: " + std::to_string(cnt[2]) +
+                   " warps hit the refinement-step cap");
+    return kErrTimeout;
+  }
+  return kOk;
+}
+
+}  // namespace bie

@@ -85,18 +85,9 @@ struct TriRule {
 };
 
 TriRule make_tri_rule(int ng) {
-  std::vector<double> x(ng), w(ng);
-  gauss_legendre(ng, x.data(), w.data());
   TriRule r;
   r.nq = ng * ng;
-  for (int i = 0; i < ng; ++i)
-    for (int j = 0; j < ng; ++j) {
-      const double a = 0.5 * (x[i] + 1.0), wa = 0.5 * w[i];
-      const double b = 0.5 * (x[j] + 1.0), wb = 0.5 * w[j];
-      r.xi.push_back(a);
-      r.eta.push_back(b * (1.0 - a));
-      r.w.push_back(wa * wb * (1.0 - a));
-    }
+  nearquad_tri_rule(ng, r.xi, r.eta, r.w);
   return r;
 }
 
@@ -319,14 +310,13 @@ int run(const K& ker, const Surf& s, int ndt, int64_t nt, const double* targs,
   std::vector<int64_t> col_ptr(s.npatches + 1), row_ind(nnz), iper(nnz);
   rsc_to_csc(s.npatches, nt, nnz, row_ptr, col_ind, col_ptr.data(), row_ind.data(), iper.data());
   // rule sizes from the requested tolerance
-  const double digits = std::max(1.0, -std::log10(std::max(eps, 1e-15)));
-  const int nself = std::min(40, std::max(12, int(std::ceil(2.2 * digits)) + 4));
+  const int nself = nearquad_self_order(eps);
   std::vector<double> xs(nself), ws(nself);
   gauss_legendre(nself, xs.data(), ws.data());
   std::map<int, TriRule> rules;
   for (int64_t p = 0; p < s.npatches; ++p) {
     const int no = int(s.norders[p]);
-    const int ng = no <= 6 ? 8 : (no <= 10 ? 10 : 12);
+    const int ng = nearquad_tri_ng(no);
     if (!rules.count(ng)) rules[ng] = make_tri_rule(ng);
   }
   std::atomic<int64_t> nev_total{0}, nself_total{0}, nnear_total{0};
@@ -362,7 +352,7 @@ int run(const K& ker, const Surf& s, int ndt, int64_t nt, const double* targs,
         }
       }
       const double tol = 0.1 * eps * std::sqrt(jwmin);
-      const int ng = g.no <= 6 ? 8 : (g.no <= 10 ? 10 : 12);
+      const int ng = nearquad_tri_ng(g.no);
       PatchTree tree(g, rules.at(ng));
       sints.resize(np);
       row.resize(np);
@@ -409,6 +399,30 @@ int run(const K& ker, const Surf& s, int ndt, int64_t nt, const double* targs,
 }
 
 }  // namespace
+
+int nearquad_tri_ng(int norder) { return norder <= 6 ? 8 : (norder <= 10 ? 10 : 12); }
+
+int nearquad_self_order(double eps) {
+  const double digits = std::max(1.0, -std::log10(std::max(eps, 1e-15)));
+  return std::min(40, std::max(12, int(std::ceil(2.2 * digits)) + 4));
+}
+
+void nearquad_tri_rule(int ng, std::vector<double>& xi, std::vector<double>& eta,
+                       std::vector<double>& w) {
+  std::vector<double> x(ng), wg(ng);
+  gauss_legendre(ng, x.data(), wg.data());
+  xi.clear();
+  eta.clear();
+  w.clear();
+  for (int i = 0; i < ng; ++i)
+    for (int j = 0; j < ng; ++j) {
+      const double a = 0.5 * (x[i] + 1.0), wa = 0.5 * wg[i];
+      const double b = 0.5 * (x[j] + 1.0), wb = 0.5 * wg[j];
+      xi.push_back(a);
+      eta.push_back(b * (1.0 - a));
+      w.push_back(wa * wb * (1.0 - a));
+    }
+}
 
 int getnearquad(const Surf& s, int ndt, int64_t nt, const double* targs, const int64_t* ipatch_id,
                 const double* uvs_targ, double eps, int kind, cdouble zk, cdouble alpha,

@@ -17,6 +17,7 @@
 #pragma once
 #include <complex>
 #include <cstdint>
+#include <vector>
 
 #include "setup.h"
 
@@ -26,7 +27,18 @@ struct NearQuadStats {
   int64_t kernel_evals = 0;
   int64_t self_targets = 0;
   int64_t near_targets = 0;
+  double device_ms = 0;  // device generator: time of its pair kernel
 };
+
+// Rule parameters shared by this generator and the device one
+// (cuda/nearquad_gpu.h): points per direction of the collapsed Gauss rule for
+// a patch of order norder (8, 10 or 12), points per direction of the self
+// rule for tolerance eps, and the collapsed rule itself on the simplex
+// (0,0),(1,0),(0,1) (ng*ng nodes, weights summing to 1/2).
+int nearquad_tri_ng(int norder);
+int nearquad_self_order(double eps);
+void nearquad_tri_rule(int ng, std::vector<double>& xi, std::vector<double>& eta,
+                       std::vector<double>& w);
 
 // kind 0: Laplace (alpha, beta real; wnear real), kind 1: Helmholtz (complex).
 // ipatch_id is 1-based, -1 for off-surface targets; uvs_targ (2,nt).

@@ -304,10 +304,27 @@ class Setup:
     rads: np.ndarray = field(repr=False)
 
 
+def _engine(engine: str) -> str:
+    if engine not in ("auto", "cpu", "gpu"):
+        raise ValueError(f"engine must be 'auto', 'cpu' or 'gpu', not {engine!r}")
+    if engine == "auto":
+        import torch
+        return "gpu" if torch.cuda.is_available() else "cpu"
+    return engine
+
+
 def getnearquad(s: Surface, kind: int, eps: float, params, targs, ipatch_id, uvs_targ,
-                row_ptr, col_ind, iquad, rfac0):
+                row_ptr, col_ind, iquad, rfac0, engine: str = "auto", stats=None):
     """getnearquad_{lap,helm}_comb_dir_eval; params = (alpha, beta) for
-    Laplace, (k, alpha, beta) for Helmholtz."""
+    Laplace, (k, alpha, beta) for Helmholtz.  engine "cpu" runs the host
+    generator, "gpu" the device one (same rules and tolerance), "auto" the
+    device one when a CUDA device is visible.  stats (engine "gpu"): an int64
+    array of 4 that receives kernel evaluations, self pairs, near pairs and
+    the device time of the pair kernel in microseconds."""
+    engine = _engine(engine)
+    if engine == "gpu":
+        return _getnearquad_gpu(s, kind, eps, params, targs, ipatch_id, uvs_targ, row_ptr,
+                                col_ind, iquad, rfac0, stats)
     lib = _init()
     targs = np.ascontiguousarray(targs, float)
     nt = targs.shape[0]
@@ -334,10 +351,43 @@ def getnearquad(s: Surface, kind: int, eps: float, params, targs, ipatch_id, uvs
     return w[:nquad]
 
 
-def setup(s: Surface, kind: int, eps: float, params, targs=None, ipatch_id=None, uvs_targ=None):
+def _getnearquad_gpu(s, kind, eps, params, targs, ipatch_id, uvs_targ, row_ptr, col_ind, iquad,
+                     rfac0, stats):
+    lib = _init()
+    targs = np.ascontiguousarray(targs, float)
+    nt = targs.shape[0]
+    nquad = int(iquad[-1] - 1)
+    ipatch_id = np.ascontiguousarray(ipatch_id, np.int64)
+    uvs_targ = np.ascontiguousarray(uvs_targ, float)
+    st = np.zeros(4, np.int64)
+    args = (s.npatches, L.ptr(s.norders), L.ptr(s.ixyzs), L.ptr(s.iptype), s.npts,
+            L.ptr(s.srccoefs), L.ptr(s.srcvals), targs.shape[1], nt, L.ptr(targs),
+            L.ptr(ipatch_id), L.ptr(uvs_targ), eps)
+    tail = (1, col_ind.shape[0], L.ptr(row_ptr), L.ptr(col_ind), L.ptr(iquad), rfac0, nquad)
+    if kind == 0:
+        dp = np.asarray(params, float)
+        w = np.zeros(max(nquad, 1))
+        L.check(lib.bie_getnearquad_lap_comb_dir_eval_gpu(*args, L.ptr(dp), *tail, L.ptr(w),
+                                                           L.ptr(st)),
+                "getnearquad_lap_comb_dir_eval_gpu")
+    else:
+        zp = np.ascontiguousarray(np.asarray(params, complex)).view(float)
+        w = np.zeros(max(nquad, 1), complex)
+        L.check(lib.bie_getnearquad_helm_comb_dir_eval_gpu(*args, L.ptr(zp), *tail,
+                                                            w.view(float).ctypes.data_as(L.PDBL),
+                                                            L.ptr(st)),
+                "getnearquad_helm_comb_dir_eval_gpu")
+    if stats is not None:
+        stats[:len(stats)] = st[:len(stats)]
+    return w[:nquad]
+
+
+def setup(s: Surface, kind: int, eps: float, params, targs=None, ipatch_id=None, uvs_targ=None,
+          engine: str = "auto", stats=None):
     """The setup of lap_comb_dir_eval / helm_comb_dir_solver: near list, far
     order, oversampled geometry and near quadrature.  targs defaults to the
-    surface nodes (on-surface, with self interactions)."""
+    surface nodes (on-surface, with self interactions).  engine and stats:
+    the near quadrature generator and its counters (see getnearquad)."""
     if targs is None:
         targs = s.srcvals
         ipatch_id, uvs_targ = s.patch_id_uvs()
@@ -360,6 +410,6 @@ def setup(s: Surface, kind: int, eps: float, params, targs=None, ipatch_id=None,
     so = Surface(novers, ixyzso, s.iptype, srcover, np.zeros((srcover.shape[0], 9)))
     wover = so.qwts()
     wnear = getnearquad(s, kind, eps, params, targs, ipatch_id, uvs_targ, row_ptr, col_ind, iquad,
-                        rfac0)
+                        rfac0, engine=engine, stats=stats)
     return Setup(NearField(row_ptr, col_ind, iquad, wnear), Oversampled(novers, ixyzso, srcover, wover),
                  rfac, rfac0, cms, rads)

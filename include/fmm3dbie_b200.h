@@ -141,6 +141,34 @@ int bie_getnearquad_helm_comb_dir_eval(int64_t npatches, const int64_t* norders,
                                        const int64_t* col_ind, const int64_t* iquad,
                                        double rfac0, int64_t nquad, double* wnear);
 
+/* The same two generators on the device (host buffers; the call returns
+ * when the weights are in wnear).  Same arguments as the host versions plus
+ * stats (nullable, 4 entries): kernel evaluations, self pairs, near pairs,
+ * device time of the generator's pair kernel in microseconds.
+ * The rules, tolerance and refinement are the host generator's; the weights
+ * agree with it to the requested tolerance.  Patches with more than 256
+ * basis functions are refused (BIE_ERR_ARG).  No reference counterpart: the
+ * reference generates near quadrature on the CPU only. */
+int bie_getnearquad_lap_comb_dir_eval_gpu(
+    int64_t npatches, const int64_t* norders, const int64_t* ixyzs, const int64_t* iptype,
+    int64_t npts, const double* srccoefs, const double* srcvals, int64_t ndtarg, int64_t ntarg,
+    const double* targs, const int64_t* ipatch_id, const double* uvs_targ, double eps,
+    const double* dpars, int64_t iquadtype, int64_t nnz, const int64_t* row_ptr,
+    const int64_t* col_ind, const int64_t* iquad, double rfac0, int64_t nquad, double* wnear,
+    int64_t* stats);
+int bie_getnearquad_helm_comb_dir_eval_gpu(
+    int64_t npatches, const int64_t* norders, const int64_t* ixyzs, const int64_t* iptype,
+    int64_t npts, const double* srccoefs, const double* srcvals, int64_t ndtarg, int64_t ntarg,
+    const double* targs, const int64_t* ipatch_id, const double* uvs_targ, double eps,
+    const double* zpars, int64_t iquadtype, int64_t nnz, const int64_t* row_ptr,
+    const int64_t* col_ind, const int64_t* iquad, double rfac0, int64_t nquad, double* wnear,
+    int64_t* stats);
+/* Near quadrature engine of the setups inside the simple evaluators and
+ * solvers (lap/helm_comb_dir_eval, *_solver): 1 = device (default), 0 =
+ * host.  Patches above the device limit always use the host generator. */
+int bie_set_nearquad_engine(int64_t engine);
+int64_t bie_get_nearquad_engine(void);
+
 /* ---- layer potentials on the GPU (host buffers) --------------------------- */
 /* lpcomp_lap_comb_dir_addsub (lap_comb_dir.f90:633): principal value of
  * (alpha S_0 + beta D_0) sigma at the surface nodes. ndd=2, dpars=(alpha,beta),
