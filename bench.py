@@ -290,6 +290,9 @@ def main():
                     help="skip the batched leg (64 plane-wave right-hand sides)")
     ap.add_argument("--torus", action="store_true",
                     help="also run the torus warm-start leg (trained warm start; ~1-2 min host setup)")
+    ap.add_argument("--nearquad-only", type=int, default=0, metavar="NREF",
+                    help="only run the device near-quadrature generator (Helmholtz, eps 1e-7) on "
+                         "the (1,2,3) ellipsoid refined NREF times, order 6, and print its counters")
     ap.add_argument("--no-nearquad", action="store_true",
                     help="skip the near-quadrature generator comparison (host vs device)")
     ap.add_argument("--uneven", action="store_true",
@@ -299,6 +302,8 @@ def main():
         return reference_arm(args)
     if args.matvec_only:
         return matvec_only(args)
+    if args.nearquad_only:
+        return nearquad_only(args.nearquad_only)
 
     import torch
     import torch.distributed as dist
@@ -693,6 +698,30 @@ def uneven_leg(dev, kinds=(0, 1)):
         res["speedup_vs_fp64"] = res["fp64"]["ms"] / res["mixed"]["ms"]
         out["laplace" if kind == 0 else "helmholtz"] = res
     return out
+
+
+def nearquad_only(nref):
+    """Device near-quadrature generator alone (two calls; the second is
+    reported), for profiling."""
+    from fmm3dbie_b200 import surface as S
+    s = S.icosa_ellipsoid(nref, 6, (1.0, 2.0, 3.0))
+    targs = s.srcvals
+    ipatch_id, uvs = s.patch_id_uvs()
+    rfac, rfac0 = S.get_rfacs(6, 1)
+    cms, rads = S.get_centroid_rads(s)
+    row_ptr, col_ind = S.findnear(cms, rads * rfac, targs)
+    iquad = S.get_iquad_rsc(s, row_ptr, col_ind)
+    gs = np.zeros(4, np.int64)
+    for _ in range(2):
+        t0 = time.time()
+        S.getnearquad(s, 1, EPS, ZPARS, targs, ipatch_id, uvs, row_ptr, col_ind, iquad, rfac0,
+                      engine="gpu", stats=gs)
+        dt = time.time() - t0
+    print(json.dumps({"nearquad": {"npts": s.npts, "pairs": int(gs[1] + gs[2]),
+                                   "self_pairs": int(gs[1]), "kernel_evals": int(gs[0]),
+                                   "device_kernel_ms": gs[3] / 1e3, "call_s": round(dt, 4),
+                                   "gevals_per_s": float(gs[0]) / (gs[3] * 1e3)}}))
+    return 0
 
 
 def matvec_only(args):

@@ -20,6 +20,8 @@
 
 #include "device.cuh"
 
+#include "trig_table.cuh"
+
 namespace bie {
 namespace dev {
 
@@ -100,42 +102,6 @@ __global__ void strengths_kernel(Geometry g, KParams kp, const double* __restric
 // The phase kr carries an absolute error of about kr 2^-24 in single
 // precision already; __sincosf's scaled argument adds an error of the same
 // order, so no separate range reduction is done.
-// Table-driven sine and cosine for the FP64 far field (the table-driven
-// reduction of P. T. P. Tang, ACM TOMS 15 (1989) / 16 (1990)):
-//   x = j (2 pi / N) + rho,  |rho| <= pi / N,
-//   sin x = S_j cos rho + C_j sin rho,  cos x = C_j cos rho - S_j sin rho,
-// with (C_j, S_j) = (cos, sin)(2 pi j / N) from a per-block table and the
-// Taylor series of sin rho (to rho^5) and cos rho (to rho^6), whose first
-// omitted terms are below 1e-17 for |rho| <= pi/256.  2 pi / N is split as
-// C1 + C2 with C1 rounded to 24 bits, so j C1 is exact for |j| < 2^29.
-constexpr int kTrigN = 256;
-constexpr double kTrigStep = 0.02454369260617026;     // 2 pi / 256
-constexpr double kTrigInvStep = 40.74366543152521;    // 256 / (2 pi)
-constexpr double kTrigC1 = 0.02454369328916073;       // float(2 pi / 256)
-constexpr double kTrigC2 = -6.829904687791004e-10;    // 2 pi / 256 - C1
-
-// Fills tab[q] = (cos, sin)(2 pi q / N) with the block's threads.
-__device__ __forceinline__ void fill_trig_table(double2* tab) {
-  for (int q = threadIdx.x; q < kTrigN; q += blockDim.x) {
-    double sq, cq;
-    sincos(double(q) * kTrigStep, &sq, &cq);
-    tab[q] = make_double2(cq, sq);
-  }
-}
-
-__device__ __forceinline__ void sincos_tab(double x, const double2* tab, double& s, double& c) {
-  const double jd = rint(x * kTrigInvStep);
-  const int j = int(jd) & (kTrigN - 1);
-  double rho = fma(-jd, kTrigC1, x);
-  rho = fma(-jd, kTrigC2, rho);
-  const double r2 = rho * rho;
-  const double sp = fma(rho * r2, fma(r2, 1.0 / 120.0, -1.0 / 6.0), rho);
-  const double cp = fma(r2, fma(r2, fma(r2, -1.0 / 720.0, 1.0 / 24.0), -0.5), 1.0);
-  const double2 t = tab[j];
-  s = fma(t.y, cp, t.x * sp);
-  c = fma(t.x, cp, -(t.y * sp));
-}
-
 // CHECK = false drops the r^2 >= thresh^2 test; callers use it only where no
 // pair of the tile can fall below the threshold, so the result is the same.
 template <bool CHECK = true>

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <string>
 #include <utility>
@@ -24,6 +25,7 @@
 
 #include "../host/basis.h"
 #include "plan.h"
+#include "trig_table.cuh"
 
 namespace bie {
 namespace {
@@ -33,7 +35,7 @@ constexpr int kNqMaxLevel = 18;
 // (one other root, three siblings per level, four at the deepest level) and
 // four children computed above the top.
 constexpr int kNqSlots = 64;
-constexpr int kNqStackDoubles = 8;  // per pending triangle: 6 vertex coordinates, level
+constexpr int kNqStackDoubles = 8;  // per pending triangle: 6 vertex coordinates, level, cache index
 constexpr int kNqMaxSteps = 1 << 16;
 constexpr int kNqTriOrder = kMaxOrder;  // Koornwinder tables up to order 20
 constexpr int kNqLeg = 41;              // tensor bases up to order 40
@@ -73,29 +75,53 @@ struct NqArgs {
   int self_off, nself;          // Gauss-Legendre x[nself], w[nself]
   const double* targ;           // 3 x nt
   const double* uvt;            // 2 x nt
-  const longlong2* items;       // (pair, target); self pairs first
-  int64_t nitems, nself_items, npatches;
+  const longlong2* items;       // (pair, target); self pairs first, then by patch
+  int64_t item_lo, item_hi;     // this launch's item range
+  int64_t nself_items, npatches;
+  // Cache of the uniform refinement levels 0..cache_levels of every root
+  // triangle of the patches in the current group: per triangle (root r,
+  // heap index h) and rule node q, the geometry xyz, unit normal and
+  // |J| w_q area2 (7 x nq, node fastest) followed by the basis rows (nq x np).
+  double* cache;
+  const int64_t* coff;  // per patch: offset of its block in `cache` (-1: not in this group)
+  int cache_levels;     // -1: no cache
+  int cache_h;          // triangles per root: (4^(cache_levels+1) - 1) / 3
   const int64_t* col_ind;
   const int64_t* iquad;
   double* wout;
   double* scratch;
   int64_t scratch_per_warp;
   int np_max, stride, warp_doubles;
-  unsigned long long* counter;  // [0] next item, [1] kernel evaluations, [2] capped pairs
+  unsigned long long* next;  // this launch's item counter
+  unsigned long long* stat;  // [0] kernel evaluations, [1] capped pairs
 };
 
 // Basis values at (u, v) -> prow[0..np) (when STORE) and the geometry
 // g = sum_l coefs_l P_l: xyz, d/du, d/dv.  Same bases as basis_pols.
-template <bool STORE>
+// Coefficients: 9 per basis function in global memory, or (SHARED) the
+// warp's copy in shared memory padded to 10 so that pairs load as one
+// 16-byte access.
+template <bool STORE, bool SHARED = false>
 __device__ void basis_geom(int iptype, int n, double u, double v, const double* __restrict__ c,
                            double* prow, double* g) {
 #pragma unroll
   for (int k = 0; k < 9; ++k) g[k] = 0.0;
   auto emit = [&](int idx, double p) {
     if (STORE) prow[idx] = p;
-    const double* ci = c + 9 * idx;
+    if (SHARED) {
+      const double2* ci = reinterpret_cast<const double2*>(c + 10 * idx);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) g[k] = fma(__ldg(ci + k), p, g[k]);
+      for (int k = 0; k < 4; ++k) {
+        const double2 cc = ci[k];
+        g[2 * k] = fma(cc.x, p, g[2 * k]);
+        g[2 * k + 1] = fma(cc.y, p, g[2 * k + 1]);
+      }
+      g[8] = fma(ci[4].x, p, g[8]);
+    } else {
+      const double* ci = c + 9 * idx;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) g[k] = fma(__ldg(ci + k), p, g[k]);
+    }
   };
   if (iptype == 1) {
     double leg[kNqTriOrder + 1];
@@ -141,15 +167,18 @@ __device__ void basis_geom(int iptype, int n, double u, double v, const double* 
 
 // Combined-field kernel (alpha G + beta dG/dn_y) / 4pi at target x of the
 // source y with unit normal nr (host/nearquad.cpp LapComb / HelmComb).
+// 1/r from rsqrt; e^{i Re(k) r} from the block's sine/cosine table; the
+// decay e^{-Im(k) r} only for complex wavenumbers.
 template <bool CPLX>
-__device__ __forceinline__ void kernel_val(const NqArgs& a, const double* y, const double* nr,
-                                           const double* x, double& re, double& im) {
+__device__ __forceinline__ void kernel_val(const NqArgs& a, const double2* tab, const double* y,
+                                           const double* nr, const double* x, double& re,
+                                           double& im) {
   const double dx = x[0] - y[0], dy = x[1] - y[1], dz = x[2] - y[2];
   const double d = dx * nr[0] + dy * nr[1] + dz * nr[2];
   const double r2 = dx * dx + dy * dy + dz * dz;
-  const double r = sqrt(r2);
-  const double ir = 1.0 / r;
-  const double dr3 = d * ir / r2;
+  const double ir = rsqrt(r2);
+  const double r = r2 * ir;
+  const double dr3 = d * ir * ir * ir;
   if (!CPLX) {
     re = (a.br * dr3 + a.ar * ir) * kNqOver4Pi;
     im = 0.0;
@@ -160,63 +189,143 @@ __device__ __forceinline__ void kernel_val(const NqArgs& a, const double* y, con
   const double tr = (a.br * omr - a.bi * omi) * dr3 + a.ar * ir;
   const double ti = (a.br * omi + a.bi * omr) * dr3 + a.ai * ir;
   double s, c;
-  sincos(a.zr * r, &s, &c);
-  const double m = exp(-a.zi * r) * kNqOver4Pi;
+  dev::sincos_tab(a.zr * r, tab, s, c);
+  const double m = (a.zi != 0.0 ? exp(-a.zi * r) : 1.0) * kNqOver4Pi;
   re = (tr * c - ti * s) * m;
   im = (tr * s + ti * c) * m;
 }
 
 // One rule node: basis row -> prow, kernel value -> (kr, ki); returns |J|.
 template <bool CPLX>
-__device__ double node_val(const NqArgs& a, const NqType* T, const double* c, double u, double v,
-                           double* prow, const double* x, double& kr, double& ki) {
+__device__ double node_val(const NqArgs& a, const double2* tab, const NqType* T, const double* c,
+                           double u, double v, double* prow, const double* x, double& kr,
+                           double& ki) {
   double g[9];
-  basis_geom<true>(T->iptype, T->norder, u, v, c, prow, g);
+  basis_geom<true, true>(T->iptype, T->norder, u, v, c, prow, g);
   const double n0 = g[4] * g[8] - g[5] * g[7];
   const double n1 = g[5] * g[6] - g[3] * g[8];
   const double n2 = g[3] * g[7] - g[4] * g[6];
-  const double jn = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
-  const double inv = 1.0 / jn;
+  const double j2 = n0 * n0 + n1 * n1 + n2 * n2;
+  const double inv = rsqrt(j2);
   const double nr[3] = {n0 * inv, n1 * inv, n2 * inv};
-  kernel_val<CPLX>(a, g, nr, x, kr, ki);
-  return jn;
+  kernel_val<CPLX>(a, tab, g, nr, x, kr, ki);
+  return j2 * inv;
 }
 
 // Lanes own basis indices l = lane, lane + 32, ...: acc_l += sum over the
-// chunk's nodes of kv_q P_q,l.
+// chunk's nodes of kv_q P_q,l (P and kv in shared memory; two partial sums
+// per component to halve the dependent FMA chain).
 template <bool CPLX>
 __device__ __forceinline__ void accumulate(const double* P, const double* kv, int nv, int np,
                                            int stride, double* acc, int lane) {
+  const double2* kv2 = reinterpret_cast<const double2*>(kv);
   for (int l = lane; l < np; l += 32) {
-    double sr = 0.0, si = 0.0;
-    for (int q = 0; q < nv; ++q) {
-      const double p = P[q * stride + l];
-      sr = fma(kv[2 * q], p, sr);
-      if (CPLX) si = fma(kv[2 * q + 1], p, si);
+    double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0;
+    int q = 0;
+    for (; q + 1 < nv; q += 2) {
+      const double p0 = P[q * stride + l], p1 = P[(q + 1) * stride + l];
+      const double2 k0 = kv2[q], k1 = kv2[q + 1];
+      s0r = fma(k0.x, p0, s0r);
+      s1r = fma(k1.x, p1, s1r);
+      if (CPLX) {
+        s0i = fma(k0.y, p0, s0i);
+        s1i = fma(k1.y, p1, s1i);
+      }
     }
-    acc[2 * l] += sr;
-    acc[2 * l + 1] += si;
+    if (q < nv) {
+      const double p0 = P[q * stride + l];
+      const double2 k0 = kv2[q];
+      s0r = fma(k0.x, p0, s0r);
+      if (CPLX) s0i = fma(k0.y, p0, s0i);
+    }
+    acc[2 * l] += s0r + s1r;
+    acc[2 * l + 1] += s0i + s1i;
+  }
+}
+
+// Asynchronous global -> shared copy of n doubles (both addresses 16-byte
+// aligned): 16-byte cp.async pieces strided over the lanes, an odd last
+// double by lane 0.  Completed by cp_async_wait_all() and a __syncwarp().
+__device__ __forceinline__ void copy_async(double* dst, const double* src, int n, int lane) {
+  const int n16 = n >> 1;
+  for (int i = lane; i < n16; i += 32) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(dst + 2 * i));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src + 2 * i)
+                 : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  if ((n & 1) && lane == 0) dst[n - 1] = __ldg(src + n - 1);
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Child q of the 4-way split of parameter triangle v (host/nearquad.cpp
+// PatchTree::children): the three corner triangles, then the middle one.
+__device__ __forceinline__ void child_tri(const double* v, int q, double* o) {
+  const double m01x = 0.5 * (v[0] + v[2]), m01y = 0.5 * (v[1] + v[3]);
+  const double m12x = 0.5 * (v[2] + v[4]), m12y = 0.5 * (v[3] + v[5]);
+  const double m20x = 0.5 * (v[4] + v[0]), m20y = 0.5 * (v[5] + v[1]);
+  if (q == 0) {
+    o[0] = v[0], o[1] = v[1], o[2] = m01x, o[3] = m01y, o[4] = m20x, o[5] = m20y;
+  } else if (q == 1) {
+    o[0] = m01x, o[1] = m01y, o[2] = v[2], o[3] = v[3], o[4] = m12x, o[5] = m12y;
+  } else if (q == 2) {
+    o[0] = m20x, o[1] = m20y, o[2] = m12x, o[3] = m12y, o[4] = v[4], o[5] = v[5];
+  } else {
+    o[0] = m01x, o[1] = m01y, o[2] = m12x, o[3] = m12y, o[4] = m20x, o[5] = m20y;
   }
 }
 
 // Integral vector over the parameter triangle v6 of K(x, y) P_l(y) dA -> dst.
+// cached: the triangle's cache block (geometry and basis rows at the rule
+// nodes) or null, in which case they are evaluated here.
 template <bool CPLX>
-__device__ void tri_integral(const NqArgs& a, const NqType* T, const double* c, const double* v6,
-                             const double* x, double* P, double* kv, double* acc, double* dst,
-                             int lane) {
+__device__ void tri_integral(const NqArgs& a, const double2* tab, const NqType* T, const double* c,
+                             const double* v6, const double* cached, const double* x, double* P,
+                             double* kv, double* acc, double* dst, int lane) {
   const int np = T->np, stride = a.stride;
   const int nq = a.rule_nq[T->rule];
+  for (int l = lane; l < np; l += 32) acc[2 * l] = acc[2 * l + 1] = 0.0;
+  if (cached) {
+    for (int q0 = 0; q0 < nq; q0 += 32) {
+      const int q = q0 + lane;
+      const int nv = min(32, nq - q0);
+      // basis rows of the chunk into the P buffer while the kernel values
+      // are computed
+      copy_async(P, cached + 7 * nq + size_t(q0) * np, nv * np, lane);
+      if (q < nq) {
+        const double y[3] = {__ldg(cached + q), __ldg(cached + nq + q), __ldg(cached + 2 * nq + q)};
+        const double nr[3] = {__ldg(cached + 3 * nq + q), __ldg(cached + 4 * nq + q),
+                              __ldg(cached + 5 * nq + q)};
+        const double wq = __ldg(cached + 6 * nq + q);
+        double kr, ki;
+        kernel_val<CPLX>(a, tab, y, nr, x, kr, ki);
+        kv[2 * lane] = kr * wq;
+        kv[2 * lane + 1] = ki * wq;
+      }
+      cp_async_wait_all();
+      __syncwarp();
+      accumulate<CPLX>(P, kv, nv, np, np, acc, lane);
+      __syncwarp();
+    }
+    for (int l = lane; l < np; l += 32) {
+      dst[2 * l] = acc[2 * l];
+      dst[2 * l + 1] = acc[2 * l + 1];
+    }
+    return;
+  }
   const double* rule = a.arena + a.rule_off[T->rule];
   const double ax = v6[2] - v6[0], ay = v6[3] - v6[1];
   const double bx = v6[4] - v6[0], by = v6[5] - v6[1];
   const double area2 = fabs(ax * by - ay * bx);
-  for (int l = lane; l < np; l += 32) acc[2 * l] = acc[2 * l + 1] = 0.0;
   for (int q0 = 0; q0 < nq; q0 += 32) {
     const int q = q0 + lane;
     if (q < nq) {
       const double xi = rule[q], eta = rule[nq + q], w = rule[2 * nq + q];
       double kr, ki;
-      const double jn = node_val<CPLX>(a, T, c, v6[0] + xi * ax + eta * bx,
+      const double jn = node_val<CPLX>(a, tab, T, c, v6[0] + xi * ax + eta * bx,
                                        v6[1] + xi * ay + eta * by, P + lane * stride, x, kr, ki);
       const double s = jn * w * area2;
       kv[2 * lane] = kr * s;
@@ -236,23 +345,28 @@ __device__ void tri_integral(const NqArgs& a, const NqType* T, const double* c, 
 // pop a triangle, integrate its four children, accept their sum when it
 // agrees with the parent to tol (max over l) or at level 18, else push them.
 template <bool CPLX>
-__device__ void near_integral(const NqArgs& a, const NqType* T, const double* c, const double* x,
-                              double tol, double* P, double* kv, double* acc, double* out,
-                              double* vec, double* stk, int lane, unsigned long long& nev,
-                              int& capped) {
+__device__ void near_integral(const NqArgs& a, const double2* tab, const NqType* T, const double* c,
+                              const double* pcache, const double* x, double tol, double* P,
+                              double* kv, double* acc, double* out, double* vec, double* stk,
+                              int lane, unsigned long long& nev, int& capped) {
   const int np = T->np, vs = 2 * a.np_max;
   const int nq = a.rule_nq[T->rule];
+  const int H = a.cache_h;
+  const size_t tri_doubles = size_t(7 + np) * nq;
+  auto block = [&](int ci) { return ci >= 0 ? pcache + size_t(ci) * tri_doubles : nullptr; };
   for (int l = lane; l < np; l += 32) out[2 * l] = out[2 * l + 1] = 0.0;
   const double* V = T->vert;
   const int nroots = T->nv == 3 ? 1 : 2;
   int sp = 0;
   for (int r = 0; r < nroots; ++r) {
     const double v6[6] = {V[0], V[1], V[2 + 2 * r], V[3 + 2 * r], V[4 + 2 * r], V[5 + 2 * r]};
+    const int ci = pcache ? r * H : -1;
     if (lane == 0) {
       for (int i = 0; i < 6; ++i) stk[kNqStackDoubles * sp + i] = v6[i];
       stk[kNqStackDoubles * sp + 6] = 0.0;
+      stk[kNqStackDoubles * sp + 7] = double(ci);
     }
-    tri_integral<CPLX>(a, T, c, v6, x, P, kv, acc, vec + size_t(sp) * vs, lane);
+    tri_integral<CPLX>(a, tab, T, c, v6, block(ci), x, P, kv, acc, vec + size_t(sp) * vs, lane);
     nev += nq;
     ++sp;
   }
@@ -267,15 +381,17 @@ __device__ void near_integral(const NqArgs& a, const NqType* T, const double* c,
     const double* e = stk + kNqStackDoubles * top;
     const double v[6] = {e[0], e[1], e[2], e[3], e[4], e[5]};
     const int lev = int(e[6]);
-    const double m01[2] = {0.5 * (v[0] + v[2]), 0.5 * (v[1] + v[3])};
-    const double m12[2] = {0.5 * (v[2] + v[4]), 0.5 * (v[3] + v[5])};
-    const double m20[2] = {0.5 * (v[4] + v[0]), 0.5 * (v[5] + v[1])};
-    const double ch[4][6] = {{v[0], v[1], m01[0], m01[1], m20[0], m20[1]},
-                             {m01[0], m01[1], v[2], v[3], m12[0], m12[1]},
-                             {m20[0], m20[1], m12[0], m12[1], v[4], v[5]},
-                             {m01[0], m01[1], m12[0], m12[1], m20[0], m20[1]}};
-    for (int q = 0; q < 4; ++q)
-      tri_integral<CPLX>(a, T, c, ch[q], x, P, kv, acc, vec + size_t(sp + q) * vs, lane);
+    const int ci = int(e[7]);
+    // children of a cached triangle above the last cached level are cached:
+    // heap index h -> 4h + 1 + q within the same root
+    const int cc = (ci >= 0 && lev < a.cache_levels) ? (ci / H) * H + 4 * (ci % H) + 1 : -1;
+
+    for (int q = 0; q < 4; ++q) {
+      double cv[6];
+      child_tri(v, q, cv);
+      tri_integral<CPLX>(a, tab, T, c, cv, block(cc >= 0 ? cc + q : -1), x, P, kv, acc,
+                         vec + size_t(sp + q) * vs, lane);
+    }
     nev += 4 * nq;
     double err = 0.0;
     const double* par = vec + size_t(top) * vs;
@@ -306,8 +422,11 @@ __device__ void near_integral(const NqArgs& a, const NqType* T, const double* c,
         }
       if (lane == 0)
         for (int q = 0; q < 4; ++q) {
-          for (int i = 0; i < 6; ++i) stk[kNqStackDoubles * (top + q) + i] = ch[q][i];
+          double cv[6];
+          child_tri(v, q, cv);
+          for (int i = 0; i < 6; ++i) stk[kNqStackDoubles * (top + q) + i] = cv[i];
           stk[kNqStackDoubles * (top + q) + 6] = double(lev + 1);
+          stk[kNqStackDoubles * (top + q) + 7] = double(cc >= 0 ? cc + q : -1);
         }
       sp = top + 4;
     }
@@ -320,12 +439,13 @@ __device__ void near_integral(const NqArgs& a, const NqType* T, const double* c,
 // on the edges into triangles, each with a Duffy map in s and a sinh map in
 // the angle-like variable anchored at the closest edge point.
 template <bool CPLX>
-__device__ void self_integral(const NqArgs& a, const NqType* T, const double* c, double u0,
+__device__ void self_integral(const NqArgs& a, const double2* tab, const NqType* T, const double* c,
+                              double u0,
                               double v0, double* P, double* kv, double* acc, double* sub,
                               int lane, unsigned long long& nev) {
   const int np = T->np, nself = a.nself;
   double g[9];
-  basis_geom<false>(T->iptype, T->norder, u0, v0, c, nullptr, g);
+  basis_geom<false, true>(T->iptype, T->norder, u0, v0, c, nullptr, g);
   const double x0[3] = {g[0], g[1], g[2]};
   const double g11 = g[3] * g[3] + g[4] * g[4] + g[5] * g[5];
   const double g12 = g[3] * g[6] + g[4] * g[7] + g[5] * g[8];
@@ -388,8 +508,8 @@ __device__ void self_integral(const NqArgs& a, const NqType* T, const double* c,
       const double s = 0.5 * (xs[is] + 1.0);
       const double jac = s * o[4] * dtw * 0.5 * ws[is];
       double kr, ki;
-      const double jn =
-          node_val<CPLX>(a, T, c, u0 + s * ex, v0 + s * ey, P + lane * a.stride, x0, kr, ki);
+      const double jn = node_val<CPLX>(a, tab, T, c, u0 + s * ex, v0 + s * ey,
+                                       P + lane * a.stride, x0, kr, ki);
       kv[2 * lane] = kr * jn * jac;
       kv[2 * lane + 1] = ki * jn * jac;
     }
@@ -423,15 +543,66 @@ __global__ void __launch_bounds__(256) nq_tol_kernel(NqArgs a) {
   if (lane == 0) a.ptol[p] = 0.1 * a.eps * sqrt(jw);
 }
 
+// Cache blocks of the patches [p0, p0 + n): one block per (patch, root,
+// heap index h < cache_h), threads over the rule nodes.  Heap order: the
+// children of h are 4h+1..4h+4 in child_tri order.
+__global__ void __launch_bounds__(128) nq_cache_kernel(NqArgs a, int64_t p0) {
+  const int H = a.cache_h;
+  const int64_t p = p0 + int64_t(blockIdx.x) / (2 * H);
+  const int rem = int(int64_t(blockIdx.x) % (2 * H));
+  const int r = rem / H, h = rem % H;
+  const NqType* T = a.types + a.ptype[p];
+  if (r >= (T->nv == 3 ? 1 : 2)) return;
+  const double* V = T->vert;
+  double v[6] = {V[0], V[1], V[2 + 2 * r], V[3 + 2 * r], V[4 + 2 * r], V[5 + 2 * r]};
+  int digit[8], nd = 0;
+  for (int k = h; k > 0 && nd < 8; k = (k - 1) / 4) digit[nd++] = (k - 1) % 4;
+  for (int i = nd - 1; i >= 0; --i) {
+    double o[6];
+    child_tri(v, digit[i], o);
+    for (int j = 0; j < 6; ++j) v[j] = o[j];
+  }
+  const int np = T->np, nq = a.rule_nq[T->rule];
+  const double* rule = a.arena + a.rule_off[T->rule];
+  const double* c = a.coefs + 9 * a.pstart[p];
+  double* blk = a.cache + a.coff[p] + size_t(r * H + h) * size_t(7 + np) * nq;
+  const double ax = v[2] - v[0], ay = v[3] - v[1];
+  const double bx = v[4] - v[0], by = v[5] - v[1];
+  const double area2 = fabs(ax * by - ay * bx);
+  for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+    const double xi = rule[q], eta = rule[nq + q], w = rule[2 * nq + q];
+    double g[9];
+    basis_geom<true>(T->iptype, T->norder, v[0] + xi * ax + eta * bx, v[1] + xi * ay + eta * by,
+                     c, blk + 7 * nq + size_t(q) * np, g);
+    const double n0 = g[4] * g[8] - g[5] * g[7];
+    const double n1 = g[5] * g[6] - g[3] * g[8];
+    const double n2 = g[3] * g[7] - g[4] * g[6];
+    const double j2 = n0 * n0 + n1 * n1 + n2 * n2;
+    const double inv = rsqrt(j2);  // as node_val, so cached and evaluated nodes agree
+    const double jn = j2 * inv;
+    blk[q] = g[0];
+    blk[nq + q] = g[1];
+    blk[2 * nq + q] = g[2];
+    blk[3 * nq + q] = n0 * inv;
+    blk[4 * nq + q] = n1 * inv;
+    blk[5 * nq + q] = n2 * inv;
+    blk[6 * nq + q] = jn * w * area2;
+  }
+}
+
 template <bool CPLX>
 __global__ void __launch_bounds__(256) nq_pair_kernel(NqArgs a) {
-  extern __shared__ double nq_smem[];
+  extern __shared__ __align__(16) double nq_smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  double* P = nq_smem + size_t(wib) * a.warp_doubles;
+  double2* tab = reinterpret_cast<double2*>(nq_smem);  // (cos, sin)(2 pi j / 256)
+  if (CPLX) dev::fill_trig_table(tab);
+  __syncthreads();
+  double* P = nq_smem + 2 * dev::kTrigN + size_t(wib) * a.warp_doubles;
   double* kv = P + 32 * a.stride;
   double* acc = kv + 64;
   double* out = acc + 2 * a.np_max;
   double* sub = out + 2 * a.np_max;
+  double* csh = sub + kNqSubDoubles;  // the patch's coefficients, 10 per basis function
   const int64_t gw = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   double* vec = a.scratch + gw * a.scratch_per_warp;
   double* stk = vec + size_t(kNqSlots) * 2 * a.np_max;
@@ -439,22 +610,31 @@ __global__ void __launch_bounds__(256) nq_pair_kernel(NqArgs a) {
   int capped = 0;
   for (;;) {
     long long idx = 0;
-    if (lane == 0) idx = (long long)atomicAdd(a.counter, 1ull);
+    if (lane == 0) idx = a.item_lo + (long long)atomicAdd(a.next, 1ull);
     idx = __shfl_sync(kFull, idx, 0);
-    if (idx >= a.nitems) break;
+    if (idx >= a.item_hi) break;
     const longlong2 it = a.items[idx];
     const int64_t k = it.x, t = it.y;
     const int64_t p = a.col_ind[k] - 1;
     const NqType* T = a.types + a.ptype[p];
-    const double* c = a.coefs + 9 * a.pstart[p];
     const int np = T->np;
+    {
+      const double* cg = a.coefs + 9 * a.pstart[p];
+      for (int i = lane; i < 9 * np; i += 32) csh[10 * (i / 9) + i % 9] = __ldg(cg + i);
+      for (int i = lane; i < np; i += 32) csh[10 * i + 9] = 0.0;
+    }
+    __syncwarp();
+    const double* c = csh;
     double* res;
     if (idx < a.nself_items) {
-      self_integral<CPLX>(a, T, c, a.uvt[2 * t], a.uvt[2 * t + 1], P, kv, acc, sub, lane, nev);
+      self_integral<CPLX>(a, tab, T, c, a.uvt[2 * t], a.uvt[2 * t + 1], P, kv, acc, sub, lane,
+                          nev);
       res = acc;
     } else {
-      near_integral<CPLX>(a, T, c, a.targ + 3 * t, a.ptol[p], P, kv, acc, out, vec, stk, lane,
-                          nev, capped);
+      const double* pcache =
+          (a.cache_levels >= 0 && a.coff[p] >= 0) ? a.cache + a.coff[p] : nullptr;
+      near_integral<CPLX>(a, tab, T, c, pcache, a.targ + 3 * t, a.ptol[p], P, kv, acc, out, vec,
+                          stk, lane, nev, capped);
       res = out;
     }
     __syncwarp();
@@ -478,8 +658,8 @@ __global__ void __launch_bounds__(256) nq_pair_kernel(NqArgs a) {
     __syncwarp();
   }
   if (lane == 0) {
-    atomicAdd(a.counter + 1, nev);
-    if (capped) atomicAdd(a.counter + 2, 1ull);
+    atomicAdd(a.stat, nev);
+    if (capped) atomicAdd(a.stat + 1, 1ull);
   }
 }
 
@@ -640,8 +820,17 @@ int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
       (self ? items : near_items).push_back(make_longlong2(k, t));
     }
   }
+  // near pairs grouped by patch (targets in order within a patch), so the
+  // warps running at one time share a few patches' cache blocks
   const int64_t nself_items = int64_t(items.size());
-  items.insert(items.end(), near_items.begin(), near_items.end());
+  std::vector<int64_t> pfirst(s.npatches + 1, 0);
+  for (const auto& it : near_items) ++pfirst[col_ind[it.x]];
+  for (int64_t p = 0; p < s.npatches; ++p) pfirst[p + 1] += pfirst[p];
+  items.resize(size_t(nself_items) + near_items.size());
+  {
+    std::vector<int64_t> fill(pfirst.begin(), pfirst.end() - 1);
+    for (const auto& it : near_items) items[size_t(nself_items + fill[col_ind[it.x] - 1]++)] = it;
+  }
   near_items.clear();
   near_items.shrink_to_fit();
   std::vector<double> targ3(3 * size_t(nt)), uvt(uvs_targ ? 2 * size_t(nt) : 0);
@@ -653,26 +842,79 @@ int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int stride = np_max | 1;
-  const int warp_doubles = 32 * stride + 64 + 4 * np_max + kNqSubDoubles;
+  const int warp_doubles = 32 * stride + 64 + 4 * np_max + kNqSubDoubles + 10 * np_max;
   const size_t warp_bytes = sizeof(double) * size_t(warp_doubles);
-  const int wpb = int(std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / warp_bytes)));
-  const size_t smem = warp_bytes * wpb;
+  const size_t tab_bytes = sizeof(double) * 2 * dev::kTrigN;
   auto kern = kind == 1 ? nq_pair_kernel<true> : nq_pair_kernel<false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  int bps = 0;
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 32 * wpb, smem);
+  // warps per block: the most resident warps per SM, larger blocks on ties
+  int wpb = 0, bps = 0;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(std::min<size_t>(tab_bytes + 8 * warp_bytes, 227u << 10)));
+  for (int w = 8; w >= 1 && e == cudaSuccess; --w) {
+    if (tab_bytes + w * warp_bytes > (227u << 10)) continue;
+    int b = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 32 * w, tab_bytes + w * warp_bytes);
+    if (e == cudaSuccess && b * w > bps * wpb) {
+      wpb = w;
+      bps = b;
+    }
+  }
+  const size_t smem = tab_bytes + warp_bytes * std::max(wpb, 1);
   if (e != cudaSuccess || bps < 1) {
     set_last_error(std::string("getnearquad_gpu: launch configuration: ") + cudaGetErrorString(e));
     return kErrCuda;
+  }
+  // cache: uniform levels 0..L of every root triangle (L from
+  // BIE_NEARQUAD_CACHE_LEVELS, default 3, at most 5, -1 = none), built for
+  // groups of consecutive patches whose blocks fit in the group budget
+  // (min(4 GiB, free memory / 4), or BIE_NEARQUAD_CACHE_BUDGET_MB)
+  int levels = 3;
+  if (const char* ev = std::getenv("BIE_NEARQUAD_CACHE_LEVELS")) levels = std::atoi(ev);
+  levels = std::max(-1, std::min(5, levels));
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  size_t budget = std::min<size_t>(size_t(4) << 30, free_b / 4);
+  if (const char* ev = std::getenv("BIE_NEARQUAD_CACHE_BUDGET_MB"))
+    budget = size_t(std::max(1, std::atoi(ev))) << 20;
+  const int H = levels >= 0 ? ((1 << (2 * (levels + 1))) - 1) / 3 : 0;
+  std::vector<int64_t> coff(s.npatches, -1);
+  std::vector<std::pair<int64_t, int64_t>> groups;  // patch ranges
+  size_t cache_doubles = 0;
+  if (levels >= 0) {
+    size_t used = 0;
+    int64_t g0 = 0;
+    for (int64_t p = 0; p < s.npatches; ++p) {
+      const NqType& T = types[ptype[p]];
+      const size_t need = size_t(T.nv == 3 ? 1 : 2) * H * size_t(7 + T.np) * a.rule_nq[T.rule];
+      if (need * sizeof(double) > budget) {
+        levels = -1;
+        break;
+      }
+      if ((used + need) * sizeof(double) > budget) {
+        groups.emplace_back(g0, p);
+        g0 = p;
+        used = 0;
+      }
+      coff[p] = int64_t(used);
+      used += need;
+      cache_doubles = std::max(cache_doubles, used);
+    }
+    if (levels >= 0) groups.emplace_back(g0, s.npatches);
+  }
+  if (levels < 0) {
+    groups.assign(1, {0, s.npatches});
+    std::fill(coff.begin(), coff.end(), -1);
+    cache_doubles = 0;
   }
   const int64_t want = (int64_t(items.size()) + wpb - 1) / wpb;
   const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(nsm) * bps, want)));
   const int64_t nwarps = int64_t(blocks) * wpb;
 
-  DBuf<double> d_coefs, d_arena, d_targ, d_uvt, d_tol, d_scratch;
+  DBuf<double> d_coefs, d_arena, d_targ, d_uvt, d_tol, d_scratch, d_cache;
   DBuf<NqType> d_types;
   DBuf<int> d_ptype;
-  DBuf<int64_t> d_pstart, d_col, d_iq;
+  DBuf<int64_t> d_pstart, d_col, d_iq, d_coff;
+  const int nlaunch = 1 + int(groups.size());
   DBuf<longlong2> d_items;
   DBuf<unsigned long long> d_cnt;
   const size_t per_warp = size_t(kNqSlots) * 2 * np_max + size_t(kNqSlots) * kNqStackDoubles;
@@ -688,8 +930,11 @@ int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
       (e = upload(d_col, col_ind, size_t(nnz), st)) != cudaSuccess ||
       (e = upload(d_iq, iquad, size_t(nnz) + 1, st)) != cudaSuccess ||
       (e = upload(d_items, items.data(), items.size(), st)) != cudaSuccess ||
-      (e = d_cnt.alloc(3)) != cudaSuccess ||
-      (e = cudaMemsetAsync(d_cnt.p, 0, 3 * sizeof(unsigned long long), st)) != cudaSuccess) {
+      (e = upload(d_coff, coff.data(), coff.size(), st)) != cudaSuccess ||
+      (e = d_cache.alloc(std::max<size_t>(cache_doubles, 1))) != cudaSuccess ||
+      (e = d_cnt.alloc(nlaunch + 2)) != cudaSuccess ||
+      (e = cudaMemsetAsync(d_cnt.p, 0, (nlaunch + 2) * sizeof(unsigned long long), st)) !=
+          cudaSuccess) {
     set_last_error(std::string("getnearquad_gpu: device buffers: ") + cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? kErrNoMem : kErrCuda;
   }
@@ -710,8 +955,11 @@ int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
   a.targ = d_targ.p;
   a.uvt = d_uvt.p;
   a.items = d_items.p;
-  a.nitems = int64_t(items.size());
   a.nself_items = nself_items;
+  a.cache = d_cache.p;
+  a.coff = d_coff.p;
+  a.cache_levels = levels;
+  a.cache_h = H;
   a.npatches = s.npatches;
   a.col_ind = d_col.p;
   a.iquad = d_iq.p;
@@ -721,17 +969,38 @@ int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
   a.np_max = np_max;
   a.stride = stride;
   a.warp_doubles = warp_doubles;
-  a.counter = d_cnt.p;
+  a.stat = d_cnt.p + nlaunch;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   cudaEventCreate(&ev[0]);
   cudaEventCreate(&ev[1]);
   nq_tol_kernel<<<unsigned((s.npatches * 32 + 255) / 256), 256, 0, st>>>(a);
   cudaEventRecord(ev[0], st);
-  kern<<<blocks, 32 * wpb, smem, st>>>(a);
+  int64_t launches = 1;
+  // self pairs (no cache), then each patch group: its cache, its near pairs
+  a.item_lo = 0;
+  a.item_hi = nself_items;
+  a.next = d_cnt.p;
+  if (nself_items > 0) {
+    kern<<<blocks, 32 * wpb, smem, st>>>(a);
+    ++launches;
+  }
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    const int64_t pa = groups[gi].first, pb = groups[gi].second;
+    a.item_lo = nself_items + pfirst[pa];
+    a.item_hi = nself_items + pfirst[pb];
+    a.next = d_cnt.p + 1 + gi;
+    if (a.item_hi == a.item_lo) continue;
+    if (levels >= 0) {
+      nq_cache_kernel<<<unsigned((pb - pa) * 2 * H), 128, 0, st>>>(a, pa);
+      ++launches;
+    }
+    kern<<<blocks, 32 * wpb, smem, st>>>(a);
+    ++launches;
+  }
   cudaEventRecord(ev[1], st);
-  dev::note_launches(2);
-  unsigned long long cnt[3] = {0, 0, 0};
-  cudaMemcpyAsync(cnt, d_cnt.p, sizeof cnt, cudaMemcpyDeviceToHost, st);
+  dev::note_launches(launches);
+  unsigned long long cnt[2] = {0, 0};
+  cudaMemcpyAsync(cnt, d_cnt.p + nlaunch, sizeof cnt, cudaMemcpyDeviceToHost, st);
   e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = cudaGetLastError();
   float ms = 0.f;
@@ -744,12 +1013,12 @@ int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
   }
   if (stats) {
     stats->device_ms = ms;
-    stats->kernel_evals = int64_t(cnt[1]);
+    stats->kernel_evals = int64_t(cnt[0]);
     stats->self_targets = nself_items;
     stats->near_targets = int64_t(items.size()) - nself_items;
   }
-  if (cnt[2]) {
-    set_last_error("getnearquad_gpu: " + std::to_string(cnt[2]) +
+  if (cnt[1]) {
+    set_last_error("getnearquad_gpu: " + std::to_string(cnt[1]) +
                    " warps hit the refinement-step cap");
     return kErrTimeout;
   }

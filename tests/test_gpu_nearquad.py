@@ -108,3 +108,15 @@ def test_setup_engine_switch():
         assert lib.bie_set_nearquad_engine(5) != 0
     finally:
         lib.bie_set_nearquad_engine(old)
+
+
+@pytest.mark.parametrize("levels,budget_mb", [("-1", None), ("0", None), ("5", None), ("2", "3")])
+def test_refinement_cache_settings(monkeypatch, levels, budget_mb):
+    """Without the cache of uniform refinement levels, with one level, with
+    five, and with a budget small enough to split the patches into groups:
+    the same weights as the host generator."""
+    monkeypatch.setenv("BIE_NEARQUAD_CACHE_LEVELS", levels)
+    if budget_mb:
+        monkeypatch.setenv("BIE_NEARQUAD_CACHE_BUDGET_MB", budget_mb)
+    s = S.icosa_ellipsoid(1, 6, (1.0, 2.0, 3.0))
+    _compare(s, 1, 1e-7, (1.5, -1.5j, 1.0), _near_setup(s))
