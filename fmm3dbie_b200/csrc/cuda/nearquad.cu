@@ -42,6 +42,11 @@ constexpr int kNqLeg = 41;              // tensor bases up to order 40
 constexpr int kNqJac = kNqTriOrder + 1;
 constexpr int kNqSubDoubles = 8 * 8 + 8;  // 8 self sub-triangles x 8, then the count
 constexpr double kNqOver4Pi = 0.07957747154594767;
+// Basis values of a chunk of 32 rule nodes in shared memory: one row of
+// kNqPS doubles per basis function, node index fastest (the pad keeps
+// 16-byte row starts and makes the lanes' 16-byte reads of one column pair
+// fall in distinct banks).
+constexpr int kNqPS = 34;
 constexpr unsigned kFull = 0xffffffffu;
 
 // Recurrence constants of the bases (uniform across a warp, so constant
@@ -81,7 +86,8 @@ struct NqArgs {
   // Cache of the uniform refinement levels 0..cache_levels of every root
   // triangle of the patches in the current group: per triangle (root r,
   // heap index h) and rule node q, the geometry xyz, unit normal and
-  // |J| w_q area2 (7 x nq, node fastest) followed by the basis rows (nq x np).
+  // |J| w_q area2 (7 x nq, node fastest) followed by the basis values
+  // (np x nq, node fastest).
   double* cache;
   const int64_t* coff;  // per patch: offset of its block in `cache` (-1: not in this group)
   int cache_levels;     // -1: no cache
@@ -91,23 +97,23 @@ struct NqArgs {
   double* wout;
   double* scratch;
   int64_t scratch_per_warp;
-  int np_max, stride, warp_doubles;
+  int np_max, warp_doubles;
   unsigned long long* next;  // this launch's item counter
   unsigned long long* stat;  // [0] kernel evaluations, [1] capped pairs
 };
 
-// Basis values at (u, v) -> prow[0..np) (when STORE) and the geometry
+// Basis values at (u, v) -> prow[l * ps], l < np (when STORE) and the geometry
 // g = sum_l coefs_l P_l: xyz, d/du, d/dv.  Same bases as basis_pols.
 // Coefficients: 9 per basis function in global memory, or (SHARED) the
 // warp's copy in shared memory padded to 10 so that pairs load as one
 // 16-byte access.
 template <bool STORE, bool SHARED = false>
 __device__ void basis_geom(int iptype, int n, double u, double v, const double* __restrict__ c,
-                           double* prow, double* g) {
+                           double* prow, int ps, double* g) {
 #pragma unroll
   for (int k = 0; k < 9; ++k) g[k] = 0.0;
   auto emit = [&](int idx, double p) {
-    if (STORE) prow[idx] = p;
+    if (STORE) prow[idx * ps] = p;
     if (SHARED) {
       const double2* ci = reinterpret_cast<const double2*>(c + 10 * idx);
 #pragma unroll
@@ -195,13 +201,14 @@ __device__ __forceinline__ void kernel_val(const NqArgs& a, const double2* tab, 
   im = (tr * s + ti * c) * m;
 }
 
-// One rule node: basis row -> prow, kernel value -> (kr, ki); returns |J|.
+// One rule node: basis values -> prow[l * kNqPS], kernel value -> (kr, ki);
+// returns |J|.
 template <bool CPLX>
 __device__ double node_val(const NqArgs& a, const double2* tab, const NqType* T, const double* c,
                            double u, double v, double* prow, const double* x, double& kr,
                            double& ki) {
   double g[9];
-  basis_geom<true, true>(T->iptype, T->norder, u, v, c, prow, g);
+  basis_geom<true, true>(T->iptype, T->norder, u, v, c, prow, kNqPS, g);
   const double n0 = g[4] * g[8] - g[5] * g[7];
   const double n1 = g[5] * g[6] - g[3] * g[8];
   const double n2 = g[3] * g[7] - g[4] * g[6];
@@ -213,48 +220,65 @@ __device__ double node_val(const NqArgs& a, const double2* tab, const NqType* T,
 }
 
 // Lanes own basis indices l = lane, lane + 32, ...: acc_l += sum over the
-// chunk's nodes of kv_q P_q,l (P and kv in shared memory; two partial sums
-// per component to halve the dependent FMA chain).
+// chunk's nv nodes of kv_q P_l,q (P rows of kNqPS doubles and kv in shared
+// memory; node pairs read as one 16-byte load, two partial sums per
+// component to halve the dependent FMA chain).
 template <bool CPLX>
 __device__ __forceinline__ void accumulate(const double* P, const double* kv, int nv, int np,
-                                           int stride, double* acc, int lane) {
+                                           double* acc, int lane) {
   const double2* kv2 = reinterpret_cast<const double2*>(kv);
   for (int l = lane; l < np; l += 32) {
+    const double* row = P + l * kNqPS;
     double s0r = 0.0, s0i = 0.0, s1r = 0.0, s1i = 0.0;
-    int q = 0;
-    for (; q + 1 < nv; q += 2) {
-      const double p0 = P[q * stride + l], p1 = P[(q + 1) * stride + l];
+    auto step = [&](int q) {
+      const double2 p = *reinterpret_cast<const double2*>(row + q);
       const double2 k0 = kv2[q], k1 = kv2[q + 1];
-      s0r = fma(k0.x, p0, s0r);
-      s1r = fma(k1.x, p1, s1r);
+      s0r = fma(k0.x, p.x, s0r);
+      s1r = fma(k1.x, p.y, s1r);
       if (CPLX) {
-        s0i = fma(k0.y, p0, s0i);
-        s1i = fma(k1.y, p1, s1i);
+        s0i = fma(k0.y, p.x, s0i);
+        s1i = fma(k1.y, p.y, s1i);
       }
-    }
-    if (q < nv) {
-      const double p0 = P[q * stride + l];
-      const double2 k0 = kv2[q];
-      s0r = fma(k0.x, p0, s0r);
-      if (CPLX) s0i = fma(k0.y, p0, s0i);
+    };
+    if (nv == 32) {
+#pragma unroll
+      for (int q = 0; q < 32; q += 2) step(q);
+    } else {
+      int q = 0;
+      for (; q + 1 < nv; q += 2) step(q);
+      if (q < nv) {
+        const double2 k0 = kv2[q];
+        s0r = fma(k0.x, row[q], s0r);
+        if (CPLX) s0i = fma(k0.y, row[q], s0i);
+      }
     }
     acc[2 * l] += s0r + s1r;
     acc[2 * l + 1] += s0i + s1i;
   }
 }
 
-// Asynchronous global -> shared copy of n doubles (both addresses 16-byte
-// aligned): 16-byte cp.async pieces strided over the lanes, an odd last
-// double by lane 0.  Completed by cp_async_wait_all() and a __syncwarp().
-__device__ __forceinline__ void copy_async(double* dst, const double* src, int n, int lane) {
-  const int n16 = n >> 1;
-  for (int i = lane; i < n16; i += 32) {
-    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(dst + 2 * i));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src + 2 * i)
+// Asynchronous copy of the chunk's basis values: rows l < np of nv doubles
+// from src + l * nq (16-byte aligned: nq and the chunk start are even) to
+// P + l * kNqPS, as 16-byte cp.async pieces strided over the lanes (an odd
+// last column by plain loads).  Completed by cp_async_wait_all() and a
+// __syncwarp().
+__device__ __forceinline__ void copy_chunk_async(double* P, const double* src, int nq, int nv,
+                                                 int np, int lane) {
+  auto piece = [&](int l, int j) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(P + l * kNqPS + 2 * j));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa),
+                 "l"(src + size_t(l) * nq + 2 * j)
                  : "memory");
+  };
+  if (nv == 32) {
+    for (int l = lane >> 4; l < np; l += 2) piece(l, lane & 15);
+  } else {
+    const int hv = nv >> 1;
+    for (int i = lane; i < np * hv; i += 32) piece(i / hv, i % hv);
+    if (nv & 1)
+      for (int l = lane; l < np; l += 32) P[l * kNqPS + nv - 1] = __ldg(src + size_t(l) * nq + nv - 1);
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
-  if ((n & 1) && lane == 0) dst[n - 1] = __ldg(src + n - 1);
 }
 
 __device__ __forceinline__ void cp_async_wait_all() {
@@ -285,7 +309,7 @@ template <bool CPLX>
 __device__ void tri_integral(const NqArgs& a, const double2* tab, const NqType* T, const double* c,
                              const double* v6, const double* cached, const double* x, double* P,
                              double* kv, double* acc, double* dst, int lane) {
-  const int np = T->np, stride = a.stride;
+  const int np = T->np;
   const int nq = a.rule_nq[T->rule];
   for (int l = lane; l < np; l += 32) acc[2 * l] = acc[2 * l + 1] = 0.0;
   if (cached) {
@@ -294,7 +318,7 @@ __device__ void tri_integral(const NqArgs& a, const double2* tab, const NqType* 
       const int nv = min(32, nq - q0);
       // basis rows of the chunk into the P buffer while the kernel values
       // are computed
-      copy_async(P, cached + 7 * nq + size_t(q0) * np, nv * np, lane);
+      copy_chunk_async(P, cached + 7 * nq + q0, nq, nv, np, lane);
       if (q < nq) {
         const double y[3] = {__ldg(cached + q), __ldg(cached + nq + q), __ldg(cached + 2 * nq + q)};
         const double nr[3] = {__ldg(cached + 3 * nq + q), __ldg(cached + 4 * nq + q),
@@ -307,7 +331,7 @@ __device__ void tri_integral(const NqArgs& a, const double2* tab, const NqType* 
       }
       cp_async_wait_all();
       __syncwarp();
-      accumulate<CPLX>(P, kv, nv, np, np, acc, lane);
+      accumulate<CPLX>(P, kv, nv, np, acc, lane);
       __syncwarp();
     }
     for (int l = lane; l < np; l += 32) {
@@ -326,13 +350,13 @@ __device__ void tri_integral(const NqArgs& a, const double2* tab, const NqType* 
       const double xi = rule[q], eta = rule[nq + q], w = rule[2 * nq + q];
       double kr, ki;
       const double jn = node_val<CPLX>(a, tab, T, c, v6[0] + xi * ax + eta * bx,
-                                       v6[1] + xi * ay + eta * by, P + lane * stride, x, kr, ki);
+                                       v6[1] + xi * ay + eta * by, P + lane, x, kr, ki);
       const double s = jn * w * area2;
       kv[2 * lane] = kr * s;
       kv[2 * lane + 1] = ki * s;
     }
     __syncwarp();
-    accumulate<CPLX>(P, kv, min(32, nq - q0), np, stride, acc, lane);
+    accumulate<CPLX>(P, kv, min(32, nq - q0), np, acc, lane);
     __syncwarp();
   }
   for (int l = lane; l < np; l += 32) {
@@ -445,7 +469,7 @@ __device__ void self_integral(const NqArgs& a, const double2* tab, const NqType*
                               int lane, unsigned long long& nev) {
   const int np = T->np, nself = a.nself;
   double g[9];
-  basis_geom<false, true>(T->iptype, T->norder, u0, v0, c, nullptr, g);
+  basis_geom<false, true>(T->iptype, T->norder, u0, v0, c, nullptr, 0, g);
   const double x0[3] = {g[0], g[1], g[2]};
   const double g11 = g[3] * g[3] + g[4] * g[4] + g[5] * g[5];
   const double g12 = g[3] * g[6] + g[4] * g[7] + g[5] * g[8];
@@ -509,12 +533,12 @@ __device__ void self_integral(const NqArgs& a, const double2* tab, const NqType*
       const double jac = s * o[4] * dtw * 0.5 * ws[is];
       double kr, ki;
       const double jn = node_val<CPLX>(a, tab, T, c, u0 + s * ex, v0 + s * ey,
-                                       P + lane * a.stride, x0, kr, ki);
+                                       P + lane, x0, kr, ki);
       kv[2 * lane] = kr * jn * jac;
       kv[2 * lane + 1] = ki * jn * jac;
     }
     __syncwarp();
-    accumulate<CPLX>(P, kv, min(32, total - q0), np, a.stride, acc, lane);
+    accumulate<CPLX>(P, kv, min(32, total - q0), np, acc, lane);
     __syncwarp();
   }
   nev += total;
@@ -532,7 +556,7 @@ __global__ void __launch_bounds__(256) nq_tol_kernel(NqArgs a) {
   for (int j = lane; j < T->np; j += 32) {
     double g[9];
     basis_geom<false>(T->iptype, T->norder, a.arena[T->uvs + 2 * j], a.arena[T->uvs + 2 * j + 1],
-                      c, nullptr, g);
+                      c, nullptr, 0, g);
     const double n0 = g[4] * g[8] - g[5] * g[7];
     const double n1 = g[5] * g[6] - g[3] * g[8];
     const double n2 = g[3] * g[7] - g[4] * g[6];
@@ -573,7 +597,7 @@ __global__ void __launch_bounds__(128) nq_cache_kernel(NqArgs a, int64_t p0) {
     const double xi = rule[q], eta = rule[nq + q], w = rule[2 * nq + q];
     double g[9];
     basis_geom<true>(T->iptype, T->norder, v[0] + xi * ax + eta * bx, v[1] + xi * ay + eta * by,
-                     c, blk + 7 * nq + size_t(q) * np, g);
+                     c, blk + 7 * nq + q, nq, g);
     const double n0 = g[4] * g[8] - g[5] * g[7];
     const double n1 = g[5] * g[6] - g[3] * g[8];
     const double n2 = g[3] * g[7] - g[4] * g[6];
@@ -598,7 +622,7 @@ __global__ void __launch_bounds__(256) nq_pair_kernel(NqArgs a) {
   if (CPLX) dev::fill_trig_table(tab);
   __syncthreads();
   double* P = nq_smem + 2 * dev::kTrigN + size_t(wib) * a.warp_doubles;
-  double* kv = P + 32 * a.stride;
+  double* kv = P + kNqPS * a.np_max;
   double* acc = kv + 64;
   double* out = acc + 2 * a.np_max;
   double* sub = out + 2 * a.np_max;
@@ -841,8 +865,7 @@ int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int stride = np_max | 1;
-  const int warp_doubles = 32 * stride + 64 + 4 * np_max + kNqSubDoubles + 10 * np_max;
+  const int warp_doubles = kNqPS * np_max + 64 + 4 * np_max + kNqSubDoubles + 10 * np_max;
   const size_t warp_bytes = sizeof(double) * size_t(warp_doubles);
   const size_t tab_bytes = sizeof(double) * 2 * dev::kTrigN;
   auto kern = kind == 1 ? nq_pair_kernel<true> : nq_pair_kernel<false>;
@@ -967,7 +990,6 @@ int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
   a.scratch = d_scratch.p;
   a.scratch_per_warp = int64_t(per_warp);
   a.np_max = np_max;
-  a.stride = stride;
   a.warp_doubles = warp_doubles;
   a.stat = d_cnt.p + nlaunch;
   cudaEvent_t ev[2] = {nullptr, nullptr};
