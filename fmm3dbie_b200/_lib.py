@@ -46,6 +46,11 @@ _SIGS = {
     "bie_get_qwts": (C.c_int, [I64, PI64, PI64, PI64, I64, PDBL, PDBL]),
     "bie_findnearmem": (C.c_int, [PDBL, I64, PDBL, I64, PDBL, I64, PI64]),
     "bie_findnear": (C.c_int, [PDBL, I64, PDBL, I64, PDBL, I64, PI64, PI64]),
+    "bie_findnear_gpu": (C.c_int, [PDBL, I64, PDBL, I64, PDBL, I64, PI64, PI64, I64]),
+    "bie_get_far_order_gpu": (C.c_int, [DBL, I64, PI64, PI64, PI64, PDBL, PDBL, I64, PDBL, I64,
+                                        I64, PDBL, I64, PDBL, I64, PI64, PI64, DBL, PI64, PI64]),
+    "bie_oversample_geom_gpu": (C.c_int, [I64, PI64, PI64, PI64, I64, PDBL, PDBL, PI64, PI64, I64,
+                                          PDBL]),
     "bie_get_iquad_rsc": (C.c_int, [I64, PI64, I64, I64, PI64, PI64, PI64]),
     "bie_get_far_order": (C.c_int, [DBL, I64, PI64, PI64, PI64, PDBL, PDBL, I64, PDBL, I64, I64,
                                     PDBL, I64, PDBL, I64, PI64, PI64, DBL, PI64, PI64]),

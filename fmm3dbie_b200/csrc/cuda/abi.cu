@@ -20,6 +20,7 @@
 #include "../host/nearquad.h"
 #include "../host/setup.h"
 #include "nearquad_gpu.h"
+#include "setup_gpu.h"
 #include "plan.h"
 
 using bie::cdouble;
@@ -105,9 +106,9 @@ struct Setup {
   double rfac = 0, rfac0 = 0;
 };
 
-// Near quadrature engine of the setup: 1 = device generator (default),
-// 0 = host generator.  Surfaces with patches above the device generator's
-// basis limit use the host generator.
+// Setup engine: 1 = device (near lists, far orders, oversampled geometry,
+// near quadrature; the default), 0 = host.  Surfaces with patches above the
+// device generators' basis limit use the host.
 std::atomic<int> g_nearquad_engine{1};
 
 int64_t max_npols(const bie::Surf& s) {
@@ -132,8 +133,22 @@ int run_setup(const bie::Surf& s, int kind, cdouble zk, cdouble alpha, cdouble b
   bie::centroid_rads(s, o.cms.data(), o.rads.data());
   std::vector<double> rad_near(s.npatches);
   for (int64_t p = 0; p < s.npatches; ++p) rad_near[p] = o.rads[p] * o.rfac;
-  bie::findnear(s.npatches, o.cms.data(), rad_near.data(), ndtarg, ntarg, targs, o.row_ptr,
-                o.col_ind);
+  const bool on_device = g_nearquad_engine.load() == 1 && max_npols(s) <= bie::kNearQuadMaxNp;
+  std::unique_ptr<Stage> stg;
+  std::unique_ptr<bie::AllocStreamScope> alloc_scope;
+  if (on_device) {
+    stg = std::make_unique<Stage>();
+    alloc_scope = std::make_unique<bie::AllocStreamScope>(stg->st);
+  }
+  int ier = 0;
+  if (on_device) {
+    ier = bie::findnear_gpu(s.npatches, o.cms.data(), rad_near.data(), ndtarg, ntarg, targs,
+                            o.row_ptr, o.col_ind, stg->st);
+    if (ier) return ier;
+  } else {
+    bie::findnear(s.npatches, o.cms.data(), rad_near.data(), ndtarg, ntarg, targs, o.row_ptr,
+                  o.col_ind);
+  }
   o.nnz = int64_t(o.col_ind.size());
   o.iquad.resize(o.nnz + 1);
   bie::iquad_rsc(s, ntarg, o.nnz, o.row_ptr.data(), o.col_ind.data(), o.iquad.data());
@@ -141,9 +156,14 @@ int run_setup(const bie::Surf& s, int kind, cdouble zk, cdouble alpha, cdouble b
   const int ikerorder = std::abs(beta) > 1e-16 ? 0 : -1;
   o.novers.resize(s.npatches);
   o.ixyzso.resize(s.npatches + 1);
-  int ier = bie::far_order(eps, s, o.cms.data(), o.rads.data(), ndtarg, ntarg, targs, ikerorder,
-                           kind == 1 ? zk : cdouble(0), o.nnz, o.row_ptr.data(), o.col_ind.data(),
-                           o.rfac, o.novers.data(), o.ixyzso.data());
+  ier = on_device
+            ? bie::far_order_gpu(eps, s, o.cms.data(), o.rads.data(), ndtarg, ntarg, targs,
+                                 ikerorder, kind == 1 ? zk : cdouble(0), o.nnz, o.row_ptr.data(),
+                                 o.col_ind.data(), o.rfac, o.novers.data(), o.ixyzso.data(),
+                                 stg->st)
+            : bie::far_order(eps, s, o.cms.data(), o.rads.data(), ndtarg, ntarg, targs,
+                             ikerorder, kind == 1 ? zk : cdouble(0), o.nnz, o.row_ptr.data(),
+                             o.col_ind.data(), o.rfac, o.novers.data(), o.ixyzso.data());
   if (ier) {
     bie::set_last_error("get_far_order failed");
     return BIE_ERR_ARG;
@@ -151,15 +171,19 @@ int run_setup(const bie::Surf& s, int kind, cdouble zk, cdouble alpha, cdouble b
   o.nptso = o.ixyzso[s.npatches] - 1;
   o.srcover.resize(12 * o.nptso);
   o.wover.resize(o.nptso);
-  bie::oversample_geom(s, o.novers.data(), o.ixyzso.data(), o.nptso, o.srcover.data());
+  if (on_device) {
+    ier = bie::oversample_geom_gpu(s, o.novers.data(), o.ixyzso.data(), o.nptso,
+                                   o.srcover.data(), stg->st);
+    if (ier) return ier;
+  } else {
+    bie::oversample_geom(s, o.novers.data(), o.ixyzso.data(), o.nptso, o.srcover.data());
+  }
   bie::Surf so = make_surf(s.npatches, o.novers.data(), o.ixyzso.data(), s.iptype, o.nptso,
                            nullptr, o.srcover.data());
   bie::qwts(so, o.wover.data());
   const size_t wl = size_t(o.nquad) * (kind == 1 ? 2 : 1);
   o.wnear.assign(wl, 0.0);
-  if (g_nearquad_engine.load() == 1 && o.nnz > 0 && max_npols(s) <= bie::kNearQuadMaxNp) {
-    Stage stg;
-    bie::AllocStreamScope alloc_scope(stg.st);
+  if (on_device && o.nnz > 0) {
     bie::DBuf<double> d_w;
     if (d_w.alloc(wl) != cudaSuccess) {
       bie::set_last_error("near quadrature: device allocation failed");
@@ -167,11 +191,11 @@ int run_setup(const bie::Surf& s, int kind, cdouble zk, cdouble alpha, cdouble b
     }
     ier = bie::getnearquad_gpu(s, ndtarg, ntarg, targs, ipatch_id, uvs_targ, eps, kind, zk, alpha,
                                beta, o.nnz, o.row_ptr.data(), o.col_ind.data(), o.iquad.data(),
-                               o.nquad, d_w.p, stg.st);
+                               o.nquad, d_w.p, stg->st);
     if (ier) return ier;
     if (cudaMemcpyAsync(o.wnear.data(), d_w.p, wl * sizeof(double), cudaMemcpyDeviceToHost,
-                        stg.st) != cudaSuccess ||
-        cudaStreamSynchronize(stg.st) != cudaSuccess) {
+                        stg->st) != cudaSuccess ||
+        cudaStreamSynchronize(stg->st) != cudaSuccess) {
       bie::set_last_error("near quadrature: copy to host failed");
       return BIE_ERR_CUDA;
     }
@@ -463,6 +487,29 @@ int bie_findnear(const double* cms, int64_t npatches, const double* rad_near, in
   });
 }
 
+int bie_findnear_gpu(const double* cms, int64_t npatches, const double* rad_near, int64_t ndtarg,
+                     const double* targs, int64_t ntarg, int64_t* row_ptr, int64_t* col_ind,
+                     int64_t col_cap) {
+  return guarded([&] {
+    if (!cms || !rad_near || !targs || !row_ptr || ndtarg < 3 || ntarg < 0 || npatches < 0) {
+      bie::set_last_error("findnear_gpu: invalid arguments");
+      return BIE_ERR_ARG;
+    }
+    Stage stg;
+    bie::AllocStreamScope alloc_scope(stg.st);
+    std::vector<int64_t> rp, ci;
+    int ier = bie::findnear_gpu(npatches, cms, rad_near, int(ndtarg), ntarg, targs, rp, ci, stg.st);
+    if (ier) return ier;
+    std::copy(rp.begin(), rp.end(), row_ptr);
+    if (int64_t(ci.size()) > col_cap || (!ci.empty() && !col_ind)) {
+      bie::set_last_error("findnear_gpu: col_ind needs " + std::to_string(ci.size()) + " entries");
+      return BIE_ERR_ARG;
+    }
+    std::copy(ci.begin(), ci.end(), col_ind);
+    return BIE_OK;
+  });
+}
+
 int bie_get_iquad_rsc(int64_t npatches, const int64_t* ixyzs, int64_t npts, int64_t nnz,
                       const int64_t* row_ptr, const int64_t* col_ind, int64_t* iquad) {
   bie::Surf s;
@@ -489,6 +536,45 @@ int bie_get_far_order(double eps, int64_t npatches, const int64_t* norders, cons
                          cms, rads, int(ndtarg), ntarg, targvals, int(ikerorder),
                          cdouble(zk[0], zk[1]), nnz, row_ptr, col_ind, rfac, nfars, ixyzso);
     return ier ? BIE_ERR_ARG : BIE_OK;
+  });
+}
+
+int bie_get_far_order_gpu(double eps, int64_t npatches, const int64_t* norders,
+                          const int64_t* ixyzs, const int64_t* iptype, const double* cms,
+                          const double* rads, int64_t npts, const double* srccoefs,
+                          int64_t ndtarg, int64_t ntarg, const double* targvals,
+                          int64_t ikerorder, const double* zk, int64_t nnz,
+                          const int64_t* row_ptr, const int64_t* col_ind, double rfac,
+                          int64_t* nfars, int64_t* ixyzso) {
+  return guarded([&] {
+    int ier = ensure_tables();
+    if (ier) return ier;
+    ier = check_surf(npatches, norders, ixyzs, iptype, npts);
+    if (ier) return ier;
+    Stage stg;
+    bie::AllocStreamScope alloc_scope(stg.st);
+    return bie::far_order_gpu(eps, make_surf(npatches, norders, ixyzs, iptype, npts, srccoefs,
+                                             nullptr),
+                              cms, rads, int(ndtarg), ntarg, targvals, int(ikerorder),
+                              cdouble(zk[0], zk[1]), nnz, row_ptr, col_ind, rfac, nfars, ixyzso,
+                              stg.st);
+  });
+}
+
+int bie_oversample_geom_gpu(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                            const int64_t* iptype, int64_t npts, const double* srccoefs,
+                            const double* srcvals, const int64_t* nfars, const int64_t* ixyzso,
+                            int64_t nptso, double* srcover) {
+  return guarded([&] {
+    int ier = ensure_tables();
+    if (ier) return ier;
+    ier = check_surf(npatches, norders, ixyzs, iptype, npts);
+    if (ier) return ier;
+    Stage stg;
+    bie::AllocStreamScope alloc_scope(stg.st);
+    return bie::oversample_geom_gpu(make_surf(npatches, norders, ixyzs, iptype, npts, srccoefs,
+                                              srcvals),
+                                    nfars, ixyzso, nptso, srcover, stg.st);
   });
 }
 

@@ -25,6 +25,7 @@
 
 #include "../host/basis.h"
 #include "plan.h"
+#include "basis_dev.cuh"
 #include "trig_table.cuh"
 
 namespace bie {
@@ -37,9 +38,6 @@ constexpr int kNqMaxLevel = 18;
 constexpr int kNqSlots = 64;
 constexpr int kNqStackDoubles = 8;  // per pending triangle: 6 vertex coordinates, level, cache index
 constexpr int kNqMaxSteps = 1 << 16;
-constexpr int kNqTriOrder = kMaxOrder;  // Koornwinder tables up to order 20
-constexpr int kNqLeg = 41;              // tensor bases up to order 40
-constexpr int kNqJac = kNqTriOrder + 1;
 constexpr int kNqSubDoubles = 8 * 8 + 8;  // 8 self sub-triangles x 8, then the count
 constexpr double kNqOver4Pi = 0.07957747154594767;
 // Basis values of a chunk of 32 rule nodes in shared memory: one row of
@@ -48,18 +46,6 @@ constexpr double kNqOver4Pi = 0.07957747154594767;
 // fall in distinct banks).
 constexpr int kNqPS = 34;
 constexpr unsigned kFull = 0xffffffffu;
-
-// Recurrence constants of the bases (uniform across a warp, so constant
-// memory broadcasts them):
-//   Koornwinder normalisation sqrt((2k+1)(2n+2)) at n(n+1)/2 + k;
-//   Jacobi P_m^{(0,2k+1)}: P_{m+1} = (cJacP x - cJacQ) P_m - cJacR P_{m-1} at k*21+m;
-//   Legendre: P_{k+1} = cLegA x P_k - cLegB P_{k-1}.
-__constant__ double cKoornNorm[(kNqTriOrder + 1) * (kNqTriOrder + 2) / 2];
-__constant__ double cJacP[kNqJac * kNqJac];
-__constant__ double cJacQ[kNqJac * kNqJac];
-__constant__ double cJacR[kNqJac * kNqJac];
-__constant__ double cLegA[kNqLeg];
-__constant__ double cLegB[kNqLeg];
 
 struct NqType {
   int iptype, norder, np, nv;
@@ -101,75 +87,6 @@ struct NqArgs {
   unsigned long long* next;  // this launch's item counter
   unsigned long long* stat;  // [0] kernel evaluations, [1] capped pairs
 };
-
-// Basis values at (u, v) -> prow[l * ps], l < np (when STORE) and the geometry
-// g = sum_l coefs_l P_l: xyz, d/du, d/dv.  Same bases as basis_pols.
-// Coefficients: 9 per basis function in global memory, or (SHARED) the
-// warp's copy in shared memory padded to 10 so that pairs load as one
-// 16-byte access.
-template <bool STORE, bool SHARED = false>
-__device__ void basis_geom(int iptype, int n, double u, double v, const double* __restrict__ c,
-                           double* prow, int ps, double* g) {
-#pragma unroll
-  for (int k = 0; k < 9; ++k) g[k] = 0.0;
-  auto emit = [&](int idx, double p) {
-    if (STORE) prow[idx * ps] = p;
-    if (SHARED) {
-      const double2* ci = reinterpret_cast<const double2*>(c + 10 * idx);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const double2 cc = ci[k];
-        g[2 * k] = fma(cc.x, p, g[2 * k]);
-        g[2 * k + 1] = fma(cc.y, p, g[2 * k + 1]);
-      }
-      g[8] = fma(ci[4].x, p, g[8]);
-    } else {
-      const double* ci = c + 9 * idx;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) g[k] = fma(__ldg(ci + k), p, g[k]);
-    }
-  };
-  if (iptype == 1) {
-    double leg[kNqTriOrder + 1];
-    const double z = 2.0 * u + v - 1.0, y = 1.0 - v, y2 = y * y, x = 1.0 - 2.0 * v;
-    leg[0] = 1.0;
-    if (n >= 1) leg[1] = z;
-    for (int k = 1; k < n; ++k) leg[k + 1] = cLegA[k] * z * leg[k] - cLegB[k] * y2 * leg[k - 1];
-    for (int k = 0; k <= n; ++k) {
-      const double lk = leg[k];
-      const double b = 2.0 * k + 1.0;
-      int idx = k * (k + 1) / 2 + k;
-      emit(idx, lk * cKoornNorm[idx]);
-      if (n - k < 1) continue;
-      double jp = 1.0, jc = 0.5 * ((b + 2.0) * x - b);
-      idx = (k + 1) * (k + 2) / 2 + k;
-      emit(idx, lk * jc * cKoornNorm[idx]);
-      for (int m = 1; m < n - k; ++m) {
-        const int t = k * kNqJac + m;
-        const double jn = (cJacP[t] * x - cJacQ[t]) * jc - cJacR[t] * jp;
-        jp = jc;
-        jc = jn;
-        const int nn = m + 1 + k;
-        idx = nn * (nn + 1) / 2 + k;
-        emit(idx, lk * jc * cKoornNorm[idx]);
-      }
-    }
-  } else {
-    const bool leg = iptype == 11;
-    double pu[kNqLeg];
-    pu[0] = 1.0;
-    if (n >= 1) pu[1] = u;
-    for (int k = 1; k < n; ++k)
-      pu[k + 1] = leg ? cLegA[k] * u * pu[k] - cLegB[k] * pu[k - 1] : 2.0 * u * pu[k] - pu[k - 1];
-    double pvm = 0.0, pvc = 1.0;
-    for (int i = 0; i <= n; ++i) {
-      for (int j = 0; j <= n; ++j) emit(j + (n + 1) * i, pu[j] * pvc);
-      const double nx = i == 0 ? v : (leg ? cLegA[i] * v * pvc - cLegB[i] * pvm : 2.0 * v * pvc - pvm);
-      pvm = pvc;
-      pvc = nx;
-    }
-  }
-}
 
 // Combined-field kernel (alpha G + beta dG/dn_y) / 4pi at target x of the
 // source y with unit normal nr (host/nearquad.cpp LapComb / HelmComb).
@@ -687,46 +604,6 @@ __global__ void __launch_bounds__(256) nq_pair_kernel(NqArgs a) {
   }
 }
 
-void fill_constants(cudaStream_t st) {
-  static thread_local std::vector<double> host;
-  if (host.empty()) {
-    host.assign((kNqTriOrder + 1) * (kNqTriOrder + 2) / 2 + 3 * kNqJac * kNqJac + 2 * kNqLeg, 0.0);
-    double* norm = host.data();
-    double* jp = norm + (kNqTriOrder + 1) * (kNqTriOrder + 2) / 2;
-    double* jq = jp + kNqJac * kNqJac;
-    double* jr = jq + kNqJac * kNqJac;
-    double* la = jr + kNqJac * kNqJac;
-    double* lb = la + kNqLeg;
-    for (int n = 0; n <= kNqTriOrder; ++n)
-      for (int k = 0; k <= n; ++k) norm[n * (n + 1) / 2 + k] = std::sqrt((2.0 * k + 1.0) * (2.0 * n + 2.0));
-    for (int k = 0; k < kNqJac; ++k) {
-      const double b = 2.0 * k + 1.0;
-      for (int m = 1; m < kNqJac; ++m) {
-        const double c0 = 2.0 * (m + 1.0) * (m + b + 1.0) * (2.0 * m + b);
-        jp[k * kNqJac + m] = (2.0 * m + b + 1.0) * (2.0 * m + b + 2.0) * (2.0 * m + b) / c0;
-        jq[k * kNqJac + m] = (2.0 * m + b + 1.0) * b * b / c0;
-        jr[k * kNqJac + m] = 2.0 * m * (m + b) * (2.0 * m + b + 2.0) / c0;
-      }
-    }
-    for (int k = 0; k < kNqLeg; ++k) {
-      la[k] = (2.0 * k + 1.0) / (k + 1.0);
-      lb[k] = k / (k + 1.0);
-    }
-  }
-  const double* h = host.data();
-  size_t off = 0;
-  auto put = [&](const void* sym, size_t n) {
-    cudaMemcpyToSymbolAsync(sym, h + off, n * sizeof(double), 0, cudaMemcpyHostToDevice, st);
-    off += n;
-  };
-  put(cKoornNorm, (kNqTriOrder + 1) * (kNqTriOrder + 2) / 2);
-  put(cJacP, kNqJac * kNqJac);
-  put(cJacQ, kNqJac * kNqJac);
-  put(cJacR, kNqJac * kNqJac);
-  put(cLegA, kNqLeg);
-  put(cLegB, kNqLeg);
-}
-
 template <class T>
 cudaError_t upload(DBuf<T>& d, const T* h, size_t n, cudaStream_t st) {
   cudaError_t e = d.alloc(std::max<size_t>(n, 1));
@@ -961,7 +838,7 @@ int getnearquad_gpu(const Surf& s, int ndt, int64_t nt, const double* targs,
     set_last_error(std::string("getnearquad_gpu: device buffers: ") + cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? kErrNoMem : kErrCuda;
   }
-  fill_constants(st);
+  fill_basis_constants(st);
   a.zr = zk.real();
   a.zi = zk.imag();
   a.ar = alpha.real();

@@ -298,6 +298,19 @@ void patch_id_uvs(const Surf& s, int64_t* ipatch_id, double* uvs) {
   }
 }
 
+namespace {
+// |c - t|^2 <= r^2 with every product and sum rounded separately (no fused
+// multiply-add), the same decision as the device near list makes.
+bool within_radius(const double* c, const double* t, double r) {
+  const double a = c[0] - t[0], b = c[1] - t[1], e = c[2] - t[2];
+  volatile double a2 = a * a, b2 = b * b, e2 = e * e;
+  volatile double s = a2 + b2;
+  volatile double s2 = s + e2;
+  volatile double r2 = r * r;
+  return s2 <= r2;
+}
+}  // namespace
+
 void findnear(int64_t npatches, const double* cms, const double* rads, int ndt, int64_t nt,
               const double* targs, std::vector<int64_t>& row_ptr, std::vector<int64_t>& col_ind) {
   // Bin patch centroids on a uniform grid of cell size >= max radius; a
@@ -352,10 +365,7 @@ void findnear(int64_t npatches, const double* cms, const double* rads, int ndt, 
           const int64_t cell = (z * dims[1] + y) * dims[0] + x;
           for (int64_t q = cstart[cell]; q < cstart[cell + 1]; ++q) {
             const int64_t j = cidx[q];
-            const double* cj = cms + 3 * j;
-            const double r2 = (cj[0] - t[0]) * (cj[0] - t[0]) + (cj[1] - t[1]) * (cj[1] - t[1]) +
-                              (cj[2] - t[2]) * (cj[2] - t[2]);
-            if (r2 <= rads[j] * rads[j]) row.push_back(j);
+            if (within_radius(cms + 3 * j, t, rads[j])) row.push_back(j);
           }
         }
     std::sort(row.begin(), row.end());
@@ -556,8 +566,8 @@ int oversample_geom(const Surf& s, const int64_t* nfars, const int64_t* ixyzso, 
       }
       finish_normal(o);
     }
-    int ic[4], icf[4];
-    const int nclash = clashing_indices(ip, no, nfar, ic, icf);
+    std::vector<int> ic(std::max(np, nf)), icf(ic.size());
+    const int nclash = clashing_indices(ip, no, nfar, ic.data(), icf.data());
     for (int c = 0; c < nclash; ++c)
       for (int k = 0; k < 12; ++k) srcover[12 * (so + icf[c]) + k] = s.srcvals[12 * (st + ic[c]) + k];
   }

@@ -187,14 +187,27 @@ def get_centroid_rads(s: Surface):
     return cms, rads
 
 
-def findnear(cms, rad_near, targs):
-    """Row-sparse near list (1-based row_ptr, col_ind)."""
+def findnear(cms, rad_near, targs, engine: str = "cpu"):
+    """Row-sparse near list (1-based row_ptr, col_ind); engine "gpu" builds it
+    on the device (the same lists), "auto" there when a device is visible."""
     lib = _init()
     cms = np.ascontiguousarray(cms, float)
     rad_near = np.ascontiguousarray(rad_near, float)
     targs = np.ascontiguousarray(targs, float)
     ndt = targs.shape[1]
     nt = targs.shape[0]
+    if _engine(engine) == "gpu":
+        row_ptr = np.zeros(nt + 1, np.int64)
+        cap = 32 * nt + 64
+        while True:
+            col_ind = np.zeros(cap, np.int64)
+            st = lib.bie_findnear_gpu(L.ptr(cms), cms.shape[0], L.ptr(rad_near), ndt, L.ptr(targs),
+                                      nt, L.ptr(row_ptr), L.ptr(col_ind), cap)
+            nnz = int(row_ptr[-1] - 1)
+            if st == 0 or nnz <= cap:
+                L.check(st, "findnear_gpu")
+                return row_ptr, col_ind[:nnz]
+            cap = nnz
     nnz = L.I64()
     L.check(lib.bie_findnearmem(L.ptr(cms), cms.shape[0], L.ptr(rad_near), ndt, L.ptr(targs), nt,
                                 L.C.byref(nnz)), "findnearmem")
@@ -214,13 +227,16 @@ def get_iquad_rsc(s: Surface, row_ptr, col_ind):
     return iquad
 
 
-def get_far_order(eps, s: Surface, cms, rads, targs, ikerorder, zk, row_ptr, col_ind, rfac):
+def get_far_order(eps, s: Surface, cms, rads, targs, ikerorder, zk, row_ptr, col_ind, rfac,
+                  engine: str = "cpu"):
+    """Far-field oversampling order per patch and ixyzso; engine as findnear."""
     lib = _init()
     targs = np.ascontiguousarray(targs, float)
     nf = np.zeros(s.npatches, np.int64)
     ixo = np.zeros(s.npatches + 1, np.int64)
     z = np.array([complex(zk).real, complex(zk).imag])
-    L.check(lib.bie_get_far_order(eps, s.npatches, L.ptr(s.norders), L.ptr(s.ixyzs),
+    fn = lib.bie_get_far_order_gpu if _engine(engine) == "gpu" else lib.bie_get_far_order
+    L.check(fn(eps, s.npatches, L.ptr(s.norders), L.ptr(s.ixyzs),
                                   L.ptr(s.iptype), L.ptr(cms), L.ptr(rads), s.npts,
                                   L.ptr(s.srccoefs), targs.shape[1], targs.shape[0], L.ptr(targs),
                                   ikerorder, L.ptr(z), col_ind.shape[0], L.ptr(row_ptr),
@@ -228,11 +244,13 @@ def get_far_order(eps, s: Surface, cms, rads, targs, ikerorder, zk, row_ptr, col
     return nf, ixo
 
 
-def oversample_geom(s: Surface, novers, ixyzso):
+def oversample_geom(s: Surface, novers, ixyzso, engine: str = "cpu"):
+    """Oversampled geometry srcover (nptso x 12); engine as findnear."""
     lib = _init()
     nptso = int(ixyzso[-1] - 1)
     so = np.zeros((nptso, 12))
-    L.check(lib.bie_oversample_geom(s.npatches, L.ptr(s.norders), L.ptr(s.ixyzs), L.ptr(s.iptype),
+    fn = lib.bie_oversample_geom_gpu if _engine(engine) == "gpu" else lib.bie_oversample_geom
+    L.check(fn(s.npatches, L.ptr(s.norders), L.ptr(s.ixyzs), L.ptr(s.iptype),
                                     s.npts, L.ptr(s.srccoefs), L.ptr(s.srcvals), L.ptr(novers),
                                     L.ptr(ixyzso), nptso, L.ptr(so)), "oversample_geom")
     return so
@@ -386,8 +404,11 @@ def setup(s: Surface, kind: int, eps: float, params, targs=None, ipatch_id=None,
           engine: str = "auto", stats=None):
     """The setup of lap_comb_dir_eval / helm_comb_dir_solver: near list, far
     order, oversampled geometry and near quadrature.  targs defaults to the
-    surface nodes (on-surface, with self interactions).  engine and stats:
-    the near quadrature generator and its counters (see getnearquad)."""
+    surface nodes (on-surface, with self interactions).  engine: where the
+    steps run ("gpu": near list, far orders, oversampled geometry and near
+    quadrature on the device; "cpu": on the host; "auto": the device when one
+    is visible); stats: the near quadrature generator's counters (see
+    getnearquad)."""
     if targs is None:
         targs = s.srcvals
         ipatch_id, uvs_targ = s.patch_id_uvs()
@@ -400,13 +421,15 @@ def setup(s: Surface, kind: int, eps: float, params, targs=None, ipatch_id=None,
     norder_avg = int(math.floor(s.norders.sum() / s.npatches))
     rfac, rfac0 = get_rfacs(norder_avg, iptype_avg)
     cms, rads = get_centroid_rads(s)
-    row_ptr, col_ind = findnear(cms, rads * rfac, targs)
+    engine = _engine(engine)
+    row_ptr, col_ind = findnear(cms, rads * rfac, targs, engine=engine)
     iquad = get_iquad_rsc(s, row_ptr, col_ind)
     beta = params[1] if kind == 0 else params[2]
     ikerorder = 0 if abs(beta) > 1e-16 else -1
     zk = 0.0 if kind == 0 else params[0]
-    novers, ixyzso = get_far_order(eps, s, cms, rads, targs, ikerorder, zk, row_ptr, col_ind, rfac)
-    srcover = oversample_geom(s, novers, ixyzso)
+    novers, ixyzso = get_far_order(eps, s, cms, rads, targs, ikerorder, zk, row_ptr, col_ind, rfac,
+                                   engine=engine)
+    srcover = oversample_geom(s, novers, ixyzso, engine=engine)
     so = Surface(novers, ixyzso, s.iptype, srcover, np.zeros((srcover.shape[0], 9)))
     wover = so.qwts()
     wnear = getnearquad(s, kind, eps, params, targs, ipatch_id, uvs_targ, row_ptr, col_ind, iquad,

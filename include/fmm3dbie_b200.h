@@ -101,6 +101,28 @@ int bie_oversample_geom(int64_t npatches, const int64_t* norders, const int64_t*
                         const int64_t* iptype, int64_t npts, const double* srccoefs,
                         const double* srcvals, const int64_t* nfars, const int64_t* ixyzso,
                         int64_t nptso, double* srcover);
+/* The three setup steps above on the device (same arguments and results;
+ * no reference counterpart, the reference runs its setup on the CPU).
+ * bie_findnear_gpu fills row_ptr and, when row_ptr[ntarg] - 1 <= col_cap,
+ * col_ind; otherwise it returns BIE_ERR_ARG and the caller retries with
+ * col_ind of row_ptr[ntarg] - 1 entries.  The near set is decided with the
+ * host's rounding (no fused multiply-add), so both return the same lists;
+ * far orders and oversampled geometry agree with the host's up to rounding
+ * (the order decision compares with a tolerance). */
+int bie_findnear_gpu(const double* cms, int64_t npatches, const double* rad_near, int64_t ndtarg,
+                     const double* targs, int64_t ntarg, int64_t* row_ptr, int64_t* col_ind,
+                     int64_t col_cap);
+int bie_get_far_order_gpu(double eps, int64_t npatches, const int64_t* norders,
+                          const int64_t* ixyzs, const int64_t* iptype, const double* cms,
+                          const double* rads, int64_t npts, const double* srccoefs,
+                          int64_t ndtarg, int64_t ntarg, const double* targvals,
+                          int64_t ikerorder, const double* zk, int64_t nnz,
+                          const int64_t* row_ptr, const int64_t* col_ind, double rfac,
+                          int64_t* nfars, int64_t* ixyzso);
+int bie_oversample_geom_gpu(int64_t npatches, const int64_t* norders, const int64_t* ixyzs,
+                            const int64_t* iptype, int64_t npts, const double* srccoefs,
+                            const double* srcvals, const int64_t* nfars, const int64_t* ixyzso,
+                            int64_t nptso, double* srcover);
 /* oversample_fun_surf (surf_routs.f90:451), nd interleaved real functions */
 int bie_oversample_fun_surf(int64_t nd, int64_t npatches, const int64_t* norders,
                             const int64_t* ixyzs, const int64_t* iptype, int64_t npts,
@@ -163,9 +185,10 @@ int bie_getnearquad_helm_comb_dir_eval_gpu(
     const double* zpars, int64_t iquadtype, int64_t nnz, const int64_t* row_ptr,
     const int64_t* col_ind, const int64_t* iquad, double rfac0, int64_t nquad, double* wnear,
     int64_t* stats);
-/* Near quadrature engine of the setups inside the simple evaluators and
- * solvers (lap/helm_comb_dir_eval, *_solver): 1 = device (default), 0 =
- * host.  Patches above the device limit always use the host generator. */
+/* Setup engine of the simple evaluators and solvers (lap/helm_comb_dir_eval,
+ * *_solver): 1 = device near lists, far orders, oversampled geometry and
+ * near quadrature (default), 0 = host.  Patches above 256 basis functions
+ * always use the host. */
 int bie_set_nearquad_engine(int64_t engine);
 int64_t bie_get_nearquad_engine(void);
 
