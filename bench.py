@@ -432,6 +432,27 @@ def main():
                "d2h_bytes_per_step": int(d2h), "path": "bie_helm_comb_dir_solver_guru_ext (host buffers)",
                "rres": float(out[1][0])}
 
+    # ---- cold solve through the reference's simple interface -------------------
+    # helm_comb_dir_solver: setup (near list, far orders, oversampled geometry,
+    # near quadrature) + plan + FP64 GMRES, host buffers in and out
+    e2e_cold = None
+    if args.e2e_steps > 0 and rank == 0:
+        lib_ = L.lib()
+        cold = {}
+        for eng, reps in ((1, 2), (0, 1)):
+            lib_.bie_set_nearquad_engine(eng)
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                niter_c, _, rres_c, _, st_c = layer.helm_comb_dir_solver(s, EPS, ZPARS, 300, 1, rhs,
+                                                                        TOL_RES)
+                cold[eng] = time.perf_counter() - t0
+        lib_.bie_set_nearquad_engine(1)
+        e2e_cold = {"value": 1.0 / cold[1], "unit": "solves/s",
+                    "path": "bie_helm_comb_dir_solver (setup + plan + FP64 GMRES, host buffers)",
+                    "s_per_solve_device_setup": round(cold[1], 3),
+                    "s_per_solve_host_setup": round(cold[0], 3), "niter": niter_c,
+                    "rres": rres_c}
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(s, st, int(info64["niter"][0]))
@@ -489,6 +510,7 @@ def main():
             "gpu_launches": launches,
             "clocks": ck,
             "e2e": e2e,
+            "e2e_cold": e2e_cold,
             "cpu_baseline": base,
             "nearquad": nearquad,
             "batched": batched,
