@@ -324,7 +324,7 @@ def main():
     r_d = torch.tensor(rhs, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
 
-    # accuracy judge: tight FP64 solution
+    # accuracy reference: tight FP64 solution
     x_ref, info_ref = P.solve(r_d, 0.5, mode=0, numit=300, eps_gmres=1e-12)
     w = torch.tensor(s.qwts(), device=dev)
 

@@ -8,7 +8,7 @@ density of the plane-wave problem
     (zid I + K_k) sigma = -exp(i k d.x)          (zid = 1/2, zpars = (k, -ik, 1))
 
 and the prediction is handed to the solver as its initial guess.  GMRES from
-zero stays the fallback and the judge: the solve runs to the same relative
+zero stays the fallback and the arbiter: the solve runs to the same relative
 residual either way, and a guess whose residual is not below ||rhs|| is
 dropped.
 
