@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 
 #include "plan.h"
@@ -207,6 +208,14 @@ int BatchPlan::tune(int precision, int nd, cudaStream_t st, std::unique_ptr<Conf
       chunk = std::max<int64_t>(kFarTileSources, (chunk + kFarTileSources - 1) / kFarTileSources * kFarTileSources);
       cand.emplace_back(v, chunk);
     }
+  }
+  // BIE_BATCH_VARIANT / BIE_BATCH_CHUNK pin the far shape and chunk length
+  if (const char* ev = std::getenv("BIE_BATCH_VARIANT")) {
+    const int v = std::min(std::max(std::atoi(ev), 0), dev::batch_far_variants(precision, nd) - 1);
+    const char* ec = std::getenv("BIE_BATCH_CHUNK");
+    int64_t chunk = ec ? std::max<int64_t>(kFarTileSources, std::atoll(ec)) : cand.front().second;
+    chunk = (chunk + kFarTileSources - 1) / kFarTileSources * kFarTileSources;
+    cand.assign(1, {v, chunk});
   }
   std::unique_ptr<Config> best;
   float best_ms = 1e30f;
