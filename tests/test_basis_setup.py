@@ -175,3 +175,14 @@ def test_reference_go3_mesh_if_present(built):
     s = S.read_go3(path)
     assert s.npatches == 192 and s.npts == 1920
     assert abs(s.qwts().sum() - 4 * np.pi) < 1e-3
+
+
+def test_chebyshev_torus_matches_legendre_torus():
+    """The Chebyshev-node torus of the device tests describes the same surface
+    as the Gauss-Legendre one: same area and the same near list sizes."""
+    from _surfaces import torus_cheb
+    from fmm3dbie_b200.warmstart import torus_surface
+    tc = torus_cheb(16, 8, 5)
+    tl = torus_surface(16, 8, 5)
+    assert abs(tc.qwts().sum() - tl.qwts().sum()) < 1e-8 * tl.qwts().sum()
+    assert np.all(tc.iptype == 12)

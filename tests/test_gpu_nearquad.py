@@ -120,3 +120,14 @@ def test_refinement_cache_settings(monkeypatch, levels, budget_mb):
         monkeypatch.setenv("BIE_NEARQUAD_CACHE_BUDGET_MB", budget_mb)
     s = S.icosa_ellipsoid(1, 6, (1.0, 2.0, 3.0))
     _compare(s, 1, 1e-7, (1.5, -1.5j, 1.0), _near_setup(s))
+
+
+def test_chebyshev_quads_and_mixed_patches():
+    """Tensor Chebyshev quads (iptype 12) and one surface mixing triangles of
+    orders 4 and 6 with Chebyshev quads of order 5."""
+    from _surfaces import concat, torus_cheb
+    t = torus_cheb()
+    _compare(t, 1, 1e-7, (2.0, -2.0j, 1.0), _near_setup(t))
+    m = concat(S.icosa_sphere(1, 4), S.icosa_ellipsoid(1, 6, (1.0, 2.0, 3.0)), torus_cheb(8, 4, 5),
+               shifts=[(0, 0, 0), (6, 0, 0), (0, 8, 0)])
+    _compare(m, 0, 1e-7, (1.0, 1.0), _near_setup(m))

@@ -15,12 +15,16 @@ pytestmark = pytest.mark.gpu
 
 
 def _surfaces():
+    from _surfaces import concat, torus_cheb
     from fmm3dbie_b200.warmstart import torus_surface
     return {
         "sphere4": S.icosa_sphere(1, 4),
         "ellipsoid6": S.icosa_ellipsoid(2, 6, (1.0, 2.0, 3.0)),
         "ellipsoid8": S.icosa_ellipsoid(1, 8, (0.7, 1.5, 2.5)),
         "torus5": torus_surface(16, 8, 5),
+        "torus5_chebyshev": torus_cheb(),
+        "mixed": concat(S.icosa_sphere(1, 4), S.icosa_ellipsoid(1, 6, (1.0, 2.0, 3.0)),
+                        torus_cheb(8, 4, 5), shifts=[(0, 0, 0), (6, 0, 0), (0, 8, 0)]),
     }
 
 
