@@ -119,6 +119,8 @@ _SIGS = {
     "bie_plan_matvec": (C.c_int, [VP, I64, I64, VP, VP, VP]),
     "bie_plan_solve": (C.c_int, [VP, I64, I64, PDBL, VP, VP, I64, DBL, VP, PI64, PDBL, PDBL, VP]),
     "bie_plan_timing": (C.c_int, [VP, I64, PDBL]),
+    "bie_plan_set_far": (C.c_int, [VP, I64, I64, I64, I64]),
+    "bie_plan_get_far": (C.c_int, [VP, I64, I64, PI64]),
     "bie_farfield_dev": (C.c_int, [I64, PDBL, I64, VP, VP, VP, VP, I64, VP, DBL, I64, VP, VP]),
     "bie_farfield_dev_noalloc": (C.c_int, [I64, PDBL, I64, VP, VP, VP, VP, I64, VP, DBL, I64, VP,
                                            VP]),

@@ -1138,6 +1138,24 @@ int bie_plan_info(void* plan, int64_t* info) {
   return BIE_OK;
 }
 
+int bie_plan_set_far(void* plan, int64_t iprec, int64_t nd, int64_t variant, int64_t nchunks) {
+  if (!plan) return BIE_ERR_ARG;
+  return guarded([&] {
+    return static_cast<bie::Plan*>(plan)->set_far_config(int(iprec), int(nd), int(variant),
+                                                         int(nchunks));
+  });
+}
+
+int bie_plan_get_far(void* plan, int64_t iprec, int64_t nd, int64_t* out) {
+  if (!plan || !out || (iprec != 0 && iprec != 1) || nd < 1) return BIE_ERR_ARG;
+  const bie::Plan* P = static_cast<bie::Plan*>(plan);
+  const auto c = P->far_config(int(iprec), int(nd));
+  out[0] = c.variant;
+  out[1] = c.nchunks;
+  out[2] = P->tc_error();
+  return BIE_OK;
+}
+
 int bie_plan_matvec(void* plan, int64_t iprec, int64_t nd, const double* sigma_dev,
                     double* pot_dev, void* stream) {
   if (!plan || (iprec != 0 && iprec != 1) || nd < 1) return BIE_ERR_ARG;

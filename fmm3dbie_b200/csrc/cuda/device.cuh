@@ -84,6 +84,7 @@ struct MatvecArgs {
   int weff_f32 = 0;
   int far_variant = 0;            // far-kernel block shape (see far_block_targets)
   const void* ab = nullptr;       // per-source constants for the multi-density kernel
+  int* tc_err = nullptr;          // set by the tensor-core far field if a completion wait timed out
 };
 
 cudaError_t launch_strengths(const Geometry& g, const KParams& kp, const MatvecArgs& a,
@@ -115,6 +116,12 @@ int far_nchunks(int64_t ntarg, int64_t nptso, int kind, int precision, int nd, i
 // chunks that fills `waves` waves of resident blocks.
 // md = 1 selects the multi-density kernel's shapes (nd > 1).
 int far_variants();
+// Tensor-core far field (variants 3 and 4 of the multi-density FP32
+// Helmholtz path): densities per CTA, 0 where the variant does not apply.
+int far_tc_group(int variant, int nd, int precision, int kind);
+// Launches it, or with occ != null reports its resident CTAs per SM.
+cudaError_t far_tc(int variant, const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                   cudaStream_t st, int* occ);
 int far_block_targets(int precision, int variant, int md = 0, int nd = 1);
 int far_md_group(int variant, int nd);
 int far_blocks_per_sm(const KParams& kp, int precision, int variant, int md = 0, int nd = 1);

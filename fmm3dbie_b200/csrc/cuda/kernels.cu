@@ -20,6 +20,7 @@
 
 #include "device.cuh"
 
+#include "pair.cuh"
 #include "trig_table.cuh"
 
 namespace bie {
@@ -31,19 +32,6 @@ std::atomic<int64_t> g_launches{0};
 inline void count(int64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 constexpr double kOver4Pi = 0.07957747154594767;
-
-template <typename R>
-struct Vec;
-template <>
-struct Vec<float> {
-  using T2 = float2;
-  using T4 = float4;
-};
-template <>
-struct Vec<double> {
-  using T2 = double2;
-  using T4 = double4;
-};
 
 // ---------------------------------------------------------------------------
 // (a) strengths
@@ -96,90 +84,6 @@ __global__ void strengths_kernel(Geometry g, KParams kp, const double* __restric
 // ---------------------------------------------------------------------------
 // (b) far field: tiled direct N-body
 // ---------------------------------------------------------------------------
-// Contribution of one source to one target: charge c = (s.x, s.y), dipole
-// strength d = (s.z, s.w) along the source normal n,
-//   e^{ikr}/r [ c + d (n.(t-s)) (1 - ikr) / r^2 ],   (1/(4 pi) is in c, d).
-// The phase kr carries an absolute error of about kr 2^-24 in single
-// precision already; __sincosf's scaled argument adds an error of the same
-// order, so no separate range reduction is done.
-// CHECK = false drops the r^2 >= thresh^2 test; callers use it only where no
-// pair of the tile can fall below the threshold, so the result is the same.
-template <bool CHECK = true>
-__device__ __forceinline__ void pair_helm(float tx, float ty, float tz, const float4 g0,
-                                          const float2 g1, const float4 s, float k, float kim,
-                                          float thr2, bool ck, float& pr, float& pi,
-                                          const double2* = nullptr) {
-  const float dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
-  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float rinv = (!CHECK || r2 >= thr2) ? rsqrtf(r2) : 0.0f;
-  const float r = r2 * rinv;
-  const float kr = k * r;
-  float sn, cs;
-  __sincosf(kr, &sn, &cs);
-  float rs = rinv;
-  if (ck) rs *= __expf(-kim * r);
-  const float dn = fmaf(dx, g0.w, fmaf(dy, g1.x, dz * g1.y));
-  const float u = dn * (rinv * rinv);
-  float xr, xi;
-  if (ck) {
-    // x = c + d u ((1 + kim r) - i kr)  for complex k = kr + i kim
-    const float ur = u * (1.0f + kim * r);
-    const float p = u * kr;
-    xr = fmaf(s.w, p, fmaf(s.z, ur, s.x));
-    xi = fmaf(-s.z, p, fmaf(s.w, ur, s.y));
-  } else {
-    // x = c + d u (1 - i kr) = c + u (d_r + d_i kr, d_i - d_r kr)
-    xr = fmaf(u, fmaf(s.w, kr, s.z), s.x);
-    xi = fmaf(u, fmaf(-s.z, kr, s.w), s.y);
-  }
-  const float er = xr * rs, ei = xi * rs;
-  pr = fmaf(cs, er, fmaf(-sn, ei, pr));
-  pi = fmaf(cs, ei, fmaf(sn, er, pi));
-}
-
-template <bool CHECK = true>
-__device__ __forceinline__ void pair_helm(double tx, double ty, double tz, const double4 g0,
-                                          const double2 g1, const double4 s, double k, double kim,
-                                          double thr2, bool ck, double& pr, double& pi,
-                                          const double2* tab = nullptr) {
-  const double dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
-  const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-  const double rinv = (!CHECK || r2 >= thr2) ? rsqrt(r2) : 0.0;
-  const double r = r2 * rinv;
-  const double kr = k * r;
-  double sn, cs;
-  if (tab)
-    sincos_tab(kr, tab, sn, cs);
-  else
-    sincos(kr, &sn, &cs);
-  double rs = rinv;
-  if (ck) rs *= exp(-kim * r);
-  const double dn = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y));
-  const double q = dn * rinv * rinv;
-  const double wr = ck ? q * (1.0 + kim * r) : q;
-  const double wi = -q * kr;
-  const double er = fma(s.z, wr, fma(-s.w, wi, s.x)) * rs;
-  const double ei = fma(s.z, wi, fma(s.w, wr, s.y)) * rs;
-  pr = fma(cs, er, fma(-sn, ei, pr));
-  pi = fma(cs, ei, fma(sn, er, pi));
-}
-
-template <typename R, bool CHECK = true>
-__device__ __forceinline__ void pair_lap(R tx, R ty, R tz, const typename Vec<R>::T4 g0,
-                                         const typename Vec<R>::T2 g1,
-                                         const typename Vec<R>::T2 s, R thr2, R& p) {
-  const R dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
-  const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-  R rinv;
-  if constexpr (sizeof(R) == 4)
-    rinv = (!CHECK || r2 >= thr2) ? rsqrtf(r2) : R(0);
-  else
-    rinv = (!CHECK || r2 >= thr2) ? rsqrt(r2) : R(0);
-  const R dn = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y));
-  const R e = fma(s.y * dn, rinv * rinv, s.x);
-  p = fma(e, rinv, p);
-}
-
 // One block's work of the far field: target block bx (NT*TPT targets),
 // source chunk by (chunk_len sources), density bz.  Shared tiles and the
 // FP64 trig table come from the calling kernel.
@@ -1270,7 +1174,15 @@ cudaError_t far_md_variant(int v, const Geometry& g, const KParams& kp, const Ma
 cudaError_t far_md_any(const Geometry& g, const KParams& kp, const MatvecArgs& a, cudaStream_t st,
                        int* occ) {
   const bool ck = kp.kind == 1 && kp.ki != 0.0;
-  const int v = a.far_variant;
+  int v = a.far_variant;
+  if (v >= 3) {
+    if (far_tc_group(v, a.nd, a.precision, kp.kind) > 0) return far_tc(v, g, kp, a, st, occ);
+    if (occ) {  // not a shape of this path: the autotuner skips it
+      *occ = 0;
+      return cudaSuccess;
+    }
+    v = 0;
+  }
   if (a.precision == 1) {
     if (kp.kind == 1)
       return ck ? far_md_variant<1, float, true>(v, g, kp, a, st, occ)
@@ -1287,6 +1199,10 @@ cudaError_t far_any(const Geometry& g, const KParams& kp, const MatvecArgs& a, c
                     int* occ) {
   const bool ck = kp.kind == 1 && kp.ki != 0.0;
   const int v = a.far_variant;
+  if (v >= 3 && occ) {  // the tensor-core shapes are multi-density only
+    *occ = 0;
+    return cudaSuccess;
+  }
   if (a.precision == 1) {
     if (kp.kind == 1)
       return ck ? far_variant<1, float, true>(v, g, kp, a, st, occ)
@@ -1598,9 +1514,10 @@ cudaError_t launch_source_consts(const Geometry& g, const KParams& kp, int preci
   return cudaGetLastError();
 }
 
-int far_variants() { return 3; }
+int far_variants() { return 5; }
 
 int far_block_targets(int precision, int variant, int md, int nd) {
+  if (md && far_tc_group(variant, nd, precision, 1) > 0) return 64;
   const int v = variant < 0 || variant > 2 ? 0 : variant;
   if (md) return kMdShapes[md_class(nd)][v][0] * kMdShapes[md_class(nd)][v][1];
   return precision == 1 ? kF32Shapes[v][0] * kF32Shapes[v][1]
@@ -1608,6 +1525,8 @@ int far_block_targets(int precision, int variant, int md, int nd) {
 }
 
 int far_md_group(int variant, int nd) {
+  const int tc = far_tc_group(variant, nd, 1, 1);
+  if (tc > 0) return tc;
   return kMdShapes[md_class(nd)][variant < 0 || variant > 2 ? 0 : variant][2];
 }
 

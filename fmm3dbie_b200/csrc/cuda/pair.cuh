@@ -1,0 +1,113 @@
+// Pair functions of the far field (one source's contribution to one target)
+// and the vector types they use, shared by the kernels that must evaluate the
+// kernel identically: the far-field kernels, the FP32 fold that cancels their
+// near-pair values, and the tensor-core far field.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "trig_table.cuh"
+
+namespace bie {
+namespace dev {
+namespace {
+
+template <typename R>
+struct Vec;
+template <>
+struct Vec<float> {
+  using T2 = float2;
+  using T4 = float4;
+};
+template <>
+struct Vec<double> {
+  using T2 = double2;
+  using T4 = double4;
+};
+
+// Contribution of one source to one target: charge c = (s.x, s.y), dipole
+// strength d = (s.z, s.w) along the source normal n,
+//   e^{ikr}/r [ c + d (n.(t-s)) (1 - ikr) / r^2 ],   (1/(4 pi) is in c, d).
+// The phase kr carries an absolute error of about kr 2^-24 in single
+// precision already; __sincosf's scaled argument adds an error of the same
+// order, so no separate range reduction is done.
+// CHECK = false drops the r^2 >= thresh^2 test; callers use it only where no
+// pair of the tile can fall below the threshold, so the result is the same.
+template <bool CHECK = true>
+__device__ __forceinline__ void pair_helm(float tx, float ty, float tz, const float4 g0,
+                                          const float2 g1, const float4 s, float k, float kim,
+                                          float thr2, bool ck, float& pr, float& pi,
+                                          const double2* = nullptr) {
+  const float dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float rinv = (!CHECK || r2 >= thr2) ? rsqrtf(r2) : 0.0f;
+  const float r = r2 * rinv;
+  const float kr = k * r;
+  float sn, cs;
+  __sincosf(kr, &sn, &cs);
+  float rs = rinv;
+  if (ck) rs *= __expf(-kim * r);
+  const float dn = fmaf(dx, g0.w, fmaf(dy, g1.x, dz * g1.y));
+  const float u = dn * (rinv * rinv);
+  float xr, xi;
+  if (ck) {
+    // x = c + d u ((1 + kim r) - i kr)  for complex k = kr + i kim
+    const float ur = u * (1.0f + kim * r);
+    const float p = u * kr;
+    xr = fmaf(s.w, p, fmaf(s.z, ur, s.x));
+    xi = fmaf(-s.z, p, fmaf(s.w, ur, s.y));
+  } else {
+    // x = c + d u (1 - i kr) = c + u (d_r + d_i kr, d_i - d_r kr)
+    xr = fmaf(u, fmaf(s.w, kr, s.z), s.x);
+    xi = fmaf(u, fmaf(-s.z, kr, s.w), s.y);
+  }
+  const float er = xr * rs, ei = xi * rs;
+  pr = fmaf(cs, er, fmaf(-sn, ei, pr));
+  pi = fmaf(cs, ei, fmaf(sn, er, pi));
+}
+
+template <bool CHECK = true>
+__device__ __forceinline__ void pair_helm(double tx, double ty, double tz, const double4 g0,
+                                          const double2 g1, const double4 s, double k, double kim,
+                                          double thr2, bool ck, double& pr, double& pi,
+                                          const double2* tab = nullptr) {
+  const double dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  const double rinv = (!CHECK || r2 >= thr2) ? rsqrt(r2) : 0.0;
+  const double r = r2 * rinv;
+  const double kr = k * r;
+  double sn, cs;
+  if (tab)
+    sincos_tab(kr, tab, sn, cs);
+  else
+    sincos(kr, &sn, &cs);
+  double rs = rinv;
+  if (ck) rs *= exp(-kim * r);
+  const double dn = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y));
+  const double q = dn * rinv * rinv;
+  const double wr = ck ? q * (1.0 + kim * r) : q;
+  const double wi = -q * kr;
+  const double er = fma(s.z, wr, fma(-s.w, wi, s.x)) * rs;
+  const double ei = fma(s.z, wi, fma(s.w, wr, s.y)) * rs;
+  pr = fma(cs, er, fma(-sn, ei, pr));
+  pi = fma(cs, ei, fma(sn, er, pi));
+}
+
+template <typename R, bool CHECK = true>
+__device__ __forceinline__ void pair_lap(R tx, R ty, R tz, const typename Vec<R>::T4 g0,
+                                         const typename Vec<R>::T2 g1,
+                                         const typename Vec<R>::T2 s, R thr2, R& p) {
+  const R dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  R rinv;
+  if constexpr (sizeof(R) == 4)
+    rinv = (!CHECK || r2 >= thr2) ? rsqrtf(r2) : R(0);
+  else
+    rinv = (!CHECK || r2 >= thr2) ? rsqrt(r2) : R(0);
+  const R dn = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y));
+  const R e = fma(s.y * dn, rinv * rinv, s.x);
+  p = fma(e, rinv, p);
+}
+
+}  // namespace
+}  // namespace dev
+}  // namespace bie

@@ -295,6 +295,8 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   BIE_CUDA(ab32_.alloc(size_t(nptso) * (cplx ? 4 : 2)));
   BIE_CUDA(dev::launch_source_consts(g, kp, 0, ab64_.p, st));
   BIE_CUDA(dev::launch_source_consts(g, kp, 1, ab32_.p, st));
+  BIE_CUDA(tc_err_.alloc(1));
+  BIE_CUDA(cudaMemsetAsync(tc_err_.p, 0, sizeof(int), st));
   for (auto& e : ev_) BIE_CUDA(cudaEventCreate(&e));
   // host vectors above are consumed by async copies: wait before they go
   BIE_CUDA(cudaStreamSynchronize(st));
@@ -323,6 +325,26 @@ double env_double(const char* name, double dflt) {
   return v && *v ? std::atof(v) : dflt;
 }
 }  // namespace
+
+int Plan::set_far_config(int precision, int nd, int variant, int nchunks) {
+  if ((precision != 0 && precision != 1) || nd < 1 || variant < 0 ||
+      variant >= dev::far_variants() || nchunks < 1 ||
+      nchunks > std::max<int64_t>(1, (nptso + dev::kFarTileSources - 1) / dev::kFarTileSources)) {
+    set_last_error("far configuration out of range");
+    return kErrArg;
+  }
+  FarConfig c;
+  c.variant = variant;
+  c.nchunks = nchunks;
+  far_cfg_[{precision, nd}] = c;
+  return ensure_workspace(precision, nd, nchunks);
+}
+
+int Plan::tc_error() const {
+  int v = 0;
+  if (tc_err_.p) cudaMemcpy(&v, tc_err_.p, sizeof(int), cudaMemcpyDeviceToHost);
+  return v;
+}
 
 Plan::FarConfig Plan::far_config(int precision, int nd) const {
   auto it = far_cfg_.find({precision, nd});
@@ -434,6 +456,7 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
   a.weff = precision == 1 ? (const void*)weff32_.p : (const void*)weff64_.p;
   a.weff_f32 = precision == 1;
   a.ab = precision == 1 ? (const void*)ab32_.p : (const void*)ab64_.p;
+  a.tc_err = tc_err_.p;
   if (timing) BIE_CUDA(cudaEventRecord(ev_[0], st));
   if (nd > 1)
     BIE_CUDA(dev::launch_oversample(g, kp, a, st));

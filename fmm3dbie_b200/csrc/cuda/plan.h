@@ -197,6 +197,11 @@ class Plan : public Operator {
     double ms = 0;
   };
   FarConfig far_config(int precision, int nd) const;
+  // Pins the far-field shape and chunk count of (precision, nd) instead of
+  // tuning it; variant as dev::far_variants().
+  int set_far_config(int precision, int nd, int variant, int nchunks);
+  // Nonzero once a tensor-core far-field launch timed out waiting for its MMAs.
+  int tc_error() const;
   const double* d_wts() const { return wts_.p; }
   // W_eff and the per-source (a, b) constants for precision 0 (f64) / 1 (f32)
   const void* weff_ptr(int precision) const {
@@ -222,6 +227,7 @@ class Plan : public Operator {
   DBuf<int64_t> cmoff_, row_ptr_, wofs_;
   DBuf<double> weff64_;
   DBuf<float> weff32_;
+  DBuf<int> tc_err_;  // timeout flag of the tensor-core far field
   DBuf<char> str_;
   DBuf<double> partial_;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};

@@ -70,6 +70,17 @@ class Plan:
         L.lib().bie_plan_info(self._h, L.ptr(info))
         return info
 
+    def set_far(self, iprec: int, nd: int, variant: int, nchunks: int):
+        """Pin the far-field shape of (iprec, nd) (variants 0-2 CUDA cores,
+        3-4 tensor cores for FP32 Helmholtz with nd >= 4)."""
+        L.check(L.lib().bie_plan_set_far(self._h, iprec, nd, variant, nchunks), "bie_plan_set_far")
+
+    def get_far(self, iprec: int, nd: int):
+        """(variant, nchunks, tensor-core timeout flag) of (iprec, nd)."""
+        out = np.zeros(3, np.int64)
+        L.check(L.lib().bie_plan_get_far(self._h, iprec, nd, L.ptr(out)), "bie_plan_get_far")
+        return tuple(int(v) for v in out)
+
     def close(self):
         if getattr(self, "_h", None):
             L.lib().bie_plan_destroy(self._h)

@@ -348,6 +348,14 @@ int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
  * strengths, far, combine (ms totals), calls for the f64 matvecs, then the
  * same four for the f32 matvecs. */
 int bie_plan_timing(void* plan, int64_t enable, double* times);
+/* Far-field shape of (iprec, nd): bie_plan_set_far pins it (variant 0-2:
+ * CUDA-core block shapes; 3-4: tensor-core kernel of the FP32 Helmholtz
+ * multi-density path, 16/32 or 64 densities per CTA, nd >= 4; nchunks source
+ * chunks) instead of the autotuner's choice; bie_plan_get_far returns the
+ * variant, the chunk count and a nonzero flag if a tensor-core launch timed
+ * out waiting for its MMAs.  No reference counterpart. */
+int bie_plan_set_far(void* plan, int64_t iprec, int64_t nd, int64_t variant, int64_t nchunks);
+int bie_plan_get_far(void* plan, int64_t iprec, int64_t nd, int64_t* out);
 
 /* ---- far field on device buffers ----------------------------------------- */
 /* The far-field sum that lfmm3d / hfmm3d compute inside lpcomp_*_addsub
