@@ -119,6 +119,7 @@ int far_variants();
 // Tensor-core far field (variants 3 and 4 of the multi-density FP32
 // Helmholtz path): densities per CTA, 0 where the variant does not apply.
 int far_tc_group(int variant, int nd, int precision, int kind);
+int far_tc_targets();  // targets per CTA
 // Launches it, or with occ != null reports its resident CTAs per SM.
 cudaError_t far_tc(int variant, const Geometry& g, const KParams& kp, const MatvecArgs& a,
                    cudaStream_t st, int* occ);

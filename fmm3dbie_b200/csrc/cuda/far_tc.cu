@@ -2,21 +2,26 @@
 //
 // For nd densities the far field is, per target t and density m,
 //   y(t, m) = sum_s K(t, s) sigma(s, m),
-// a product of the kernel matrix with the density matrix.  Each CTA takes 64
-// targets, one source chunk and N densities.  Per tile of 32 sources its 128
-// threads evaluate the 64 x 32 kernel values with the same FP32 pair function
-// and block centring as the CUDA-core kernels (so the error-matched W_eff32
-// fold still cancels their near-pair values) and lay the complex product out
-// as one real GEMM of M = 128 rows (real parts of the 64 targets, then their
-// imaginary parts) and K = 64 (source real parts, then imaginary parts):
-//   A = [[Kr, -Ki], [Ki, Kr]],  B = [sigma_r; sigma_i],  Y = A B.
-// Both operands are split into high and low parts (x = hi + lo, hi exact in
-// TF32) and one thread issues tcgen05.mma kind::tf32 for
-// hi*hi + hi*lo + lo*hi (the 3xTF32 scheme, about FP32 accuracy) into an
-// FP32 accumulator of N columns in tensor memory.  Every 4 tiles (128
-// sources, the tile length of the CUDA-core kernels) the accumulator is read
-// with tcgen05.ld and added into FP64 registers; the partial sums of the
-// chunk are written in the CUDA-core kernels' layout.  Operands sit in shared
+// a product of the kernel matrix with the density matrix.  Each CTA takes
+// 128 targets, one source chunk and N densities.  Per tile of 32 sources its
+// 512 threads evaluate the 128 x 32 kernel values with the same FP32 pair
+// function and block centring as the CUDA-core kernels (so the
+// error-matched W_eff32 fold still cancels their near-pair values) and lay
+// the complex product out as one real GEMM of M = 128 rows (targets),
+// K = 64 (kernel real parts, then imaginary parts) and 2N columns (the
+// densities' real parts, then their imaginary parts):
+//   A = [Kr | Ki],  B = [[sr, si], [-si, sr]],  Y = A B = [Re y | Im y].
+// Both operands are split into high and low parts (x = hi + lo, hi rounded
+// to TF32, lo rounded to TF32 as well) and one thread issues tcgen05.mma
+// kind::tf32 for hi*hi + hi*lo + lo*hi (the 3xTF32 scheme, about FP32
+// accuracy) into an FP32 accumulator of 2N columns in tensor memory, which
+// is read with tcgen05.ld after every tile and added into FP64 registers;
+// the partial sums of the chunk are written in the CUDA-core kernels'
+// layout.  While the tensor core works on a tile, the threads load the next
+// tile's sources and densities into registers.  (Double-buffering the kernel
+// values and the accumulator, so that a tile's kernel values are computed
+// while the previous tile's MMAs run, measured slower: the kernel-value
+// stage, not the tensor core, sets the pace.)  Operands sit in shared
 // memory in the canonical no-swizzle K-major layout (8-row x 16-byte core
 // matrices, row groups 128 B apart, K-direction core matrices (rows / 8) x
 // 128 B apart).  Completion waits are bounded; on timeout the kernel records
@@ -33,25 +38,24 @@ namespace bie {
 namespace dev {
 namespace {
 
-constexpr int kTcT = 64;                      // targets per CTA
-constexpr int kTcRows = 128;                  // accumulator rows
+constexpr int kTcT = 128;                     // targets per CTA = accumulator rows
+constexpr int kTcRows = kTcT;
 constexpr int kTcS = 32;                      // sources per tile
 constexpr int kTcK = 2 * kTcS;                // reduction length of a tile
-constexpr int kTcFlush = 1;                   // tiles per FP32 accumulation
-constexpr int kTcThreads = 256;
+constexpr int kTcThreads = 512;
 constexpr uint32_t kTcLboA = (kTcRows / 8) * 128;
 constexpr uint32_t kTcSbo = 128;
 constexpr uint32_t kTcWaitLimit = 1u << 24;
-static_assert(kFarTileSources % (kTcS * kTcFlush) == 0, "chunks are whole flush groups");
+static_assert(kFarTileSources % kTcS == 0, "chunks are whole tiles");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// High part of x exactly representable in TF32 (the low 13 mantissa bits
-// cleared); x - hi is exact, and the tensor core reads its TF32 part.
-__device__ __forceinline__ float tf32_hi(float x) {
-  return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+// x rounded to TF32 (10 mantissa bits, ties away from zero) by integer
+// operations: add half of the dropped range, clear the low 13 bits.
+__device__ __forceinline__ float tf32_rn(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 // Shared-memory matrix descriptor: no swizzle, K-major, sm_100 version bits.
@@ -78,13 +82,13 @@ __device__ __forceinline__ int op_off(int r, int k, uint32_t lbo) {
 }
 
 // Four consecutive columns of one row, split into high and low parts
-// (x = hi + lo exactly; the tensor core truncates lo to TF32, an error of at
-// most 2^-21 |x|).
+// (hi = x rounded to TF32, lo = x - hi, exact, then rounded to TF32).
 __device__ __forceinline__ void store_split(float* hi, float* lo, int off, float a, float b,
                                             float c, float d) {
-  const float ha = tf32_hi(a), hb = tf32_hi(b), hc = tf32_hi(c), hd = tf32_hi(d);
+  const float ha = tf32_rn(a), hb = tf32_rn(b), hc = tf32_rn(c), hd = tf32_rn(d);
   *reinterpret_cast<float4*>(hi + off) = make_float4(ha, hb, hc, hd);
-  *reinterpret_cast<float4*>(lo + off) = make_float4(a - ha, b - hb, c - hc, d - hd);
+  *reinterpret_cast<float4*>(lo + off) =
+      make_float4(tf32_rn(a - ha), tf32_rn(b - hb), tf32_rn(c - hc), tf32_rn(d - hd));
 }
 
 // Bounded wait for phase `parity` of the barrier (thread 0 polls, the others
@@ -172,13 +176,14 @@ __device__ __forceinline__ void tile_load(const Geometry& g, const float* __rest
 }
 
 template <int N, bool CK>
-__global__ void __launch_bounds__(kTcThreads, 2)
+__global__ void __launch_bounds__(kTcThreads, 1)
     far_tc_kernel(Geometry g, KParams kp, const float* __restrict__ ab,
                   const float* __restrict__ sig, int nd, double* __restrict__ partial,
                   int64_t chunk_len, int* __restrict__ err) {
-  constexpr int NH = N / 2;  // accumulator columns per thread (two warps per TMEM lane quarter)
-  constexpr uint32_t kLboB = (N / 8) * 128;
-  constexpr uint32_t kCols = N < 32 ? 32 : N;  // tensor-memory allocation (power of 2 >= 32)
+  constexpr int NB = 2 * N;  // GEMM columns: real parts, then imaginary parts
+  constexpr int NH = NB / 4;  // accumulator columns per thread (four warps per TMEM lane quarter)
+  constexpr uint32_t kLboB = (NB / 8) * 128;
+  constexpr uint32_t kCols = NB < 32 ? 32 : NB;  // tensor-memory allocation (power of 2 >= 32)
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_base;
@@ -190,7 +195,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
   float* sAh = reinterpret_cast<float*>(base);
   float* sAl = sAh + kTcRows * kTcK;
   float* sBh = sAl + kTcRows * kTcK;
-  float* sBl = sBh + N * kTcK;
+  float* sBl = sBh + NB * kTcK;
 
   const int64_t ntarg = g.ntarg, nptso = g.nptso;
   const int64_t tbase = int64_t(blockIdx.x) * kTcT;
@@ -200,13 +205,13 @@ __global__ void __launch_bounds__(kTcThreads, 2)
   const int64_t tcc = tcen < ntarg ? tcen : ntarg - 1;
   const double cx = g.tx[tcc], cy = g.ty[tcc], cz = g.tz[tcc];
   // kernel values: target t against sources 4 (4 j + sgrp) .. + 3, j = 0, 1
-  const int t = tid & (kTcT - 1), sgrp = tid >> 6;
+  const int t = tid & (kTcT - 1), sgrp = tid >> 7;
   const int64_t it = tbase + t;
   const int64_t ic = it < ntarg ? it : ntarg - 1;
   const float tx = float(g.tx[ic] - cx), ty = float(g.ty[ic] - cy), tz = float(g.tz[ic] - cz);
   const float thr2 = float(kp.thresh * kp.thresh);
   const float k = float(kp.kr), kim = float(kp.ki);
-  // accumulator: row 32 (warp % 4) + lane, columns c0 .. c0 + NH - 1
+  // accumulator: row (target) 32 (warp % 4) + lane, columns c0 .. c0 + NH - 1
   const int row = 32 * (warp & 3) + lane, c0 = (warp >> 2) * NH;
 
   if (warp == 0) {
@@ -250,7 +255,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
       ok = wait_phase(&bar, uint32_t(i - 1) & 1u);
       if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      if (i % kTcFlush == 0) flush<NH>(tmem, c0, acc);
+      flush<NH>(tmem, c0, acc);
     }
     // the prefetched tile -> shared memory
     if (tid < kTcS) {
@@ -265,7 +270,8 @@ __global__ void __launch_bounds__(kTcThreads, 2)
         sab[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
     }
-    // densities: B[n][s] = sigma_r(s, m0 + n), B[n][32 + s] = sigma_i(s, m0 + n)
+    // densities: column n (real part of density m0 + n) = [sr; -si], column
+    // N + n (imaginary part) = [si; sr], over sources s (rows s, 32 + s)
 #pragma unroll
     for (int kq = 0; kq < TileRegs<N>::kTasks; ++kq) {
       const int q = tid + kq * kTcThreads;
@@ -273,10 +279,13 @@ __global__ void __launch_bounds__(kTcThreads, 2)
         const int n = q % N, sq = 4 * (q / N);
         const float2* v = pre.sig[kq];
         store_split(sBh, sBl, op_off(n, sq, kLboB), v[0].x, v[1].x, v[2].x, v[3].x);
-        store_split(sBh, sBl, op_off(n, kTcS + sq, kLboB), v[0].y, v[1].y, v[2].y, v[3].y);
+        store_split(sBh, sBl, op_off(n, kTcS + sq, kLboB), -v[0].y, -v[1].y, -v[2].y, -v[3].y);
+        store_split(sBh, sBl, op_off(N + n, sq, kLboB), v[0].y, v[1].y, v[2].y, v[3].y);
+        store_split(sBh, sBl, op_off(N + n, kTcS + sq, kLboB), v[0].x, v[1].x, v[2].x, v[3].x);
       }
     }
     __syncthreads();
+    // kernel values of the tile: [Kr | Ki] for this thread's target
 #pragma unroll 1
     for (int j = 0; j < kTcS / 16; ++j) {
       const int sq = 4 * (4 * j + sgrp);
@@ -289,9 +298,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                   ki[u]);
       }
       store_split(sAh, sAl, op_off(t, sq, kTcLboA), kr[0], kr[1], kr[2], kr[3]);
-      store_split(sAh, sAl, op_off(t, kTcS + sq, kTcLboA), -ki[0], -ki[1], -ki[2], -ki[3]);
-      store_split(sAh, sAl, op_off(kTcT + t, sq, kTcLboA), ki[0], ki[1], ki[2], ki[3]);
-      store_split(sAh, sAl, op_off(kTcT + t, kTcS + sq, kTcLboA), kr[0], kr[1], kr[2], kr[3]);
+      store_split(sAh, sAl, op_off(t, kTcS + sq, kTcLboA), ki[0], ki[1], ki[2], ki[3]);
     }
     // make the operands visible to the tensor core, then one thread issues
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -299,8 +306,8 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (tid == 0) {
-      constexpr uint32_t idesc = idesc_tf32(kTcRows, N);
-      uint32_t accf = (i % kTcFlush == 0) ? 0u : 1u;
+      constexpr uint32_t idesc = idesc_tf32(kTcRows, NB);
+      uint32_t accf = 0u;
 #pragma unroll
       for (int p = 0; p < 3; ++p)
 #pragma unroll
@@ -335,14 +342,15 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     for (uint32_t r = 0; r < 4 && issued >= 0; ++r)
       if (wait_phase(&bar, uint32_t(issued) & 1u)) break;
   } else {
-    // row: real part (row < 64) or imaginary part of target tbase + (row & 63)
-    const int64_t to = tbase + (row & (kTcT - 1));
-    const int comp = row >> 6;
+    // row: target tbase + row; column c0 + n: real (< N) or imaginary part of
+    // density m0 + (c0 + n) % N
+    const int64_t to = tbase + row;
+    const int comp = c0 >= N ? 1 : 0, d0 = m0 + (c0 % N);
     if (to < ntarg)
 #pragma unroll
       for (int n = 0; n < NH; ++n)
-        if (m0 + c0 + n < nd)
-          partial[((size_t(blockIdx.y) * ntarg + to) * nd + m0 + c0 + n) * 2 + comp] = acc[n];
+        if (d0 + n < nd)
+          partial[((size_t(blockIdx.y) * ntarg + to) * nd + d0 + n) * 2 + comp] = acc[n];
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -352,7 +360,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
 
 template <int N>
 size_t tc_smem_bytes() {
-  return sizeof(float) * (2 * kTcRows * kTcK + 2 * N * kTcK) + 1024;
+  return sizeof(float) * (2 * kTcRows * kTcK + 2 * (2 * N) * kTcK) + 1024;
 }
 
 template <int N, bool CK>
@@ -383,6 +391,8 @@ cudaError_t far_tc_n(const Geometry& g, const KParams& kp, const MatvecArgs& a, 
 }
 
 }  // namespace
+
+int far_tc_targets() { return kTcT; }
 
 int far_tc_group(int variant, int nd, int precision, int kind) {
   if (variant < 3 || variant > 4 || precision != 1 || kind != 1 || nd < 4) return 0;

@@ -1517,7 +1517,7 @@ cudaError_t launch_source_consts(const Geometry& g, const KParams& kp, int preci
 int far_variants() { return 5; }
 
 int far_block_targets(int precision, int variant, int md, int nd) {
-  if (md && far_tc_group(variant, nd, precision, 1) > 0) return 64;
+  if (md && far_tc_group(variant, nd, precision, 1) > 0) return far_tc_targets();
   const int v = variant < 0 || variant > 2 ? 0 : variant;
   if (md) return kMdShapes[md_class(nd)][v][0] * kMdShapes[md_class(nd)][v][1];
   return precision == 1 ? kF32Shapes[v][0] * kF32Shapes[v][1]
