@@ -15,7 +15,8 @@
 // to TF32, lo rounded to TF32 as well) and one thread issues tcgen05.mma
 // kind::tf32 for hi*hi + hi*lo + lo*hi (the 3xTF32 scheme, about FP32
 // accuracy) into an FP32 accumulator of 2N columns in tensor memory, which
-// is read with tcgen05.ld after every tile and added into FP64 registers;
+// is read with tcgen05.ld after every tile and added into compensated
+// (Kahan) FP32 sums in registers;
 // the partial sums of the chunk are written in the CUDA-core kernels'
 // layout.  While the tensor core works on a tile, the threads load the next
 // tile's sources and densities into registers.  (Double-buffering the kernel
@@ -105,10 +106,20 @@ __device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t parity) {
   return __syncthreads_or(int(!done)) == 0;
 }
 
-// acc[n] += accumulator row 32 (w % 4) + lane, columns c0 .. c0 + NH - 1 (a
-// warp may read only the tensor-memory lanes of its quarter, w % 4).
+// Compensated (Kahan) FP32 sum s + v: the running error sits in c, so the
+// sum stays accurate to about FP32 rounding over the whole chunk without
+// FP32-to-FP64 conversions (which would load the XU pipe).
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+  const float y = v - c;
+  const float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+// (acc, cmp)[n] += accumulator row 32 (w % 4) + lane, columns c0 .. c0 + NH - 1
+// (a warp may read only the tensor-memory lanes of its quarter, w % 4).
 template <int NH>
-__device__ __forceinline__ void flush(uint32_t tmem, int c0, double* acc) {
+__device__ __forceinline__ void flush(uint32_t tmem, int c0, float* acc, float* cmp) {
   const int quarter = (threadIdx.x >> 5) & 3;
   const uint32_t lanes = uint32_t(quarter * 32) << 16;
   if constexpr (NH == 8) {
@@ -120,7 +131,7 @@ __device__ __forceinline__ void flush(uint32_t tmem, int c0, double* acc) {
         : "r"(tmem + lanes + uint32_t(c0)));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[j] += double(__uint_as_float(v[j]));
+    for (int j = 0; j < 8; ++j) kahan_add(acc[j], cmp[j], __uint_as_float(v[j]));
   } else {
 #pragma unroll
     for (int cc = 0; cc < NH; cc += 16) {
@@ -134,7 +145,7 @@ __device__ __forceinline__ void flush(uint32_t tmem, int c0, double* acc) {
           : "r"(tmem + lanes + uint32_t(c0 + cc)));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-      for (int j = 0; j < 16; ++j) acc[cc + j] += double(__uint_as_float(v[j]));
+      for (int j = 0; j < 16; ++j) kahan_add(acc[cc + j], cmp[cc + j], __uint_as_float(v[j]));
     }
   }
 }
@@ -234,9 +245,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint64_t desc_b[3] = {smem_desc(smem_u32(sBh), kLboB), smem_desc(smem_u32(sBl), kLboB),
                               smem_desc(smem_u32(sBh), kLboB)};
 
-  double acc[NH];
+  float acc[NH], cmp[NH];
 #pragma unroll
-  for (int n = 0; n < NH; ++n) acc[n] = 0.0;
+  for (int n = 0; n < NH; ++n) acc[n] = cmp[n] = 0.f;
   const int64_t s0 = int64_t(blockIdx.y) * chunk_len;
   const int64_t s1 = s0 + chunk_len < nptso ? s0 + chunk_len : nptso;
   const int ntiles = s1 > s0 ? int((s1 - s0 + kTcS - 1) / kTcS) : 0;
@@ -255,7 +266,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       ok = wait_phase(&bar, uint32_t(i - 1) & 1u);
       if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      flush<NH>(tmem, c0, acc);
+      flush<NH>(tmem, c0, acc, cmp);
     }
     // the prefetched tile -> shared memory
     if (tid < kTcS) {
@@ -334,7 +345,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (ok && ntiles > 0) {
     ok = wait_phase(&bar, uint32_t(ntiles - 1) & 1u);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ok) flush<NH>(tmem, c0, acc);
+    if (ok) flush<NH>(tmem, c0, acc, cmp);
   }
   if (!ok) {
     if (tid == 0 && err) atomicExch(err, 1 + int(blockIdx.x));
@@ -350,7 +361,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
       for (int n = 0; n < NH; ++n)
         if (d0 + n < nd)
-          partial[((size_t(blockIdx.y) * ntarg + to) * nd + d0 + n) * 2 + comp] = acc[n];
+          partial[((size_t(blockIdx.y) * ntarg + to) * nd + d0 + n) * 2 + comp] =
+              double(acc[n]) - double(cmp[n]);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
