@@ -295,6 +295,12 @@ def main():
                          "the (1,2,3) ellipsoid refined NREF times, order 6, and print its counters")
     ap.add_argument("--no-nearquad", action="store_true",
                     help="skip the near-quadrature generator comparison (host vs device)")
+    ap.add_argument("--tree-only", type=int, default=0, metavar="NREF",
+                    help="only compare the hierarchical and direct far fields on the (1,2,3) "
+                         "ellipsoid refined NREF times (order --tree-order)")
+    ap.add_argument("--tree-order", type=int, default=6)
+    ap.add_argument("--tree", type=int, default=0, metavar="NREF",
+                    help="add the hierarchical far-field leg on the ellipsoid refined NREF times")
     ap.add_argument("--uneven", action="store_true",
                     help="add the uneven batch leg (32 ellipsoids; ~2 min of CPU setup)")
     args = ap.parse_args()
@@ -304,6 +310,9 @@ def main():
         return matvec_only(args)
     if args.nearquad_only:
         return nearquad_only(args.nearquad_only)
+    if args.tree_only:
+        print(json.dumps({"tree": tree_leg(args.tree_only, args.tree_order)}))
+        return 0
 
     import torch
     import torch.distributed as dist
@@ -471,6 +480,10 @@ def main():
     if rank == 0 and world == 1 and args.torus:
         P.close()
         torus = torus_leg(dev)
+    tree = None
+    if rank == 0 and world == 1 and args.tree:
+        P.close()
+        tree = tree_leg(args.tree)
 
     if rank == 0:
         line = {
@@ -516,6 +529,7 @@ def main():
             "batched": batched,
             "uneven": uneven,
             "torus_warm_start": torus,
+            "tree": tree,
         }
         print(json.dumps(line), flush=True)
     P.close()
@@ -763,6 +777,89 @@ def matvec_only(args):
     t = P.timing(False)
     print(json.dumps({"matvec_prec": args.prec, "stage_ms": t}))
     return 0
+
+
+def tree_leg(nref, norder=6, solve=True):
+    """Hierarchical against direct far field on a large ellipsoid (1,2,3):
+    icosahedron refined nref times, order norder, Helmholtz k = 2 (zpars
+    (2, -2i, 1)), eps 1e-7, device setup.  Per precision: far-stage time of
+    one matvec (CUDA events) with each method, the tree's kernel
+    evaluations, and the tree matvec's weighted relative L2 difference from
+    the direct FP64 matvec; then the mixed-precision solve with each method
+    (the FP32 inner and FP64 outer matvecs both on the tree) and the
+    difference of the two solutions."""
+    import torch
+    from fmm3dbie_b200 import Plan
+    from fmm3dbie_b200 import surface as S
+    s = S.icosa_ellipsoid(nref, norder, (1.0, 2.0, 3.0))
+    t0 = time.time()
+    st = S.setup(s, 1, EPS, ZPARS)
+    t_setup = time.time() - t0
+    r = np.linalg.norm(s.xyz - X0, axis=1)
+    rhs = torch.tensor(np.exp(1j * ZK * r) / (4 * np.pi * r), device="cuda")
+    t0 = time.time()
+    P = Plan(1, ZPARS, s, st.near, st.over)
+    t_plan = time.time() - t0
+    w = torch.tensor(s.qwts(), device="cuda")
+
+    def rel(a, b):
+        return float(torch.sqrt((w * (a - b).abs() ** 2).sum() / (w * b.abs() ** 2).sum()))
+
+    def far_ms(prec, reps=3):
+        P.matvec(rhs, prec)
+        torch.cuda.synchronize()
+        P.timing(True)
+        for _ in range(reps):
+            P.matvec(rhs, prec)
+        torch.cuda.synchronize()
+        t = P.timing(False)
+        k = "f32" if prec == 1 else "f64"
+        return t[k]["far_ms"] / reps, (t[k]["strengths_ms"] + t[k]["combine_ms"]) / reps
+
+    out = {"workload": f"ellipsoid (1,2,3), {20 * 4 ** nref} order-{norder} patches, zk=2, "
+                       f"zpars=(2,-2i,1), eps=1e-7",
+           "npts": s.npts, "nptso": P.nptso, "pairs": float(s.npts) * P.nptso,
+           "setup_s": round(t_setup, 2), "plan_s": round(t_plan, 2)}
+    P.set_far_method(0, 0)
+    y_ref = P.matvec(rhs, 0)
+    for prec in (0, 1):
+        k = "f32" if prec == 1 else "f64"
+        P.set_far_method(prec, 0)
+        d_far, d_rest = far_ms(prec)
+        yd = P.matvec(rhs, prec)
+        t0 = time.time()
+        P.set_far_method(prec, 1)
+        t_build = time.time() - t0
+        info = P.get_far_method(prec)
+        t_far, t_rest = far_ms(prec)
+        yt = P.matvec(rhs, prec)
+        out[k] = {"direct_far_ms": d_far, "tree_far_ms": t_far, "other_stages_ms": t_rest,
+                  "speedup": d_far / t_far, "tree_build_s": round(t_build, 3),
+                  "tree_p": info["p"], "tree_theta": info["theta"],
+                  "tree_kernel_evals": info["kernel_evals"],
+                  "tree_updown_terms": info["updown_terms"],
+                  "evals_frac_of_direct": info["kernel_evals"] / (float(s.npts) * P.nptso),
+                  "forms_pp_pc_cp_cc": [int(info["pp"] + info["pp_check"]), int(info["pc"]),
+                                        int(info["cp"]), int(info["cc"])],
+                  "tree_vs_direct_f64": rel(yt, y_ref), "direct_vs_direct_f64": rel(yd, y_ref)}
+    if solve:
+        res = {}
+        for method in (0, 1):
+            P.set_far_method(0, method)
+            P.set_far_method(1, method)
+            P.solve(rhs, 0.5, mode=1, numit=200, eps_gmres=1e-7)  # warm (autotune)
+            torch.cuda.synchronize()
+            t0 = time.time()
+            x, inf = P.solve(rhs, 0.5, mode=1, numit=200, eps_gmres=1e-7)
+            torch.cuda.synchronize()
+            res[method] = (time.time() - t0, x, inf)
+        out["mixed_solve"] = {"direct_s": res[0][0], "tree_s": res[1][0],
+                              "speedup": res[0][0] / res[1][0],
+                              "tree_vs_direct_solution": rel(res[1][1], res[0][1]),
+                              "rres_direct": float(res[0][2]["rres"][0]),
+                              "rres_tree": float(res[1][2]["rres"][0])}
+    P.close()
+    return out
 
 
 def ctypes_double_pair(lib):

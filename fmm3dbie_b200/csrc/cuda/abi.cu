@@ -22,6 +22,7 @@
 #include "nearquad_gpu.h"
 #include "setup_gpu.h"
 #include "plan.h"
+#include "tree_far.h"
 
 using bie::cdouble;
 
@@ -1154,6 +1155,90 @@ int bie_plan_get_far(void* plan, int64_t iprec, int64_t nd, int64_t* out) {
   out[1] = c.nchunks;
   out[2] = P->tc_error();
   return BIE_OK;
+}
+
+int bie_plan_set_far_method(void* plan, int64_t iprec, int64_t method, double theta, int64_t p,
+                            void* stream) {
+  if (!plan || (iprec != 0 && iprec != 1) || (method != 0 && method != 1)) return BIE_ERR_ARG;
+  return guarded([&] {
+    bie::Plan& P = *static_cast<bie::Plan*>(plan);
+    bie::tree::Params prm = bie::Plan::default_tree_params(int(iprec), P.kp);
+    if (theta > 0.0) prm.theta = theta;
+    if (p > 0) prm.p = int(p);
+    return P.set_far_method(int(iprec), int(method), method == 1 ? &prm : nullptr,
+                            static_cast<cudaStream_t>(stream));
+  });
+}
+
+int bie_plan_get_far_method(void* plan, int64_t iprec, double* out) {
+  if (!plan || !out || (iprec != 0 && iprec != 1)) return BIE_ERR_ARG;
+  const bie::Plan& P = *static_cast<bie::Plan*>(plan);
+  for (int q = 0; q < 16; ++q) out[q] = 0.0;
+  out[0] = P.far_method(int(iprec));
+  const bie::TreeStats* s = P.tree_stats(int(iprec));
+  if (!s) return BIE_OK;
+  const bie::tree::Params prm = P.tree_params(int(iprec));
+  out[1] = prm.p;
+  out[2] = prm.theta;
+  out[3] = double(s->tnodes);
+  out[4] = double(s->snodes);
+  out[5] = double(s->leaves);
+  for (int q = 0; q < 5; ++q) out[6 + q] = double(s->interactions[q]);
+  out[11] = double(s->source_proxies);
+  out[12] = double(s->target_proxies);
+  out[13] = s->pair_evals;
+  out[14] = s->build_ms;
+  out[15] = s->up_evals + s->down_evals;
+  return BIE_OK;
+}
+
+int bie_tree_check(int64_t nt, const double* targ, int64_t ns, const double* src, double theta,
+                   int64_t p, double k, int64_t leaf_t, int64_t leaf_s, double* out) {
+  if (nt < 1 || ns < 1 || !targ || !src || !out || !(theta > 0.0 && theta < 1.0) || p < 1 ||
+      p > bie::tree::kMaxP || leaf_t < 1 || leaf_s < 1)
+    return BIE_ERR_ARG;
+  return guarded([&] {
+    std::vector<double> tx(nt), ty(nt), tz(nt), sx(ns), sy(ns), sz(ns);
+    for (int64_t i = 0; i < nt; ++i) {
+      tx[i] = targ[3 * i];
+      ty[i] = targ[3 * i + 1];
+      tz[i] = targ[3 * i + 2];
+    }
+    for (int64_t i = 0; i < ns; ++i) {
+      sx[i] = src[3 * i];
+      sy[i] = src[3 * i + 1];
+      sz[i] = src[3 * i + 2];
+    }
+    bie::tree::Params prm;
+    prm.theta = theta;
+    prm.p = int(p);
+    prm.k = k;
+    prm.leaf_t = int(leaf_t);
+    prm.leaf_s = int(leaf_s);
+    bie::tree::Tree T, S;
+    bie::tree::build_tree(nt, tx.data(), ty.data(), tz.data(), prm.leaf_t, T);
+    bie::tree::build_tree(ns, sx.data(), sy.data(), sz.data(), prm.leaf_s, S);
+    bie::tree::set_proxies(T, prm);
+    bie::tree::set_proxies(S, prm);
+    std::vector<bie::tree::Interaction> ia;
+    bie::tree::traverse(T, S, prm, 0.0, ia);
+    for (int q = 0; q < 10; ++q) out[q] = 0.0;
+    out[0] = bie::tree::check_coverage(T, S, ia);
+    out[1] = double(T.nodes.size());
+    out[2] = double(S.nodes.size());
+    double evals = 0.0;
+    for (const auto& x : ia) {
+      out[3 + x.kind] += 1.0;
+      const auto& a = T.nodes[x.t];
+      const auto& b = S.nodes[x.s];
+      const double nt_ = x.kind == bie::tree::kCP || x.kind == bie::tree::kCC ? a.nprox() : a.n();
+      const double ns_ = x.kind == bie::tree::kPC || x.kind == bie::tree::kCC ? b.nprox() : b.n();
+      evals += nt_ * ns_;
+    }
+    out[8] = evals;
+    out[9] = double(nt) * double(ns);
+    return int(bie::kOk);
+  });
 }
 
 int bie_plan_matvec(void* plan, int64_t iprec, int64_t nd, const double* sigma_dev,

@@ -51,6 +51,9 @@ struct Geometry {
   const double* tbox = nullptr;
   const double* sbox = nullptr;
   double box_margin2 = 0.0;
+  // FP32 coordinate centre per target (3 doubles) of the hierarchical far
+  // field; null for the direct far kernels (first target of each block)
+  const double* tcen = nullptr;
 };
 constexpr int kFarBlockTargets32 = 512;
 constexpr int kFarTileSources = 128;
@@ -85,6 +88,7 @@ struct MatvecArgs {
   int far_variant = 0;            // far-kernel block shape (see far_block_targets)
   const void* ab = nullptr;       // per-source constants for the multi-density kernel
   int* tc_err = nullptr;          // set by the tensor-core far field if a completion wait timed out
+  const int32_t* sdest = nullptr; // strengths: source s is stored at position sdest[s]
 };
 
 cudaError_t launch_strengths(const Geometry& g, const KParams& kp, const MatvecArgs& a,
@@ -97,6 +101,8 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
 // match32 = 0: exact FP64 kernel, weff is double* (may alias wnear);
 // match32 = 1: kernel values as the FP32 far kernel computes them
 // (same centring and pair functions), weff is float*.
+// match32 = 2: wnear is the FP64 W_eff; weff (float*) = wnear + exact part -
+// FP32-matched part (an FP32 W_eff for another far-field centring).
 cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp,
                         const double* wnear, void* weff, int match32, cudaStream_t st);
 cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t st);

@@ -39,7 +39,8 @@ constexpr double kOver4Pi = 0.07957747154594767;
 template <typename R, int CPLX>
 __device__ __forceinline__ void strengths_body(const Geometry& g, const KParams& kp,
                                                const double* __restrict__ sigma,
-                                               R* __restrict__ str, int nd, int p, double* sh) {
+                                               R* __restrict__ str, int nd, int p, double* sh,
+                                               const int32_t* __restrict__ sdest = nullptr) {
   const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
   const int os = g.ostart[p], nf = g.ostart[p + 1] - os;
   const double* M = g.imat + g.cmoff[g.pclass[p]];
@@ -60,7 +61,8 @@ __device__ __forceinline__ void strengths_body(const Geometry& g, const KParams&
       for (int j = 0; j < np; ++j) sr = fma(row[j], sh[j * nd + m], sr);
     }
     const double f = g.sw[os + l] * kOver4Pi;
-    const size_t o = size_t(os + l) * nd + m;
+    // sdest: the hierarchical far field keeps its sources in tree order
+    const size_t o = size_t(sdest ? sdest[os + l] : os + l) * nd + m;
     if (CPLX) {
       // c = alpha * sigma_over * f, d = beta * sigma_over * f
       str[4 * o + 0] = R((kp.ar * sr - kp.ai * si) * f);
@@ -76,9 +78,9 @@ __device__ __forceinline__ void strengths_body(const Geometry& g, const KParams&
 
 template <typename R, int CPLX>
 __global__ void strengths_kernel(Geometry g, KParams kp, const double* __restrict__ sigma,
-                                 R* __restrict__ str, int nd) {
+                                 R* __restrict__ str, int nd, const int32_t* __restrict__ sdest) {
   extern __shared__ double sh[];
-  strengths_body<R, CPLX>(g, kp, sigma, str, nd, blockIdx.x, sh);
+  strengths_body<R, CPLX>(g, kp, sigma, str, nd, blockIdx.x, sh, sdest);
 }
 
 // ---------------------------------------------------------------------------
@@ -643,6 +645,11 @@ __global__ void __launch_bounds__(kCombineThreads)
 // the FP32 far field's error on near pairs -- where n.(t-s) = O(r^2) cancels
 // in single precision -- is removed exactly by the subtraction; only the
 // well-separated pairs are then left to the FP32 far sum.
+// MATCH32 = 2: refold an FP32 W_eff from the FP64 one (wnear = W_eff f64):
+// out = W_eff64 + exact part - FP32-matched part.
+// The FP32 coordinates are centred as the FP32 far field centres them: on
+// the first target of the target's 512-target block, or on g.tcen[3 i ..]
+// (the leaf centre of the hierarchical far field) when that is set.
 // ---------------------------------------------------------------------------
 constexpr int kFarBlockTargetsF32 = 512;  // kFarThreads * kTptF32 (checked below)
 
@@ -670,13 +677,15 @@ __global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __res
   const int os = g.ostart[p], nf = g.ostart[p + 1] - os;
   const double* M = g.imat + g.cmoff[g.pclass[p]];
   const double thr2 = kp.thresh * kp.thresh;
-  // block centre of target i in the FP32 far kernel
+  // centre of target i's FP32 coordinates in the far field
   const int64_t tb = (i / kFarBlockTargetsF32) * kFarBlockTargetsF32;
-  const double cx = g.tx[tb], cy = g.ty[tb], cz = g.tz[tb];
+  const double cx = g.tcen ? g.tcen[3 * i] : g.tx[tb];
+  const double cy = g.tcen ? g.tcen[3 * i + 1] : g.ty[tb];
+  const double cz = g.tcen ? g.tcen[3 * i + 2] : g.tz[tb];
   const float tx32 = float(tx - cx), ty32 = float(ty - cy), tz32 = float(tz - cz);
   for (int l = lane; l < nf; l += 32) {
     const int s = os + l;
-    double vr = 0, vi = 0;
+    double vr = 0, vi = 0, fr = 0, fi = 0;
     if (MATCH32) {
       const float4 g0 = make_float4(float(g.sx[s] - cx), float(g.sy[s] - cy), float(g.sz[s] - cz),
                                     float(g.snx[s]));
@@ -698,9 +707,14 @@ __global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __res
         pair_lap<float>(tx32, ty32, tz32, g0, g1, make_float2(0.f, 1.f), thr2f, pd);
         vr = (kp.ar * pc + kp.br * pd) * f;
       }
-      a[2 * l] = vr;
-      a[2 * l + 1] = vi;
-      continue;
+      if (MATCH32 == 1) {
+        a[2 * l] = vr;
+        a[2 * l + 1] = vi;
+        continue;
+      }
+      fr = vr;
+      fi = vi;
+      vr = vi = 0;
     }
     const double dx = tx - g.sx[s], dy = ty - g.sy[s], dz = tz - g.sz[s];
     const double r2 = dx * dx + dy * dy + dz * dz;
@@ -723,6 +737,10 @@ __global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __res
       } else {
         vr = (kp.ar + kp.br * dn * rinv * rinv) * rinv * f;
       }
+    }
+    if (MATCH32 == 2) {
+      vr = fr - vr;
+      vi = fi - vi;
     }
     a[2 * l] = vr;
     a[2 * l + 1] = vi;
@@ -1042,18 +1060,18 @@ cudaError_t launch_strengths(const Geometry& g, const KParams& kp, const MatvecA
       cudaFuncSetAttribute(strengths_kernel<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
     }
     if (cplx)
-      strengths_kernel<float, 1><<<grid, block, sh, st>>>(g, kp, a.sigma, (float*)a.strengths, a.nd);
+      strengths_kernel<float, 1><<<grid, block, sh, st>>>(g, kp, a.sigma, (float*)a.strengths, a.nd, a.sdest);
     else
-      strengths_kernel<float, 0><<<grid, block, sh, st>>>(g, kp, a.sigma, (float*)a.strengths, a.nd);
+      strengths_kernel<float, 0><<<grid, block, sh, st>>>(g, kp, a.sigma, (float*)a.strengths, a.nd, a.sdest);
   } else {
     if (sh > 48 * 1024) {
       cudaFuncSetAttribute(strengths_kernel<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
       cudaFuncSetAttribute(strengths_kernel<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
     }
     if (cplx)
-      strengths_kernel<double, 1><<<grid, block, sh, st>>>(g, kp, a.sigma, (double*)a.strengths, a.nd);
+      strengths_kernel<double, 1><<<grid, block, sh, st>>>(g, kp, a.sigma, (double*)a.strengths, a.nd, a.sdest);
     else
-      strengths_kernel<double, 0><<<grid, block, sh, st>>>(g, kp, a.sigma, (double*)a.strengths, a.nd);
+      strengths_kernel<double, 0><<<grid, block, sh, st>>>(g, kp, a.sigma, (double*)a.strengths, a.nd, a.sdest);
   }
   count();
   return cudaGetLastError();
@@ -1587,12 +1605,16 @@ cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp, co
   if (sh > 48 * 1024) return cudaErrorInvalidValue;  // max_nf <= 289 keeps this <= 18.5 KB
   const dim3 grid(static_cast<unsigned>((nr.nnz + warps - 1) / warps)), block(32 * warps);
   if (kp.kind == 1) {
-    if (match32)
+    if (match32 == 2)
+      fold_kernel<1, 2, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
+    else if (match32)
       fold_kernel<1, 1, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
     else
       fold_kernel<1, 0, double><<<grid, block, sh, st>>>(g, nr, kp, wnear, (double*)weff);
   } else {
-    if (match32)
+    if (match32 == 2)
+      fold_kernel<0, 2, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
+    else if (match32)
       fold_kernel<0, 1, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
     else
       fold_kernel<0, 0, double><<<grid, block, sh, st>>>(g, nr, kp, wnear, (double*)weff);

@@ -108,6 +108,54 @@ __device__ __forceinline__ void pair_lap(R tx, R ty, R tz, const typename Vec<R>
   p = fma(e, rinv, p);
 }
 
+// Contribution of a charge q = (q.x, q.y) (complex for Helmholtz) at g0.xyz to
+// a well-separated target: q e^{ikr}/r (Laplace: q.x / r).  Used for the
+// proxy charges of the hierarchical far field, which carry no dipoles.
+template <int KIND>
+__device__ __forceinline__ void pair_charge(float tx, float ty, float tz, const float4 g0,
+                                            const float4 q, float k, float kim, bool ck, float& pr,
+                                            float& pi, const double2* = nullptr) {
+  const float dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float rinv = rsqrtf(r2);
+  if constexpr (KIND == 1) {
+    const float r = r2 * rinv;
+    float sn, cs;
+    __sincosf(k * r, &sn, &cs);
+    float rs = rinv;
+    if (ck) rs *= __expf(-kim * r);
+    const float er = q.x * rs, ei = q.y * rs;
+    pr = fmaf(cs, er, fmaf(-sn, ei, pr));
+    pi = fmaf(cs, ei, fmaf(sn, er, pi));
+  } else {
+    pr = fmaf(q.x, rinv, pr);
+  }
+}
+
+template <int KIND>
+__device__ __forceinline__ void pair_charge(double tx, double ty, double tz, const double4 g0,
+                                            const double4 q, double k, double kim, bool ck,
+                                            double& pr, double& pi, const double2* tab = nullptr) {
+  const double dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  const double rinv = rsqrt(r2);
+  if constexpr (KIND == 1) {
+    const double r = r2 * rinv;
+    double sn, cs;
+    if (tab)
+      sincos_tab(k * r, tab, sn, cs);
+    else
+      sincos(k * r, &sn, &cs);
+    double rs = rinv;
+    if (ck) rs *= exp(-kim * r);
+    const double er = q.x * rs, ei = q.y * rs;
+    pr = fma(cs, er, fma(-sn, ei, pr));
+    pi = fma(cs, ei, fma(sn, er, pi));
+  } else {
+    pr = fma(q.x, rinv, pr);
+  }
+}
+
 }  // namespace
 }  // namespace dev
 }  // namespace bie

@@ -12,6 +12,7 @@
 
 #include "../host/basis.h"
 #include "../host/setup.h"
+#include "tree_far.h"
 
 namespace bie {
 
@@ -61,6 +62,13 @@ AllocStreamScope::AllocStreamScope(cudaStream_t s) : prev(alloc_stream()) {
     }
   }
   alloc_stream() = s;
+}
+
+Plan::Plan() = default;
+
+Plan::~Plan() {
+  for (auto& e : ev_)
+    if (e) cudaEventDestroy(e);
 }
 
 int Plan::build(const PlanSpec& s, cudaStream_t st) {
@@ -227,6 +235,7 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   for (size_t b = 0; b + 5 < hsb.size(); b += 6)
     for (int c = 0; c < 3; ++c) ext = std::max(ext, std::fabs(hsb[b + c]) + std::fabs(hsb[b + 3 + c]));
   const double margin = kp.thresh + std::ldexp(ext, -12);
+  sep_min_ = margin;
   // ---- upload ----------------------------------------------------------------
   BIE_CUDA(upload(tx_, htx, st));
   BIE_CUDA(upload(ty_, hty, st));
@@ -300,6 +309,20 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   for (auto& e : ev_) BIE_CUDA(cudaEventCreate(&e));
   // host vectors above are consumed by async copies: wait before they go
   BIE_CUDA(cudaStreamSynchronize(st));
+  // far-field method by problem size
+  {
+    const char* fm = std::getenv("BIE_FAR_METHOD");
+    const std::string m = fm ? fm : "auto";
+    const char* tp = std::getenv("BIE_TREE_PAIRS");
+    const double pairs_min = tp && *tp ? std::atof(tp) : kTreeAutoPairs;
+    const bool tree = m == "tree" || (m == "auto" && double(ntarg) * double(nptso) >= pairs_min);
+    if (tree && ntarg > 0)
+      for (int prec = 0; prec < 2; ++prec) {
+        if (prec == 1 && !s.keep_f32) continue;
+        const int ier = set_far_method(prec, 1, nullptr, st);
+        if (ier) return ier;
+      }
+  }
   // as a solver operator: one segment of npts nodes
   nodes = npts;
   d_node_wts = wts_.p;
@@ -307,7 +330,83 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   return init_segments(st);
 }
 
-int Plan::nchunks_for(int precision, int nd) const { return far_config(precision, nd).nchunks; }
+int Plan::nchunks_for(int precision, int nd) const {
+  return far_method_[precision & 1] == 1 ? 1 : far_config(precision, nd).nchunks;
+}
+
+tree::Params Plan::default_tree_params(int precision, const dev::KParams& kp) {
+  tree::Params prm;
+  prm.theta = 0.5;
+  // p = 8 at theta 0.5: the FP64 matvec stays within about 5e-9 of the
+  // direct sum on the test surfaces (p = 10: 1e-10), below FP32 rounding
+  // for the FP32 matvec; Helmholtz grids grow with k times the side
+  prm.p = 8;
+  prm.k = kp.kind == 1 ? std::fabs(kp.kr) : 0.0;
+  prm.kscale = 1.0;
+  const char* e = std::getenv("BIE_TREE_P");
+  if (e && *e) prm.p = std::max(1, std::min(tree::kMaxP, std::atoi(e)));
+  e = std::getenv("BIE_TREE_THETA");
+  if (e && *e) prm.theta = std::atof(e);
+  return prm;
+}
+
+tree::Params Plan::tree_params(int precision) const {
+  const auto& t = tree_[precision & 1];
+  return t ? t->params() : default_tree_params(precision, kp);
+}
+
+const TreeStats* Plan::tree_stats(int precision) const {
+  const auto& t = tree_[precision & 1];
+  return t ? &t->stats() : nullptr;
+}
+
+int Plan::refold32(const double* tcen, cudaStream_t st) {
+  if (!weff32_.p) return kOk;
+  dev::Geometry gg = g;
+  gg.tcen = tcen;
+  BIE_CUDA(dev::launch_fold(gg, nr, kp, weff64_.p, weff32_.p, 2, st));
+  return kOk;
+}
+
+int Plan::set_far_method(int precision, int method, const tree::Params* prm, cudaStream_t st) {
+  if ((precision != 0 && precision != 1) || (method != 0 && method != 1)) {
+    set_last_error("far method: precision 0/1, method 0 (direct) or 1 (tree)");
+    return kErrArg;
+  }
+  if (precision == 1 && !weff32_.p) {
+    set_last_error("plan built without an f32 copy of W_eff");
+    return kErrArg;
+  }
+  if (method == 1) {
+    tree::Params p = prm ? *prm : default_tree_params(precision, kp);
+    if (!(p.theta > 0.0 && p.theta < 1.0) || p.p < 1 || p.p > tree::kMaxP || p.leaf_t < 1 ||
+        p.leaf_t > 128 || p.leaf_s < 1) {
+      set_last_error("tree parameters out of range (0 < theta < 1, 1 <= p <= 16, leaf_t <= 128)");
+      return kErrArg;
+    }
+    if (ntarg <= 0) {
+      set_last_error("tree far field needs targets");
+      return kErrArg;
+    }
+    auto t = std::make_unique<TreeFar>();
+    const int ier = t->build(g, p, sep_min_, st);
+    if (ier) return ier;
+    tree_[precision] = std::move(t);
+    if (precision == 1) {
+      const int e2 = refold32(tree_[1]->tcentre(), st);
+      if (e2) return e2;
+    }
+  } else {
+    if (precision == 1 && far_method_[1] == 1) {
+      const int e2 = refold32(nullptr, st);
+      if (e2) return e2;
+    }
+    tree_[precision].reset();
+  }
+  far_method_[precision] = method;
+  BIE_CUDA(cudaStreamSynchronize(st));
+  return kOk;
+}
 
 namespace {
 // Process-wide cache of tuned far-kernel shapes, keyed by everything the
@@ -441,6 +540,7 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
     set_last_error("plan built without an f32 copy of W_eff");
     return kErrArg;
   }
+  if (far_method_[precision & 1] == 1) return matvec_tree(precision, nd, d_sigma, d_pot, st);
   FarConfig fc = far_config(precision, nd);
   int ier = ensure_workspace(precision, nd, fc.nchunks);
   if (ier) return ier;
@@ -476,6 +576,43 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
     BIE_CUDA(cudaEventRecord(ev_[1], st));
   }
   BIE_CUDA(launch_far_stage(a, st));
+  if (timing) BIE_CUDA(cudaEventRecord(ev_[2], st));
+  BIE_CUDA(dev::launch_combine(g, nr, kp, a, st));
+  if (timing) {
+    BIE_CUDA(cudaEventRecord(ev_[3], st));
+    BIE_CUDA(cudaEventSynchronize(ev_[3]));
+    float t01, t12, t23;
+    cudaEventElapsedTime(&t01, ev_[0], ev_[1]);
+    cudaEventElapsedTime(&t12, ev_[1], ev_[2]);
+    cudaEventElapsedTime(&t23, ev_[2], ev_[3]);
+    times.strengths_ms[precision] += t01;
+    times.far_ms[precision] += t12;
+    times.combine_ms[precision] += t23;
+    times.calls[precision] += 1;
+  }
+  return kOk;
+}
+
+int Plan::matvec_tree(int precision, int nd, const double* d_sigma, double* d_pot,
+                      cudaStream_t st) {
+  TreeFar& T = *tree_[precision];
+  int ier = ensure_workspace(precision, nd, 1);
+  if (ier) return ier;
+  dev::MatvecArgs a;
+  a.precision = precision;
+  a.nd = nd;
+  a.nchunks = 1;
+  a.sigma = d_sigma;
+  a.pot = d_pot;
+  a.strengths = str_.p;
+  a.partial = partial_.p;
+  a.weff = precision == 1 ? (const void*)weff32_.p : (const void*)weff64_.p;
+  a.weff_f32 = precision == 1;
+  a.sdest = T.sdest();
+  if (timing) BIE_CUDA(cudaEventRecord(ev_[0], st));
+  BIE_CUDA(dev::launch_strengths(g, kp, a, st));
+  if (timing) BIE_CUDA(cudaEventRecord(ev_[1], st));
+  BIE_CUDA(T.run(precision, nd, kp, str_.p, partial_.p, st));
   if (timing) BIE_CUDA(cudaEventRecord(ev_[2], st));
   BIE_CUDA(dev::launch_combine(g, nr, kp, a, st));
   if (timing) {

@@ -11,9 +11,17 @@
 
 #include <cuda_runtime.h>
 
+#include "../host/tree.h"
 #include "device.cuh"
 
 namespace bie {
+
+class TreeFar;
+struct TreeStats;
+
+// Default problem size (targets x oversampled sources) from which a plan
+// uses the hierarchical far field.
+constexpr double kTreeAutoPairs = 1.5e10;
 
 using cdouble = std::complex<double>;
 
@@ -171,6 +179,10 @@ class Operator {
 
 class Plan : public Operator {
  public:
+  Plan();
+  ~Plan() override;
+  Plan(const Plan&) = delete;
+  Plan& operator=(const Plan&) = delete;
   int kind = 0;
   dev::KParams kp;
   dev::Geometry g;
@@ -202,6 +214,18 @@ class Plan : public Operator {
   int set_far_config(int precision, int nd, int variant, int nchunks);
   // Nonzero once a tensor-core far-field launch timed out waiting for its MMAs.
   int tc_error() const;
+  // Far-field method of a precision: 0 = direct sum over all pairs (the
+  // kernels above), 1 = hierarchical (dual-tree barycentric Lagrange
+  // interpolation, tree_far.h).  Chosen at build from the problem size
+  // (BIE_FAR_METHOD = direct | tree | auto, BIE_TREE_PAIRS the threshold on
+  // ntarg * nptso); set_far_method switches it and, for precision 1,
+  // refolds the FP32 W_eff for the new FP32 centring.  prm: tree
+  // parameters (null: defaults of the precision).
+  int set_far_method(int precision, int method, const tree::Params* prm, cudaStream_t st);
+  int far_method(int precision) const { return far_method_[precision & 1]; }
+  const TreeStats* tree_stats(int precision) const;
+  tree::Params tree_params(int precision) const;
+  static tree::Params default_tree_params(int precision, const dev::KParams& kp);
   const double* d_wts() const { return wts_.p; }
   // W_eff and the per-source (a, b) constants for precision 0 (f64) / 1 (f32)
   const void* weff_ptr(int precision) const {
@@ -217,6 +241,8 @@ class Plan : public Operator {
 
  private:
   int ensure_workspace(int precision, int nd, int nchunks);
+  int refold32(const double* tcen, cudaStream_t st);
+  int matvec_tree(int precision, int nd, const double* d_sigma, double* d_pot, cudaStream_t st);
   int tune_far(int precision, int nd, dev::MatvecArgs& a, cudaStream_t st, FarConfig& out);
   cudaError_t launch_far_stage(const dev::MatvecArgs& a, cudaStream_t st);
   DBuf<double> ab64_;
@@ -228,6 +254,9 @@ class Plan : public Operator {
   DBuf<double> weff64_;
   DBuf<float> weff32_;
   DBuf<int> tc_err_;  // timeout flag of the tensor-core far field
+  std::unique_ptr<TreeFar> tree_[2];
+  int far_method_[2] = {0, 0};
+  double sep_min_ = 0.0;  // accepted particle pairs closer than this keep the threshold test
   DBuf<char> str_;
   DBuf<double> partial_;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};

@@ -1,0 +1,221 @@
+// Cluster trees, proxy grids, dual traversal and the flattened interaction
+// lists of the hierarchical far field (see tree.h).
+#include "tree.h"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace bie {
+namespace tree {
+
+void cheb_nodes(int p, double* x, double* w) {
+  if (p <= 1) {
+    x[0] = 0.0;
+    w[0] = 1.0;
+    return;
+  }
+  for (int j = 0; j < p; ++j) x[j] = std::cos(M_PI * j / (p - 1));
+  for (int j = 0; j < p; ++j) {
+    double d = 1.0;
+    for (int i = 0; i < p; ++i)
+      if (i != j) d *= x[j] - x[i];
+    w[j] = 1.0 / d;
+  }
+}
+
+void build_tree(int64_t n, const double* x, const double* y, const double* z, int leaf, Tree& t) {
+  t.perm.resize(size_t(n));
+  std::iota(t.perm.begin(), t.perm.end(), int64_t(0));
+  t.nodes.clear();
+  Node root;
+  root.b = 0;
+  root.e = n;
+  t.nodes.push_back(root);
+  std::vector<int64_t> tmp(static_cast<size_t>(n));
+  std::vector<uint8_t> code(static_cast<size_t>(n));
+  const double* X[3] = {x, y, z};
+  // breadth-first: the children of a node are appended together
+  for (size_t i = 0; i < t.nodes.size(); ++i) {
+    Node nd = t.nodes[i];
+    const int64_t m = nd.n();
+    if (m > 0) {
+      for (int d = 0; d < 3; ++d) {
+        nd.lo[d] = 1e300;
+        nd.hi[d] = -1e300;
+      }
+      for (int64_t q = nd.b; q < nd.e; ++q)
+        for (int d = 0; d < 3; ++d) {
+          const double v = X[d][t.perm[q]];
+          nd.lo[d] = std::min(nd.lo[d], v);
+          nd.hi[d] = std::max(nd.hi[d], v);
+        }
+    }
+    double r2 = 0.0, emax = 0.0, ext[3];
+    for (int d = 0; d < 3; ++d) {
+      nd.c[d] = 0.5 * (nd.lo[d] + nd.hi[d]);
+      ext[d] = nd.hi[d] - nd.lo[d];
+      r2 += 0.25 * ext[d] * ext[d];
+      emax = std::max(emax, ext[d]);
+    }
+    nd.r = std::sqrt(r2);
+    if (m > leaf && emax > 0.0) {
+      int dims[3], nd_split = 0;
+      for (int d = 0; d < 3; ++d)
+        if (ext[d] > emax * M_SQRT1_2 || ext[d] == emax) dims[nd_split++] = d;
+      const int nb = 1 << nd_split;
+      int64_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int64_t q = nd.b; q < nd.e; ++q) {
+        int cc = 0;
+        for (int k = 0; k < nd_split; ++k)
+          cc |= (X[dims[k]][t.perm[q]] > nd.c[dims[k]] ? 1 : 0) << k;
+        code[q] = uint8_t(cc);
+        ++cnt[cc];
+      }
+      int64_t start[8], pos = nd.b;
+      for (int cc = 0; cc < nb; ++cc) {
+        start[cc] = pos;
+        pos += cnt[cc];
+      }
+      int64_t fill[8];
+      std::copy(start, start + 8, fill);
+      for (int64_t q = nd.b; q < nd.e; ++q) tmp[fill[code[q]]++] = t.perm[q];
+      std::copy(tmp.begin() + nd.b, tmp.begin() + nd.e, t.perm.begin() + nd.b);
+      nd.child0 = int(t.nodes.size());
+      for (int cc = 0; cc < nb; ++cc) {
+        if (cnt[cc] == 0) continue;
+        Node ch;
+        ch.b = start[cc];
+        ch.e = start[cc] + cnt[cc];
+        ch.parent = int(i);
+        ch.level = nd.level + 1;
+        t.nodes.push_back(ch);
+        ++nd.nchild;
+      }
+    }
+    t.nodes[i] = nd;
+  }
+}
+
+void set_proxies(Tree& t, const Params& prm) {
+  for (Node& nd : t.nodes) {
+    nd.np[0] = nd.np[1] = nd.np[2] = 0;
+    if (nd.n() <= 1) continue;
+    double ext[3], emax = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      ext[d] = nd.hi[d] - nd.lo[d];
+      emax = std::max(emax, ext[d]);
+    }
+    int np[3];
+    if (emax <= 0.0) {
+      np[0] = np[1] = np[2] = 1;  // coincident points: one proxy is exact
+    } else {
+      // Bernstein-ellipse parameter of a side for a singularity at distance
+      // r / theta from the centre: rho = a + sqrt(a^2 - 1), a = 2 D / side
+      const double D = nd.r / prm.theta;
+      auto rho = [&](double side) {
+        const double a = std::max(2.0 * D / side, 1.0 + 1e-12);
+        return a + std::sqrt(a * a - 1.0);
+      };
+      const double lmax = std::log(rho(emax));
+      for (int d = 0; d < 3; ++d) {
+        int pd = 1;
+        if (ext[d] > 1e-12 * emax) {
+          pd = int(std::ceil(prm.p * lmax / std::log(rho(ext[d])) - 1e-9));
+          pd += int(std::ceil(prm.kscale * prm.k * 0.5 * ext[d] - 1e-9));
+        }
+        np[d] = std::min(std::max(pd, 1), kMaxP);
+      }
+      while (np[0] * np[1] * np[2] > kMaxProxies) {
+        const int d = int(std::max_element(np, np + 3) - np);
+        --np[d];
+      }
+    }
+    if (int64_t(np[0]) * np[1] * np[2] >= nd.n()) continue;
+    for (int d = 0; d < 3; ++d) nd.np[d] = np[d];
+  }
+}
+
+void traverse(const Tree& T, const Tree& S, const Params& prm, double sep_min,
+              std::vector<Interaction>& out) {
+  out.clear();
+  if (T.nodes.empty() || S.nodes.empty() || T.nodes[0].n() == 0 || S.nodes[0].n() == 0) return;
+  std::vector<std::pair<int, int>> stack{{0, 0}};
+  while (!stack.empty()) {
+    const auto [a, b] = stack.back();
+    stack.pop_back();
+    const Node& t = T.nodes[a];
+    const Node& s = S.nodes[b];
+    double d2 = 0.0;
+    for (int d = 0; d < 3; ++d) d2 += (t.c[d] - s.c[d]) * (t.c[d] - s.c[d]);
+    const double D = std::sqrt(d2);
+    if (t.r + s.r < prm.theta * D) {
+      const double nt = double(t.n()), ns = double(s.n());
+      const double pt = t.nprox(), ps = s.nprox();
+      double best = nt * ns;
+      int kind = D - t.r - s.r > sep_min ? kPP : kPPCheck;
+      if (ps > 0 && nt * ps < best) {
+        best = nt * ps;
+        kind = kPC;
+      }
+      if (pt > 0 && pt * ns < best) {
+        best = pt * ns;
+        kind = kCP;
+      }
+      if (pt > 0 && ps > 0 && pt * ps < best) {
+        best = pt * ps;
+        kind = kCC;
+      }
+      out.push_back({a, b, kind});
+      continue;
+    }
+    const bool tleaf = t.nchild == 0, sleaf = s.nchild == 0;
+    if (tleaf && sleaf) {
+      out.push_back({a, b, kPPCheck});
+    } else if (sleaf || (!tleaf && t.r >= s.r)) {
+      for (int c = 0; c < t.nchild; ++c) stack.push_back({t.child0 + c, b});
+    } else {
+      for (int c = 0; c < s.nchild; ++c) stack.push_back({a, s.child0 + c});
+    }
+  }
+}
+
+namespace {
+void leaves_under(const Tree& t, int a, std::vector<int>& out) {
+  const Node& nd = t.nodes[a];
+  if (nd.nchild == 0) {
+    out.push_back(a);
+    return;
+  }
+  for (int c = 0; c < nd.nchild; ++c) leaves_under(t, nd.child0 + c, out);
+}
+}  // namespace
+
+int check_coverage(const Tree& T, const Tree& S, const std::vector<Interaction>& ia) {
+  std::vector<int> tl, sl;
+  leaves_under(T, 0, tl);
+  leaves_under(S, 0, sl);
+  std::vector<int> tid(T.nodes.size(), -1), sid(S.nodes.size(), -1);
+  for (size_t i = 0; i < tl.size(); ++i) tid[tl[i]] = int(i);
+  for (size_t i = 0; i < sl.size(); ++i) sid[sl[i]] = int(i);
+  std::vector<int> cnt(tl.size() * sl.size(), 0);
+  std::vector<int> a, b;
+  for (const auto& x : ia) {
+    a.clear();
+    b.clear();
+    leaves_under(T, x.t, a);
+    leaves_under(S, x.s, b);
+    for (int u : a)
+      for (int v : b) ++cnt[size_t(tid[u]) * sl.size() + sid[v]];
+  }
+  int bad = 0;
+  for (size_t i = 0; i < tl.size(); ++i)
+    for (size_t j = 0; j < sl.size(); ++j) {
+      const bool empty = T.nodes[tl[i]].n() == 0 || S.nodes[sl[j]].n() == 0;
+      if (!empty && cnt[i * sl.size() + j] != 1) ++bad;
+    }
+  return bad;
+}
+
+}  // namespace tree
+}  // namespace bie

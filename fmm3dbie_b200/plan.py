@@ -81,6 +81,23 @@ class Plan:
         L.check(L.lib().bie_plan_get_far(self._h, iprec, nd, L.ptr(out)), "bie_plan_get_far")
         return tuple(int(v) for v in out)
 
+    def set_far_method(self, iprec: int, method: int, theta: float = 0.0, p: int = 0):
+        """Far field of precision iprec: 0 direct sum, 1 hierarchical
+        (dual-tree barycentric Lagrange interpolation; theta, p: opening
+        angle and grid points per side, 0 = defaults)."""
+        L.check(L.lib().bie_plan_set_far_method(self._h, iprec, method, float(theta), int(p),
+                                                None), "bie_plan_set_far_method")
+
+    def get_far_method(self, iprec: int) -> dict:
+        """Method and tree statistics of precision iprec."""
+        out = np.zeros(16)
+        L.check(L.lib().bie_plan_get_far_method(self._h, iprec, L.ptr(out)),
+                "bie_plan_get_far_method")
+        keys = ["method", "p", "theta", "target_nodes", "source_nodes", "leaves", "pp_check",
+                "pp", "pc", "cp", "cc", "source_proxies", "target_proxies", "kernel_evals",
+                "build_ms", "updown_terms"]
+        return {k: float(v) for k, v in zip(keys, out)}
+
     def close(self):
         if getattr(self, "_h", None):
             L.lib().bie_plan_destroy(self._h)

@@ -356,6 +356,32 @@ int bie_plan_timing(void* plan, int64_t enable, double* times);
  * out waiting for its MMAs.  No reference counterpart. */
 int bie_plan_set_far(void* plan, int64_t iprec, int64_t nd, int64_t variant, int64_t nchunks);
 int bie_plan_get_far(void* plan, int64_t iprec, int64_t nd, int64_t* out);
+/* Far-field method of precision iprec, replacing the lfmm3d / hfmm3d calls
+ * of lpcomp_*_addsub (lap_comb_dir.f90:1094, helm_comb_dir.f:1117):
+ * method 0 = direct sum over all target-source pairs, 1 = hierarchical
+ * (dual-tree barycentric Lagrange interpolation on Chebyshev proxy grids;
+ * theta = opening angle of the acceptance test r_T + r_S < theta |c_T - c_S|,
+ * p = grid points along a cluster's longest side; theta <= 0 or p <= 0
+ * select the defaults, 0.5 and 8).  A plan picks method
+ * 1 by itself when ntarg * nptso >= 1.5e10 (BIE_FAR_METHOD = direct | tree |
+ * auto and BIE_TREE_PAIRS override).  Switching the FP32 method refolds
+ * the FP32 W_eff.  bie_plan_get_far_method: out[16] = method, p, theta,
+ * target nodes, source nodes, target leaves, interactions by form (PP with
+ * the self test, PP, PC, CP, CC), source proxies, target proxies, kernel
+ * evaluations per density, build ms, basis terms of the upward and downward
+ * passes per density (zeros after the method for method 0). */
+int bie_plan_set_far_method(void* plan, int64_t iprec, int64_t method, double theta, int64_t p,
+                            void* stream);
+int bie_plan_get_far_method(void* plan, int64_t iprec, double* out);
+/* Host-only check of the hierarchical far field's lists: builds the target
+ * tree (leaves <= leaf_t points) and source tree (<= leaf_s) of the points
+ * targ[3 nt] and src[3 ns] (xyz per point), the proxy grids for (theta, p,
+ * wavenumber k) and the dual traversal.  out[10] = number of (target leaf,
+ * source leaf) pairs not covered exactly once (0 when correct), target
+ * nodes, source nodes, interactions by form (5), kernel evaluations of the
+ * lists, ntarg * nsrc.  No GPU is used. */
+int bie_tree_check(int64_t nt, const double* targ, int64_t ns, const double* src, double theta,
+                   int64_t p, double k, int64_t leaf_t, int64_t leaf_s, double* out);
 
 /* ---- far field on device buffers ----------------------------------------- */
 /* The far-field sum that lfmm3d / hfmm3d compute inside lpcomp_*_addsub

@@ -1,0 +1,61 @@
+"""Host side of the hierarchical far field (no GPU): the cluster trees and
+the dual traversal cover every (target, source) pair exactly once, for
+point sets on a surface, in a volume, with coincident points and with a
+single point, and the lists cost far fewer kernel evaluations than the
+direct sum once the problem is large."""
+import numpy as np
+import pytest
+
+from fmm3dbie_b200 import _lib as L
+
+
+def _check(t, s, theta=0.5, p=8, k=0.0, leaf_t=128, leaf_s=256):
+    t = np.ascontiguousarray(t, float)
+    s = np.ascontiguousarray(s, float)
+    out = np.zeros(10)
+    st = L.lib().bie_tree_check(len(t), L.ptr(t), len(s), L.ptr(s), theta, p, k, leaf_t, leaf_s,
+                                L.ptr(out))
+    assert st == 0
+    return out
+
+
+def _ellipsoid(rng, n):
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    return v * np.array([1.0, 2.0, 3.0])
+
+
+@pytest.mark.parametrize("theta,p,k", [(0.5, 8, 0.0), (0.7, 4, 0.0), (0.5, 10, 5.0),
+                                       (0.3, 6, 0.0)])
+def test_coverage_surface(theta, p, k):
+    rng = np.random.default_rng(1)
+    out = _check(_ellipsoid(rng, 6000), _ellipsoid(rng, 9000), theta, p, k)
+    assert out[0] == 0
+    assert out[3:8].sum() > 0
+
+
+def test_coverage_volume_and_small_leaves():
+    rng = np.random.default_rng(2)
+    out = _check(rng.uniform(-1, 1, (4000, 3)), rng.uniform(-1, 1, (5000, 3)), 0.6, 4,
+                 leaf_t=16, leaf_s=16)
+    assert out[0] == 0
+    # every form appears with small grids and leaves
+    assert all(out[3 + q] > 0 for q in (2, 3, 4))
+
+
+def test_coincident_and_single_points():
+    rng = np.random.default_rng(3)
+    t = np.repeat(rng.uniform(-1, 1, (40, 3)), 3, axis=0)  # triples of coincident targets
+    s = np.repeat(rng.uniform(-1, 1, (60, 3)), 5, axis=0)
+    assert _check(t, s, 0.5, 4, leaf_t=8, leaf_s=8)[0] == 0
+    assert _check(np.zeros((1, 3)), np.ones((1, 3)))[0] == 0
+    assert _check(np.zeros((1, 3)), rng.uniform(-1, 1, (700, 3)), 0.5, 4, leaf_s=16)[0] == 0
+
+
+def test_lists_cheaper_than_direct():
+    rng = np.random.default_rng(4)
+    out = _check(_ellipsoid(rng, 150000), _ellipsoid(rng, 250000), 0.5, 8)
+    assert out[0] == 0
+    frac = out[8] / out[9]
+    print(f"\nkernel evaluations of the lists: {frac:.3f} of the direct sum")
+    assert frac < 0.3
