@@ -299,7 +299,7 @@ def main():
                     help="only compare the hierarchical and direct far fields on the (1,2,3) "
                          "ellipsoid refined NREF times (order --tree-order)")
     ap.add_argument("--tree-order", type=int, default=6)
-    ap.add_argument("--tree", type=int, default=0, metavar="NREF",
+    ap.add_argument("--tree", type=int, default=4, metavar="NREF",
                     help="add the hierarchical far-field leg on the ellipsoid refined NREF times")
     ap.add_argument("--uneven", action="store_true",
                     help="add the uneven batch leg (32 ellipsoids; ~2 min of CPU setup)")

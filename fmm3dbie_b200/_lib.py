@@ -121,7 +121,7 @@ _SIGS = {
     "bie_plan_timing": (C.c_int, [VP, I64, PDBL]),
     "bie_plan_set_far": (C.c_int, [VP, I64, I64, I64, I64]),
     "bie_plan_get_far": (C.c_int, [VP, I64, I64, PI64]),
-    "bie_plan_set_far_method": (C.c_int, [VP, I64, I64, DBL, I64, VP]),
+    "bie_plan_set_far_method": (C.c_int, [VP, I64, I64, DBL, I64, I64, I64, VP]),
     "bie_plan_get_far_method": (C.c_int, [VP, I64, PDBL]),
     "bie_tree_check": (C.c_int, [I64, PDBL, I64, PDBL, DBL, I64, DBL, I64, I64, PDBL]),
     "bie_farfield_dev": (C.c_int, [I64, PDBL, I64, VP, VP, VP, VP, I64, VP, DBL, I64, VP, VP]),

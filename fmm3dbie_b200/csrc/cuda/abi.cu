@@ -1158,13 +1158,15 @@ int bie_plan_get_far(void* plan, int64_t iprec, int64_t nd, int64_t* out) {
 }
 
 int bie_plan_set_far_method(void* plan, int64_t iprec, int64_t method, double theta, int64_t p,
-                            void* stream) {
+                            int64_t leaf_t, int64_t leaf_s, void* stream) {
   if (!plan || (iprec != 0 && iprec != 1) || (method != 0 && method != 1)) return BIE_ERR_ARG;
   return guarded([&] {
     bie::Plan& P = *static_cast<bie::Plan*>(plan);
     bie::tree::Params prm = bie::Plan::default_tree_params(int(iprec), P.kp);
     if (theta > 0.0) prm.theta = theta;
     if (p > 0) prm.p = int(p);
+    if (leaf_t > 0) prm.leaf_t = int(std::min<int64_t>(leaf_t, 1 << 20));
+    if (leaf_s > 0) prm.leaf_s = int(std::min<int64_t>(leaf_s, 1 << 20));
     return P.set_far_method(int(iprec), int(method), method == 1 ? &prm : nullptr,
                             static_cast<cudaStream_t>(stream));
   });

@@ -337,10 +337,11 @@ int Plan::nchunks_for(int precision, int nd) const {
 tree::Params Plan::default_tree_params(int precision, const dev::KParams& kp) {
   tree::Params prm;
   prm.theta = 0.5;
-  // p = 8 at theta 0.5: the FP64 matvec stays within about 5e-9 of the
-  // direct sum on the test surfaces (p = 10: 1e-10), below FP32 rounding
-  // for the FP32 matvec; Helmholtz grids grow with k times the side
-  prm.p = 8;
+  // theta 0.5: p = 10 keeps the FP64 matvec within about 1e-10 of the
+  // direct sum on the test surfaces (p = 8: 1e-7 .. 1e-6); for the FP32
+  // matvec p = 8 stays below the FP32 rounding of the proxy terms.
+  // Helmholtz grids grow with k times the side.
+  prm.p = precision == 1 ? 8 : 10;
   prm.k = kp.kind == 1 ? std::fabs(kp.kr) : 0.0;
   prm.kscale = 1.0;
   const char* e = std::getenv("BIE_TREE_P");

@@ -25,76 +25,78 @@ void cheb_nodes(int p, double* x, double* w) {
 }
 
 void build_tree(int64_t n, const double* x, const double* y, const double* z, int leaf, Tree& t) {
-  t.perm.resize(size_t(n));
-  std::iota(t.perm.begin(), t.perm.end(), int64_t(0));
+  // points with their original index, kept contiguous per node while the
+  // nodes of one level are split in parallel
+  struct Pt {
+    double v[3];
+    int64_t id;
+  };
+  std::vector<Pt> pts(static_cast<size_t>(n));
+  for (int64_t q = 0; q < n; ++q) pts[q] = {{x[q], y[q], z[q]}, q};
   t.nodes.clear();
   Node root;
   root.b = 0;
   root.e = n;
   t.nodes.push_back(root);
-  std::vector<int64_t> tmp(static_cast<size_t>(n));
-  std::vector<uint8_t> code(static_cast<size_t>(n));
-  const double* X[3] = {x, y, z};
-  // breadth-first: the children of a node are appended together
-  for (size_t i = 0; i < t.nodes.size(); ++i) {
-    Node nd = t.nodes[i];
-    const int64_t m = nd.n();
-    if (m > 0) {
+  size_t lev0 = 0, lev1 = 1;  // nodes of the current level
+  std::vector<int64_t> split;
+  while (lev0 < lev1) {
+    const int64_t cnt = int64_t(lev1 - lev0);
+    split.assign(static_cast<size_t>(cnt), 0);
+#pragma omp parallel for schedule(dynamic, 1) if (cnt > 1)
+    for (int64_t i = 0; i < cnt; ++i) {
+      Node& nd = t.nodes[lev0 + i];
+      const int64_t m = nd.n();
       for (int d = 0; d < 3; ++d) {
-        nd.lo[d] = 1e300;
-        nd.hi[d] = -1e300;
+        nd.lo[d] = m > 0 ? 1e300 : 0.0;
+        nd.hi[d] = m > 0 ? -1e300 : 0.0;
       }
       for (int64_t q = nd.b; q < nd.e; ++q)
         for (int d = 0; d < 3; ++d) {
-          const double v = X[d][t.perm[q]];
-          nd.lo[d] = std::min(nd.lo[d], v);
-          nd.hi[d] = std::max(nd.hi[d], v);
+          nd.lo[d] = std::min(nd.lo[d], pts[q].v[d]);
+          nd.hi[d] = std::max(nd.hi[d], pts[q].v[d]);
         }
-    }
-    double r2 = 0.0, emax = 0.0, ext[3];
-    for (int d = 0; d < 3; ++d) {
-      nd.c[d] = 0.5 * (nd.lo[d] + nd.hi[d]);
-      ext[d] = nd.hi[d] - nd.lo[d];
-      r2 += 0.25 * ext[d] * ext[d];
-      emax = std::max(emax, ext[d]);
-    }
-    nd.r = std::sqrt(r2);
-    if (m > leaf && emax > 0.0) {
-      int dims[3], nd_split = 0;
-      for (int d = 0; d < 3; ++d)
-        if (ext[d] > emax * M_SQRT1_2 || ext[d] == emax) dims[nd_split++] = d;
-      const int nb = 1 << nd_split;
-      int64_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      for (int64_t q = nd.b; q < nd.e; ++q) {
-        int cc = 0;
-        for (int k = 0; k < nd_split; ++k)
-          cc |= (X[dims[k]][t.perm[q]] > nd.c[dims[k]] ? 1 : 0) << k;
-        code[q] = uint8_t(cc);
-        ++cnt[cc];
+      double r2 = 0.0, ext[3];
+      for (int d = 0; d < 3; ++d) {
+        nd.c[d] = 0.5 * (nd.lo[d] + nd.hi[d]);
+        ext[d] = nd.hi[d] - nd.lo[d];
+        r2 += 0.25 * ext[d] * ext[d];
       }
-      int64_t start[8], pos = nd.b;
-      for (int cc = 0; cc < nb; ++cc) {
-        start[cc] = pos;
-        pos += cnt[cc];
+      nd.r = std::sqrt(r2);
+      const int d = ext[0] >= ext[1] ? (ext[0] >= ext[2] ? 0 : 2) : (ext[1] >= ext[2] ? 1 : 2);
+      if (m > leaf && ext[d] > 0.0) {
+        // two children split at a multiple of 32 points near the median
+        // along the longest side, so that leaves hold leaf/2 .. leaf points
+        // and fill whole warps
+        int64_t k = ((m / 2 + 16) / 32) * 32;
+        k = std::min<int64_t>(std::max<int64_t>(k, std::min<int64_t>(32, m - 1)), m - 1);
+        auto first = pts.begin() + nd.b;
+        std::nth_element(first, first + k, first + m,
+                         [d](const Pt& a, const Pt& b) { return a.v[d] < b.v[d]; });
+        split[i] = k;
       }
-      int64_t fill[8];
-      std::copy(start, start + 8, fill);
-      for (int64_t q = nd.b; q < nd.e; ++q) tmp[fill[code[q]]++] = t.perm[q];
-      std::copy(tmp.begin() + nd.b, tmp.begin() + nd.e, t.perm.begin() + nd.b);
-      nd.child0 = int(t.nodes.size());
-      for (int cc = 0; cc < nb; ++cc) {
-        if (cnt[cc] == 0) continue;
+    }
+    // children of this level, appended in order (siblings contiguous)
+    const size_t next0 = t.nodes.size();
+    for (int64_t i = 0; i < cnt; ++i) {
+      if (split[i] == 0) continue;
+      const size_t pi = lev0 + i;
+      t.nodes[pi].child0 = int(t.nodes.size());
+      t.nodes[pi].nchild = 2;
+      for (int cc = 0; cc < 2; ++cc) {
         Node ch;
-        ch.b = start[cc];
-        ch.e = start[cc] + cnt[cc];
-        ch.parent = int(i);
-        ch.level = nd.level + 1;
+        ch.b = cc == 0 ? t.nodes[pi].b : t.nodes[pi].b + split[i];
+        ch.e = cc == 0 ? t.nodes[pi].b + split[i] : t.nodes[pi].e;
+        ch.parent = int(pi);
+        ch.level = t.nodes[pi].level + 1;
         t.nodes.push_back(ch);
-        ++nd.nchild;
       }
     }
-    t.nodes[i] = nd;
+    lev0 = next0;
+    lev1 = t.nodes.size();
   }
+  t.perm.resize(static_cast<size_t>(n));
+  for (int64_t q = 0; q < n; ++q) t.perm[q] = pts[q].id;
 }
 
 void set_proxies(Tree& t, const Params& prm) {

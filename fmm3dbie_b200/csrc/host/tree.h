@@ -15,9 +15,11 @@
 //  * a target cluster T with a proxy grid x_k receives proxy potentials
 //    phi_k and passes them to its targets as u(t) += sum_k L_k(t) phi_k.
 //
-// Both trees split a node's tight bounding box at its midpoint along the
-// sides longer than 1/sqrt(2) of the longest side (2, 4 or 8 children), so
-// the clusters of points on a surface stay compact.  The dual traversal
+// Both trees are k-d trees: a node splits its points in two along the
+// longest side of its tight bounding box, at a multiple of 32 points near the
+// median, so that leaves hold between half and all of the leaf size and the
+// target leaves fill whole warps of the thread block that evaluates them.
+// The dual traversal
 // accepts a pair (T, S) when r_T + r_S < theta |c_T - c_S| and then picks
 // the cheapest of the four forms particle-particle (PP), particle-cluster
 // (PC: targets of T, proxies of S), cluster-particle (CP) and
@@ -61,7 +63,7 @@ struct Tree {
 };
 
 // Builds the tree of n points (leaves hold at most `leaf` points unless the
-// points coincide).
+// points coincide; siblings are contiguous, children follow their parents).
 void build_tree(int64_t n, const double* x, const double* y, const double* z, int leaf, Tree& t);
 
 // Chooses each node's proxy grid: along side d, np_d nodes such that the

@@ -81,12 +81,15 @@ class Plan:
         L.check(L.lib().bie_plan_get_far(self._h, iprec, nd, L.ptr(out)), "bie_plan_get_far")
         return tuple(int(v) for v in out)
 
-    def set_far_method(self, iprec: int, method: int, theta: float = 0.0, p: int = 0):
+    def set_far_method(self, iprec: int, method: int, theta: float = 0.0, p: int = 0,
+                       leaf_t: int = 0, leaf_s: int = 0):
         """Far field of precision iprec: 0 direct sum, 1 hierarchical
-        (dual-tree barycentric Lagrange interpolation; theta, p: opening
-        angle and grid points per side, 0 = defaults)."""
+        (dual-tree barycentric Lagrange interpolation; theta, p, leaf_t,
+        leaf_s: opening angle, grid points per side, targets / sources per
+        leaf; 0 = defaults)."""
         L.check(L.lib().bie_plan_set_far_method(self._h, iprec, method, float(theta), int(p),
-                                                None), "bie_plan_set_far_method")
+                                                int(leaf_t), int(leaf_s), None),
+                "bie_plan_set_far_method")
 
     def get_far_method(self, iprec: int) -> dict:
         """Method and tree statistics of precision iprec."""

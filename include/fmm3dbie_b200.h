@@ -361,8 +361,9 @@ int bie_plan_get_far(void* plan, int64_t iprec, int64_t nd, int64_t* out);
  * method 0 = direct sum over all target-source pairs, 1 = hierarchical
  * (dual-tree barycentric Lagrange interpolation on Chebyshev proxy grids;
  * theta = opening angle of the acceptance test r_T + r_S < theta |c_T - c_S|,
- * p = grid points along a cluster's longest side; theta <= 0 or p <= 0
- * select the defaults, 0.5 and 8).  A plan picks method
+ * p = grid points along a cluster's longest side, leaf_t / leaf_s = most
+ * targets (<= 128) / sources per leaf; values <= 0 select the defaults,
+ * theta 0.5, p 10 (FP64) / 8 (FP32), leaves 128 / 256).  A plan picks method
  * 1 by itself when ntarg * nptso >= 1.5e10 (BIE_FAR_METHOD = direct | tree |
  * auto and BIE_TREE_PAIRS override).  Switching the FP32 method refolds
  * the FP32 W_eff.  bie_plan_get_far_method: out[16] = method, p, theta,
@@ -371,7 +372,7 @@ int bie_plan_get_far(void* plan, int64_t iprec, int64_t nd, int64_t* out);
  * evaluations per density, build ms, basis terms of the upward and downward
  * passes per density (zeros after the method for method 0). */
 int bie_plan_set_far_method(void* plan, int64_t iprec, int64_t method, double theta, int64_t p,
-                            void* stream);
+                            int64_t leaf_t, int64_t leaf_s, void* stream);
 int bie_plan_get_far_method(void* plan, int64_t iprec, double* out);
 /* Host-only check of the hierarchical far field's lists: builds the target
  * tree (leaves <= leaf_t points) and source tree (<= leaf_s) of the points
