@@ -67,7 +67,8 @@ def test_tree_matches_direct_fp64(plan, theta, p, tol, nd):
     assert err < tol
 
 
-@pytest.mark.parametrize("theta,p,leaf,tol", [(0.6, 4, 32, 2e-2), (0.5, 8, 64, 1e-5)])
+@pytest.mark.parametrize("theta,p,leaf,tol",
+                         [(0.6, 2, 16, 0.5), (0.6, 4, 32, 2e-2), (0.5, 8, 64, 1e-5)])
 def test_tree_small_leaves(plan, theta, p, leaf, tol):
     """Small leaves: many CP and CC interactions and proxy-target items."""
     kind, P, s, w = plan
@@ -88,7 +89,7 @@ def test_tree_forms_exercised(plan):
     """The accuracy cases above include lists with every interaction form."""
     kind, P, s, w = plan
     seen = {"pp": 0, "pc": 0, "cp": 0, "cc": 0}
-    for theta, p, leaf in ((0.7, 4, 0), (0.8, 2, 0), (0.6, 4, 32)):
+    for theta, p, leaf in ((0.7, 4, 0), (0.6, 4, 32), (0.6, 2, 16)):
         P.set_far_method(0, 1, theta, p, leaf, leaf)
         info = P.get_far_method(0)
         for f in seen:
