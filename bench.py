@@ -803,7 +803,8 @@ def tree_leg(nref, norder=6, solve=True):
     w = torch.tensor(s.qwts(), device="cuda")
 
     def rel(a, b):
-        return float(torch.sqrt((w * (a - b).abs() ** 2).sum() / (w * b.abs() ** 2).sum()))
+        ww = w if a.dim() == 1 else w[:, None]
+        return float(torch.sqrt((ww * (a - b).abs() ** 2).sum() / (ww * b.abs() ** 2).sum()))
 
     def far_ms(prec, reps=3):
         P.matvec(rhs, prec)
@@ -842,6 +843,22 @@ def tree_leg(nref, norder=6, solve=True):
                   "forms_pp_pc_cp_cc": [int(info["pp"] + info["pp_check"]), int(info["pc"]),
                                         int(info["cp"]), int(info["cc"])],
                   "tree_vs_direct_f64": rel(yt, y_ref), "direct_vs_direct_f64": rel(yd, y_ref)}
+    # 16 densities at once (FP32): the direct multi-density kernels (their
+    # autotuned shape) against the multi-density tree kernel
+    nd = 16
+    xm = (rhs[:, None] * torch.arange(1, nd + 1, device="cuda")).contiguous()
+    md = {}
+    for method in (0, 1):
+        P.set_far_method(1, method)
+        ym = P.matvec(xm, 1)
+        torch.cuda.synchronize()
+        P.timing(True)
+        P.matvec(xm, 1)
+        torch.cuda.synchronize()
+        md[method] = (P.timing(False)["f32"]["far_ms"], ym)
+    out["f32_nd16"] = {"direct_far_ms": md[0][0], "tree_far_ms": md[1][0],
+                       "speedup": md[0][0] / md[1][0],
+                       "tree_vs_direct": rel(md[1][1], md[0][1])}
     if solve:
         res = {}
         for method in (0, 1):

@@ -108,6 +108,75 @@ __device__ __forceinline__ void pair_lap(R tx, R ty, R tz, const typename Vec<R>
   p = fma(e, rinv, p);
 }
 
+// Unit responses of one source at one target, for evaluating several
+// densities from one kernel evaluation: G = e^{ikr}/r and D = G u (1 - ikr)
+// with u = n.(t-s)/r^2 (complex k = kr + i kim: 1 - ikr becomes
+// (1 + kim r) - i kr r); a source with charge c and dipole strength d then
+// contributes c G + d D, as pair_helm computes it.  Laplace: G = 1/r,
+// D = u/r.  CHECK = false drops the threshold test (as in pair_helm).
+template <bool CHECK = true>
+__device__ __forceinline__ void pair_helm_unit(float tx, float ty, float tz, const float4 g0,
+                                               const float2 g1, float k, float kim, float thr2,
+                                               bool ck, float& gr, float& gi, float& dr,
+                                               float& di, const double2* = nullptr) {
+  const float dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float rinv = (!CHECK || r2 >= thr2) ? rsqrtf(r2) : 0.0f;
+  const float r = r2 * rinv;
+  const float kr = k * r;
+  float sn, cs;
+  __sincosf(kr, &sn, &cs);
+  float rs = rinv;
+  if (ck) rs *= __expf(-kim * r);
+  gr = cs * rs;
+  gi = sn * rs;
+  const float u = fmaf(dx, g0.w, fmaf(dy, g1.x, dz * g1.y)) * (rinv * rinv);
+  const float fr = ck ? u * (1.0f + kim * r) : u, fi = -u * kr;
+  dr = fmaf(gr, fr, -gi * fi);
+  di = fmaf(gr, fi, gi * fr);
+}
+
+template <bool CHECK = true>
+__device__ __forceinline__ void pair_helm_unit(double tx, double ty, double tz, const double4 g0,
+                                               const double2 g1, double k, double kim,
+                                               double thr2, bool ck, double& gr, double& gi,
+                                               double& dr, double& di,
+                                               const double2* tab = nullptr) {
+  const double dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  const double rinv = (!CHECK || r2 >= thr2) ? rsqrt(r2) : 0.0;
+  const double r = r2 * rinv;
+  const double kr = k * r;
+  double sn, cs;
+  if (tab)
+    sincos_tab(kr, tab, sn, cs);
+  else
+    sincos(kr, &sn, &cs);
+  double rs = rinv;
+  if (ck) rs *= exp(-kim * r);
+  gr = cs * rs;
+  gi = sn * rs;
+  const double u = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y)) * (rinv * rinv);
+  const double fr = ck ? u * (1.0 + kim * r) : u, fi = -u * kr;
+  dr = fma(gr, fr, -gi * fi);
+  di = fma(gr, fi, gi * fr);
+}
+
+template <typename R, bool CHECK = true>
+__device__ __forceinline__ void pair_lap_unit(R tx, R ty, R tz, const typename Vec<R>::T4 g0,
+                                              const typename Vec<R>::T2 g1, R thr2, R& g, R& dd) {
+  const R dx = tx - g0.x, dy = ty - g0.y, dz = tz - g0.z;
+  const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  R rinv;
+  if constexpr (sizeof(R) == 4)
+    rinv = (!CHECK || r2 >= thr2) ? rsqrtf(r2) : R(0);
+  else
+    rinv = (!CHECK || r2 >= thr2) ? rsqrt(r2) : R(0);
+  const R dn = fma(dx, g0.w, fma(dy, g1.x, dz * g1.y));
+  g = rinv;
+  dd = dn * rinv * rinv * rinv;
+}
+
 // Contribution of a charge q = (q.x, q.y) (complex for Helmholtz) at g0.xyz to
 // a well-separated target: q e^{ikr}/r (Laplace: q.x / r).  Used for the
 // proxy charges of the hierarchical far field, which carry no dipoles.

@@ -426,6 +426,254 @@ __global__ void __launch_bounds__(kEvThreads)
   }
 }
 
+// Several densities per block (MD of them, densities m0 .. m0 + MD - 1 on
+// grid y): each pair's unit responses G and D (pair_helm_unit) are computed
+// once and applied to every density's charge and dipole strengths; proxy
+// charges use G alone.  Otherwise as tree_eval_kernel.
+constexpr int kMdTile = 64;
+
+template <int KIND, typename R, bool CK, bool PROXYT, int MD>
+__global__ void __launch_bounds__(kEvThreads)
+    tree_eval_md_kernel(TreeArgs ta, KParams kp, const R* __restrict__ str,
+                        const R* __restrict__ qhat, R* __restrict__ phi,
+                        double* __restrict__ partial, int nd) {
+  using R2 = typename Vec<R>::T2;
+  using R4 = typename Vec<R>::T4;
+  constexpr int SW = KIND == 1 ? 4 : 2;
+  constexpr int C = KIND == 1 ? 2 : 1;
+  constexpr bool F32 = sizeof(R) == 4;
+  __shared__ R4 sg0[kMdTile];
+  __shared__ R2 sg1[kMdTile];
+  // the source strengths of the list phase and the proxy potentials of the
+  // downward phase share one buffer
+  constexpr size_t kSstBytes = sizeof(R) * kMdTile * MD * SW;
+  constexpr size_t kPhiBytes = PROXYT ? 0 : sizeof(R2) * tree::kMaxProxies;
+  __shared__ __align__(16) unsigned char sbuf[kSstBytes > kPhiBytes ? kSstBytes : kPhiBytes];
+  R(*sst)[MD][SW] = reinterpret_cast<R(*)[MD][SW]>(sbuf);
+  R2* sphi = reinterpret_cast<R2*>(sbuf);
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  const double2* tab = nullptr;
+  if constexpr (sizeof(R) == 8 && KIND == 1) {
+    fill_trig_table(stab);  // published by the first __syncthreads below
+    tab = stab;
+  }
+  const int tid = threadIdx.x;
+  const int m0 = blockIdx.y * MD;
+  const int nm = min(MD, nd - m0);
+  int node;
+  int64_t k0 = 0;
+  if constexpr (PROXYT) {
+    const int2 pi = ta.pitems[blockIdx.x];
+    node = pi.x;
+    k0 = pi.y;
+  } else {
+    node = ta.leaves[blockIdx.x];
+  }
+  const TNodeD tn = ta.tn[node];
+  const double cx = 0.5 * (tn.lo[0] + tn.hi[0]), cy = 0.5 * (tn.lo[1] + tn.hi[1]),
+               cz = 0.5 * (tn.lo[2] + tn.hi[2]);
+  bool act, wact;
+  double x = cx, y = cy, z = cz;
+  if constexpr (PROXYT) {
+    const int64_t P = int64_t(tn.np0) * tn.np1 * tn.np2;
+    act = k0 + tid < P;
+    wact = k0 + (tid & ~31) < P;
+    if (act) {
+      const int64_t q = tn.tpoff + k0 + tid;
+      x = ta.tpx[q];
+      y = ta.tpy[q];
+      z = ta.tpz[q];
+    }
+  } else {
+    act = tn.b + tid < tn.e;
+    wact = tn.b + (tid & ~31) < tn.e;
+    if (act) {
+      const int64_t q = tn.b + tid;
+      x = ta.tx[q];
+      y = ta.ty[q];
+      z = ta.tz[q];
+    }
+  }
+  const R tx = R(x - cx), ty = R(y - cy), tz = R(z - cz);
+  const R thr2 = R(kp.thresh * kp.thresh), k = R(kp.kr), kim = R(kp.ki);
+  double accr[MD], acci[MD];
+#pragma unroll
+  for (int mm = 0; mm < MD; ++mm) accr[mm] = acci[mm] = 0.0;
+  int n = node;
+  int64_t e0 = PROXYT ? tn.ce0 : tn.pe0, e1 = PROXYT ? tn.ce1 : tn.pe1;
+  const EntryD* ents = PROXYT ? ta.cent : ta.pent;
+  while (true) {
+    for (int64_t q = e0; q < e1; ++q) {
+      const EntryD en = ents[q];
+      for (int sb = en.b; sb < en.e; sb += kMdTile) {
+        const int ns = min(kMdTile, en.e - sb);
+        __syncthreads();
+        for (int qq = tid; qq < ns; qq += kEvThreads) {
+          const int s = sb + qq;
+          if (en.kind == 2) {
+            sg0[qq] = R4{R(ta.spx[s] - cx), R(ta.spy[s] - cy), R(ta.spz[s] - cz), R(0)};
+          } else {
+            sg0[qq] = R4{R(ta.sx[s] - cx), R(ta.sy[s] - cy), R(ta.sz[s] - cz), R(ta.snx[s])};
+            sg1[qq] = R2{R(ta.sny[s]), R(ta.snz[s])};
+          }
+        }
+        for (int qq = tid; qq < ns * MD * SW; qq += kEvThreads) {
+          const int sj = qq / (MD * SW), rem = qq - sj * (MD * SW);
+          const int mm = rem / SW, c = rem - mm * SW;
+          R v = R(0);
+          if (mm < nm) {
+            if (en.kind == 2) {
+              if (c < C) v = qhat[(size_t(sb + sj) * nd + m0 + mm) * C + c];
+            } else {
+              v = str[(size_t(sb + sj) * nd + m0 + mm) * SW + c];
+            }
+          }
+          sst[sj][mm][c] = v;
+        }
+        __syncthreads();
+        if (!wact) continue;  // a warp without targets only helps load the tiles
+        R tr[MD], ti[MD];
+#pragma unroll
+        for (int mm = 0; mm < MD; ++mm) tr[mm] = ti[mm] = R(0);
+        if (en.kind == 2) {
+          for (int j = 0; j < ns; ++j) {
+            R gr = R(0), gi = R(0);
+            pair_charge<KIND>(tx, ty, tz, sg0[j], R4{R(1), R(0), R(0), R(0)}, k, kim, CK, gr, gi, tab);
+#pragma unroll
+            for (int mm = 0; mm < MD; ++mm) {
+              const R qr = sst[j][mm][0];
+              if constexpr (KIND == 1) {
+                const R qi = sst[j][mm][1];
+                tr[mm] = fma(qr, gr, fma(-qi, gi, tr[mm]));
+                ti[mm] = fma(qr, gi, fma(qi, gr, ti[mm]));
+              } else {
+                tr[mm] = fma(qr, gr, tr[mm]);
+              }
+            }
+          }
+        } else {
+          const bool chk = en.kind == 0;
+          for (int j = 0; j < ns; ++j) {
+            if constexpr (KIND == 1) {
+              R gr, gi, dr, di;
+              if (chk)
+                pair_helm_unit<true>(tx, ty, tz, sg0[j], sg1[j], k, kim, thr2, CK, gr, gi, dr, di, tab);
+              else
+                pair_helm_unit<false>(tx, ty, tz, sg0[j], sg1[j], k, kim, thr2, CK, gr, gi, dr, di, tab);
+#pragma unroll
+              for (int mm = 0; mm < MD; ++mm) {
+                const R4 sv = *reinterpret_cast<const R4*>(sst[j][mm]);
+                tr[mm] = fma(sv.x, gr, fma(-sv.y, gi, fma(sv.z, dr, fma(-sv.w, di, tr[mm]))));
+                ti[mm] = fma(sv.x, gi, fma(sv.y, gr, fma(sv.z, di, fma(sv.w, dr, ti[mm]))));
+              }
+            } else {
+              R g, dd;
+              if (chk)
+                pair_lap_unit<R, true>(tx, ty, tz, sg0[j], sg1[j], thr2, g, dd);
+              else
+                pair_lap_unit<R, false>(tx, ty, tz, sg0[j], sg1[j], thr2, g, dd);
+#pragma unroll
+              for (int mm = 0; mm < MD; ++mm)
+                tr[mm] = fma(sst[j][mm][0], g, fma(sst[j][mm][1], dd, tr[mm]));
+            }
+          }
+        }
+#pragma unroll
+        for (int mm = 0; mm < MD; ++mm) {
+          accr[mm] += double(tr[mm]);
+          acci[mm] += double(ti[mm]);
+        }
+      }
+    }
+    if (PROXYT) break;
+    n = ta.tn[n].parent;
+    if (n < 0) break;
+    e0 = ta.tn[n].pe0;
+    e1 = ta.tn[n].pe1;
+  }
+  (void)F32;
+  if constexpr (!PROXYT) {
+    for (int a = node; a >= 0; a = ta.tn[a].parent) {
+      const TNodeD an = ta.tn[a];
+      if (an.tpoff < 0) continue;
+      const int P = an.np0 * an.np1 * an.np2;
+      R Lx[kP], Ly[kP], Lz[kP];
+      {
+        const double h0 = 0.5 * (an.hi[0] - an.lo[0]), h1 = 0.5 * (an.hi[1] - an.lo[1]),
+                     h2 = 0.5 * (an.hi[2] - an.lo[2]);
+        const R u0 = h0 > 0.0 ? R((x - 0.5 * (an.lo[0] + an.hi[0])) / h0) : R(0);
+        const R u1 = h1 > 0.0 ? R((y - 0.5 * (an.lo[1] + an.hi[1])) / h1) : R(0);
+        const R u2 = h2 > 0.0 ? R((z - 0.5 * (an.lo[2] + an.hi[2])) / h2) : R(0);
+        lagrange(an.np0, u0, Lx);
+        lagrange(an.np1, u1, Ly);
+        lagrange(an.np2, u2, Lz);
+      }
+      for (int mm = 0; mm < nm; ++mm) {
+        __syncthreads();
+        for (int q = tid; q < P; q += kEvThreads) {
+          const R* pp = phi + (size_t(an.tpoff + q) * nd + m0 + mm) * C;
+          sphi[q] = R2{pp[0], C == 2 ? pp[C - 1] : R(0)};
+        }
+        __syncthreads();
+        if (!act) continue;
+        R sr = R(0), si = R(0);
+        for (int i = 0; i < an.np0; ++i)
+          for (int j = 0; j < an.np1; ++j) {
+            const R w = Lx[i] * Ly[j];
+            const R2* ph = sphi + (i * an.np1 + j) * an.np2;
+            R qr = R(0), qi = R(0);
+#pragma unroll
+            for (int l = 0; l < kP; ++l)
+              if (l < an.np2) {
+                qr = fma(Lz[l], ph[l].x, qr);
+                qi = fma(Lz[l], ph[l].y, qi);
+              }
+            sr = fma(w, qr, sr);
+            si = fma(w, qi, si);
+          }
+        // mm is runtime: add through a register-indexed loop
+#pragma unroll
+        for (int q2 = 0; q2 < MD; ++q2)
+          if (q2 == mm) {
+            accr[q2] += double(sr);
+            acci[q2] += double(si);
+          }
+      }
+    }
+  }
+  if (!act) return;
+#pragma unroll
+  for (int mm = 0; mm < MD; ++mm) {
+    if (mm >= nm) break;
+    if constexpr (PROXYT) {
+      R* o = phi + (size_t(tn.tpoff + k0 + tid) * nd + m0 + mm) * C;
+      o[0] = R(accr[mm]);
+      if constexpr (C == 2) o[1] = R(acci[mm]);
+    } else {
+      const int64_t it = ta.tperm[tn.b + tid];
+      double* o = partial + (size_t(it) * nd + m0 + mm) * C;
+      o[0] = accr[mm];
+      if constexpr (C == 2) o[1] = acci[mm];
+    }
+  }
+}
+
+template <int KIND, typename R, bool CK, int MD>
+void launch_md(const TreeArgs& ta, const KParams& kp, int npitems, int nleaf, const R* str,
+               const R* qhat, R* phi, double* partial, int nd, cudaStream_t st, int& launches) {
+  const unsigned gy = unsigned((nd + MD - 1) / MD);
+  if (npitems > 0) {
+    tree_eval_md_kernel<KIND, R, CK, true, MD>
+        <<<dim3(unsigned(npitems), gy), kEvThreads, 0, st>>>(ta, kp, str, qhat, phi, partial, nd);
+    ++launches;
+  }
+  if (nleaf > 0) {
+    tree_eval_md_kernel<KIND, R, CK, false, MD>
+        <<<dim3(unsigned(nleaf), gy), kEvThreads, 0, st>>>(ta, kp, str, qhat, phi, partial, nd);
+    ++launches;
+  }
+}
+
 template <int KIND, typename R, bool CK>
 cudaError_t run_t(const TreeArgs& ta, const KParams& kp, int nup, const UpItemD* up, int nred,
                   const RedD* red, int npitems, int nleaf, const R* str, double* up_part, R* qhat,
@@ -438,15 +686,25 @@ cudaError_t run_t(const TreeArgs& ta, const KParams& kp, int nup, const UpItemD*
     tree_reduce_kernel<R, C><<<unsigned(nred), 256, 0, st>>>(red, up_part, nd, qhat);
     launches += 2;
   }
-  if (npitems > 0) {
-    tree_eval_kernel<KIND, R, CK, true>
-        <<<dim3(unsigned(npitems), unsigned(nd)), kEvThreads, 0, st>>>(ta, kp, str, qhat, phi, partial, nd);
-    ++launches;
-  }
-  if (nleaf > 0) {
-    tree_eval_kernel<KIND, R, CK, false>
-        <<<dim3(unsigned(nleaf), unsigned(nd)), kEvThreads, 0, st>>>(ta, kp, str, qhat, phi, partial, nd);
-    ++launches;
+  if (nd >= 2) {
+    // several densities: one kernel evaluation per pair for a group of them
+    if (nd <= 4)
+      launch_md<KIND, R, CK, 4>(ta, kp, npitems, nleaf, str, qhat, phi, partial, nd, st, launches);
+    else if (nd <= 8)
+      launch_md<KIND, R, CK, 8>(ta, kp, npitems, nleaf, str, qhat, phi, partial, nd, st, launches);
+    else
+      launch_md<KIND, R, CK, 16>(ta, kp, npitems, nleaf, str, qhat, phi, partial, nd, st, launches);
+  } else {
+    if (npitems > 0) {
+      tree_eval_kernel<KIND, R, CK, true>
+          <<<dim3(unsigned(npitems), 1u), kEvThreads, 0, st>>>(ta, kp, str, qhat, phi, partial, nd);
+      ++launches;
+    }
+    if (nleaf > 0) {
+      tree_eval_kernel<KIND, R, CK, false>
+          <<<dim3(unsigned(nleaf), 1u), kEvThreads, 0, st>>>(ta, kp, str, qhat, phi, partial, nd);
+      ++launches;
+    }
   }
   note_launches(launches);
   return cudaGetLastError();

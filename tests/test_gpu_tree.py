@@ -143,3 +143,25 @@ def test_tree_solve(plan):
     err = _rel(sol_t[:, None], sol_d[:, None], w)
     print(f"\nkind {kind}: tree solve vs direct solve {err:.2e}")
     assert err < 1e-5
+
+
+@pytest.mark.parametrize("nd", [2, 7, 9, 20])
+def test_tree_multi_density(plan, nd):
+    """Several densities per block (groups of 4, 8, 16; the last group
+    partial) equal the one-density tree matvec column by column (FP64: same
+    interactions, other summation order) and, in FP32, stay within FP32
+    accuracy of it."""
+    import torch
+    kind, P, s, w = plan
+    x = _density(s, nd, kind, 20 + nd)
+    for iprec, tol in ((0, 1e-11), (1, 3e-6)):
+        P.set_far_method(iprec, 1, 0.6, 4, 32, 32)  # small leaves: every form
+        y = P.matvec(x, iprec)
+        cols = [0, nd // 2, nd - 1]
+        err = 0.0
+        for m in cols:
+            y1 = P.matvec(x[:, m].contiguous(), iprec)
+            err = max(err, _rel(y[:, m:m + 1], y1[:, None], w))
+        P.set_far_method(iprec, 0)
+        print(f"\nkind {kind} nd {nd} prec {iprec}: multi-density vs one density {err:.2e}")
+        assert err < tol
