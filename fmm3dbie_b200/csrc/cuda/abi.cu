@@ -1345,6 +1345,34 @@ int bie_farfield_dev(int64_t kind, const double* zk, int64_t ns, const double* s
     }
     kp.thresh = thresh;
     const int c = kind == 1 ? 2 : 1;
+    // large sums: the hierarchical far field (same selection rule as a plan)
+    {
+      const char* fm = std::getenv("BIE_FAR_METHOD");
+      const std::string m = fm ? fm : "auto";
+      const char* tp = std::getenv("BIE_TREE_PAIRS");
+      const double pairs_min = tp && *tp ? std::atof(tp) : bie::kTreeAutoPairs;
+      if (ns > 0 && (m == "tree" || (m == "auto" && double(ns) * double(nt) >= pairs_min))) {
+        bie::TreeFar T;
+        const int ier = T.build(g, bie::Plan::default_tree_params(int(iprec), kp), thresh, st);
+        if (ier == bie::kOk) {
+          bie::DBuf<double> str;
+          if (str.alloc(size_t(ns) * 2 * c)) {
+            bie::set_last_error("device allocation failed");
+            return BIE_ERR_NOMEM;
+          }
+          cudaError_t e = bie::dev::launch_pack_strengths(int(kind), int(iprec), ns, charge_dev,
+                                                          dipstr_dev, str.p, st, T.sdest());
+          if (e == cudaSuccess) e = T.run(int(iprec), 1, kp, str.p, pot_dev, st);
+          if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // scratch is released below
+          if (e != cudaSuccess) {
+            bie::set_last_error(cudaGetErrorString(e));
+            return BIE_ERR_CUDA;
+          }
+          return BIE_OK;
+        }
+        if (ier != bie::kErrArg) return ier;  // else: inputs the trees cannot take
+      }
+    }
     const int nch = bie::dev::far_nchunks(nt, std::max<int64_t>(ns, 1), int(kind), int(iprec), 1, sms);
     bie::DBuf<double> str, partial;
     if (str.alloc(std::max<int64_t>(ns, 1) * 2 * c) ||

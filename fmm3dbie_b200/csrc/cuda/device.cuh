@@ -108,8 +108,10 @@ cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp,
 cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t st);
 // Caller strengths (charge, dipole strength per source; complex interleaved
 // when kind == 1) -> far-kernel layout in the far precision, times 1/(4 pi).
+// sdest (optional): source s is stored at position sdest[s].
 cudaError_t launch_pack_strengths(int kind, int precision, int64_t ns, const double* charge,
-                                  const double* dipstr, void* str, cudaStream_t st);
+                                  const double* dipstr, void* str, cudaStream_t st,
+                                  const int32_t* sdest = nullptr);
 // pot[i] = sum_c partial[c][i] (complex when kind == 1).
 cudaError_t launch_reduce_partials(int kind, const double* partial, int nchunks, int64_t ntarg,
                                    double* pot, cudaStream_t st);

@@ -768,17 +768,18 @@ __global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __res
 template <typename R, int CPLX>
 __global__ void pack_strengths_kernel(const double* __restrict__ charge,
                                       const double* __restrict__ dipstr, int64_t ns,
-                                      R* __restrict__ str) {
+                                      R* __restrict__ str, const int32_t* __restrict__ sdest) {
   for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < ns;
        s += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t o = sdest ? int64_t(sdest[s]) : s;
     if (CPLX) {
-      str[4 * s + 0] = R(charge[2 * s] * kOver4Pi);
-      str[4 * s + 1] = R(charge[2 * s + 1] * kOver4Pi);
-      str[4 * s + 2] = R(dipstr[2 * s] * kOver4Pi);
-      str[4 * s + 3] = R(dipstr[2 * s + 1] * kOver4Pi);
+      str[4 * o + 0] = R(charge[2 * s] * kOver4Pi);
+      str[4 * o + 1] = R(charge[2 * s + 1] * kOver4Pi);
+      str[4 * o + 2] = R(dipstr[2 * s] * kOver4Pi);
+      str[4 * o + 3] = R(dipstr[2 * s + 1] * kOver4Pi);
     } else {
-      str[2 * s + 0] = R(charge[s] * kOver4Pi);
-      str[2 * s + 1] = R(dipstr[s] * kOver4Pi);
+      str[2 * o + 0] = R(charge[s] * kOver4Pi);
+      str[2 * o + 1] = R(dipstr[s] * kOver4Pi);
     }
   }
 }
@@ -1631,19 +1632,20 @@ cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t 
 }
 
 cudaError_t launch_pack_strengths(int kind, int precision, int64_t ns, const double* charge,
-                                  const double* dipstr, void* str, cudaStream_t st) {
+                                  const double* dipstr, void* str, cudaStream_t st,
+                                  const int32_t* sdest) {
   if (ns == 0) return cudaSuccess;
   const int b = grid_for(ns, 256);
   if (precision == 1) {
     if (kind == 1)
-      pack_strengths_kernel<float, 1><<<b, 256, 0, st>>>(charge, dipstr, ns, (float*)str);
+      pack_strengths_kernel<float, 1><<<b, 256, 0, st>>>(charge, dipstr, ns, (float*)str, sdest);
     else
-      pack_strengths_kernel<float, 0><<<b, 256, 0, st>>>(charge, dipstr, ns, (float*)str);
+      pack_strengths_kernel<float, 0><<<b, 256, 0, st>>>(charge, dipstr, ns, (float*)str, sdest);
   } else {
     if (kind == 1)
-      pack_strengths_kernel<double, 1><<<b, 256, 0, st>>>(charge, dipstr, ns, (double*)str);
+      pack_strengths_kernel<double, 1><<<b, 256, 0, st>>>(charge, dipstr, ns, (double*)str, sdest);
     else
-      pack_strengths_kernel<double, 0><<<b, 256, 0, st>>>(charge, dipstr, ns, (double*)str);
+      pack_strengths_kernel<double, 0><<<b, 256, 0, st>>>(charge, dipstr, ns, (double*)str, sdest);
   }
   count();
   return cudaGetLastError();

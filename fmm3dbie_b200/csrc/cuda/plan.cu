@@ -235,7 +235,6 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   for (size_t b = 0; b + 5 < hsb.size(); b += 6)
     for (int c = 0; c < 3; ++c) ext = std::max(ext, std::fabs(hsb[b + c]) + std::fabs(hsb[b + 3 + c]));
   const double margin = kp.thresh + std::ldexp(ext, -12);
-  sep_min_ = margin;
   // ---- upload ----------------------------------------------------------------
   BIE_CUDA(upload(tx_, htx, st));
   BIE_CUDA(upload(ty_, hty, st));
@@ -320,6 +319,9 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
       for (int prec = 0; prec < 2; ++prec) {
         if (prec == 1 && !s.keep_f32) continue;
         const int ier = set_far_method(prec, 1, nullptr, st);
+        // inputs the trees cannot take (more than 128 coincident targets)
+        // keep the direct sum; device errors stop the build
+        if (ier == kErrArg) continue;
         if (ier) return ier;
       }
   }
@@ -390,7 +392,7 @@ int Plan::set_far_method(int precision, int method, const tree::Params* prm, cud
       return kErrArg;
     }
     auto t = std::make_unique<TreeFar>();
-    const int ier = t->build(g, p, sep_min_, st);
+    const int ier = t->build(g, p, kp.thresh, st);
     if (ier) return ier;
     tree_[precision] = std::move(t);
     if (precision == 1) {

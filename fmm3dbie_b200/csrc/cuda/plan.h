@@ -256,7 +256,6 @@ class Plan : public Operator {
   DBuf<int> tc_err_;  // timeout flag of the tensor-core far field
   std::unique_ptr<TreeFar> tree_[2];
   int far_method_[2] = {0, 0};
-  double sep_min_ = 0.0;  // accepted particle pairs closer than this keep the threshold test
   DBuf<char> str_;
   DBuf<double> partial_;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};

@@ -761,7 +761,7 @@ void grid_points(const tree::Node& nd, std::vector<double>& px, std::vector<doub
 }
 }  // namespace
 
-int TreeFar::build(const dev::Geometry& g, const tree::Params& prm, double sep_min,
+int TreeFar::build(const dev::Geometry& g, const tree::Params& prm, double thresh,
                    cudaStream_t st) {
   const auto t0 = std::chrono::steady_clock::now();
   prm_ = prm;
@@ -779,6 +779,10 @@ int TreeFar::build(const dev::Geometry& g, const tree::Params& prm, double sep_m
   const std::vector<double> htx = get(g.tx, ntarg_), hty = get(g.ty, ntarg_), htz = get(g.tz, ntarg_);
   const std::vector<double> hsx = get(g.sx, nptso_), hsy = get(g.sy, nptso_), hsz = get(g.sz, nptso_);
   const std::vector<double> hnx = get(g.snx, nptso_), hny = get(g.sny, nptso_), hnz = get(g.snz, nptso_);
+  double ext = 0.0;
+  for (const auto* v : {&htx, &hty, &htz, &hsx, &hsy, &hsz})
+    for (double c : *v) ext = std::max(ext, 2.0 * std::fabs(c));
+  const double sep_min = thresh + std::ldexp(ext, -12);
   tree::Tree T, S;
   tree::build_tree(ntarg_, htx.data(), hty.data(), htz.data(), prm.leaf_t, T);
   tree::build_tree(nptso_, hsx.data(), hsy.data(), hsz.data(), prm.leaf_s, S);

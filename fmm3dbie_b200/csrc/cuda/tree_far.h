@@ -28,9 +28,11 @@ struct TreeStats {
 class TreeFar {
  public:
   // Builds the trees and lists for the plan's targets and oversampled
-  // sources (read back from the device geometry).  sep_min: accepted
-  // particle pairs closer than this keep the self-interaction test.
-  int build(const dev::Geometry& g, const tree::Params& prm, double sep_min, cudaStream_t st);
+  // sources (read back from the device geometry).  Accepted particle pairs
+  // closer than thresh plus 2^-12 of the coordinates' extent (a margin far
+  // above the FP32 rounding of centred coordinates) keep the
+  // self-interaction test r >= thresh.
+  int build(const dev::Geometry& g, const tree::Params& prm, double thresh, cudaStream_t st);
   // Far field of per-source strengths stored in sorted source order
   // (str_sorted[(s * nd + m) * SW], SW = 4 Helmholtz / 2 Laplace, far
   // precision) into partial[(i * nd + m) * C] at original target index i.

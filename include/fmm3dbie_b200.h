@@ -394,6 +394,10 @@ int bie_tree_check(int64_t nt, const double* targ, int64_t ns, const double* src
  * nrm_dev (unit vectors) likewise; targ_dev = x[nt], y[nt], z[nt].
  * kind 0: real charge/dipstr/pot; kind 1: complex interleaved, zk = (re,im).
  * iprec 0: FP64 sum, 1: FP32 pair sum accumulated in FP64 per source tile.
+ * From ns * nt >= 1.5e10 on (BIE_FAR_METHOD = direct | tree | auto,
+ * BIE_TREE_PAIRS) the sum is evaluated hierarchically, as by a plan
+ * (bie_plan_set_far_method defaults; about 1e-9 relative in FP64, 1e-6 in
+ * FP32) -- the FMM's contract of a sum accurate to a tolerance.
  * Allocates its scratch (per-chunk partial sums) with cudaMalloc and
  * returns after the stream has finished the call. */
 int bie_farfield_dev(int64_t kind, const double* zk, int64_t ns, const double* src_dev,

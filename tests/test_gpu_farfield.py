@@ -74,3 +74,20 @@ def test_farfield_matches_direct_sum(torch, kind, zk):
     assert np.max(np.abs(got64 - ref)) < 1e-12 * scale
     tol32 = 2e-5 if abs(zk) < 10 else 2e-4
     assert np.max(np.abs(got32 - ref)) < tol32 * scale
+
+
+@pytest.mark.parametrize("kind,zk", [(0, 0j), (1, 2.5 + 0j), (1, 1.5 + 0.3j)])
+def test_farfield_hierarchical(torch, kind, zk, monkeypatch):
+    """Above the size threshold (forced here with BIE_FAR_METHOD=tree) the
+    sum is evaluated hierarchically: within 1e-8 (FP64) and 1e-5 (FP32) of
+    the direct sum, coincident source/target points included."""
+    src, nrm, ch, dp, targ = problem(2, ns=40000, nt=30000)
+    thresh = 1e-14
+    monkeypatch.setenv("BIE_FAR_METHOD", "direct")
+    ref = run(torch, kind, zk, src, nrm, ch, dp, targ, thresh, 0)
+    monkeypatch.setenv("BIE_FAR_METHOD", "tree")
+    for iprec, tol in ((0, 1e-8), (1, 1e-5)):
+        got = run(torch, kind, zk, src, nrm, ch, dp, targ, thresh, iprec)
+        err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+        print(f"\nkind {kind} zk {zk} iprec {iprec}: tree vs direct {err:.2e}")
+        assert err < tol
