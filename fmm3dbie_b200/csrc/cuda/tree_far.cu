@@ -441,7 +441,6 @@ __global__ void __launch_bounds__(kEvThreads)
   using R4 = typename Vec<R>::T4;
   constexpr int SW = KIND == 1 ? 4 : 2;
   constexpr int C = KIND == 1 ? 2 : 1;
-  constexpr bool F32 = sizeof(R) == 4;
   __shared__ R4 sg0[kMdTile];
   __shared__ R2 sg1[kMdTile];
   // the source strengths of the list phase and the proxy potentials of the
@@ -591,8 +590,8 @@ __global__ void __launch_bounds__(kEvThreads)
     e0 = ta.tn[n].pe0;
     e1 = ta.tn[n].pe1;
   }
-  (void)F32;
   if constexpr (!PROXYT) {
+    // downward pass, one density at a time through the shared buffer
     for (int a = node; a >= 0; a = ta.tn[a].parent) {
       const TNodeD an = ta.tn[a];
       if (an.tpoff < 0) continue;
