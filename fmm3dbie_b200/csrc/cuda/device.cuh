@@ -143,8 +143,9 @@ cudaError_t launch_far_md(const Geometry& g, const KParams& kp, const MatvecArgs
                           cudaStream_t st);
 cudaError_t launch_oversample(const Geometry& g, const KParams& kp, const MatvecArgs& a,
                               cudaStream_t st);
+// sdest (optional): source s is stored at position sdest[s].
 cudaError_t launch_source_consts(const Geometry& g, const KParams& kp, int precision, void* ab,
-                                 cudaStream_t st);
+                                 cudaStream_t st, const int32_t* sdest = nullptr);
 
 // ---- GMRES helpers --------------------------------------------------------
 // Vectors hold npts nodes x nd densities (point-major).  The nodes form

@@ -392,7 +392,8 @@ __global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
 // densities); feeds far_md_kernel.
 template <typename R, int CPLX>
 __device__ __forceinline__ void oversample_body(const Geometry& g, const double* __restrict__ sigma,
-                                                R* __restrict__ sover, int nd, int p, double* sh) {
+                                                R* __restrict__ sover, int nd, int p, double* sh,
+                                                const int32_t* __restrict__ sdest = nullptr) {
   const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
   const int os = g.ostart[p], nf = g.ostart[p + 1] - os;
   const double* M = g.imat + g.cmoff[g.pclass[p]];
@@ -408,7 +409,7 @@ __device__ __forceinline__ void oversample_body(const Geometry& g, const double*
       sr = fma(mv, sh[C * (j * nd + m)], sr);
       if (CPLX) si = fma(mv, sh[C * (j * nd + m) + 1], si);
     }
-    const size_t o = size_t(os + l) * nd + m;
+    const size_t o = size_t(sdest ? sdest[os + l] : os + l) * nd + m;
     sover[C * o] = R(sr);
     if (CPLX) sover[C * o + 1] = R(si);
   }
@@ -416,25 +417,27 @@ __device__ __forceinline__ void oversample_body(const Geometry& g, const double*
 
 template <typename R, int CPLX>
 __global__ void oversample_kernel(Geometry g, const double* __restrict__ sigma,
-                                  R* __restrict__ sover, int nd) {
+                                  R* __restrict__ sover, int nd, const int32_t* __restrict__ sdest) {
   extern __shared__ double sh[];
-  oversample_body<R, CPLX>(g, sigma, sover, nd, blockIdx.x, sh);
+  oversample_body<R, CPLX>(g, sigma, sover, nd, blockIdx.x, sh, sdest);
 }
 
 // Per-source constants a_s = alpha w_s/(4pi), b_s = beta w_s/(4pi).
 template <typename R, int CPLX>
-__global__ void source_consts_kernel(Geometry g, KParams kp, R* __restrict__ ab) {
+__global__ void source_consts_kernel(Geometry g, KParams kp, R* __restrict__ ab,
+                                     const int32_t* __restrict__ sdest) {
   for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < g.nptso;
        s += int64_t(gridDim.x) * blockDim.x) {
     const double f = g.sw[s] * kOver4Pi;
+    const int64_t o = sdest ? int64_t(sdest[s]) : s;
     if (CPLX) {
-      ab[4 * s + 0] = R(kp.ar * f);
-      ab[4 * s + 1] = R(kp.ai * f);
-      ab[4 * s + 2] = R(kp.br * f);
-      ab[4 * s + 3] = R(kp.bi * f);
+      ab[4 * o + 0] = R(kp.ar * f);
+      ab[4 * o + 1] = R(kp.ai * f);
+      ab[4 * o + 2] = R(kp.br * f);
+      ab[4 * o + 3] = R(kp.bi * f);
     } else {
-      ab[2 * s + 0] = R(kp.ar * f);
-      ab[2 * s + 1] = R(kp.br * f);
+      ab[2 * o + 0] = R(kp.ar * f);
+      ab[2 * o + 1] = R(kp.br * f);
     }
   }
 }
@@ -1497,7 +1500,7 @@ cudaError_t launch_oversample(const Geometry& g, const KParams& kp, const Matvec
   const dim3 grid(static_cast<unsigned>(g.npatches)), block(128);
   auto go = [&](auto kern, auto* out) {
     if (sh > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sh));
-    kern<<<grid, block, sh, st>>>(g, a.sigma, out, a.nd);
+    kern<<<grid, block, sh, st>>>(g, a.sigma, out, a.nd, a.sdest);
   };
   if (a.precision == 1) {
     if (cplx)
@@ -1515,19 +1518,19 @@ cudaError_t launch_oversample(const Geometry& g, const KParams& kp, const Matvec
 }
 
 cudaError_t launch_source_consts(const Geometry& g, const KParams& kp, int precision, void* ab,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, const int32_t* sdest) {
   if (g.nptso == 0) return cudaSuccess;
   const int b = grid_for(g.nptso, 256);
   if (precision == 1) {
     if (kp.kind == 1)
-      source_consts_kernel<float, 1><<<b, 256, 0, st>>>(g, kp, (float*)ab);
+      source_consts_kernel<float, 1><<<b, 256, 0, st>>>(g, kp, (float*)ab, sdest);
     else
-      source_consts_kernel<float, 0><<<b, 256, 0, st>>>(g, kp, (float*)ab);
+      source_consts_kernel<float, 0><<<b, 256, 0, st>>>(g, kp, (float*)ab, sdest);
   } else {
     if (kp.kind == 1)
-      source_consts_kernel<double, 1><<<b, 256, 0, st>>>(g, kp, (double*)ab);
+      source_consts_kernel<double, 1><<<b, 256, 0, st>>>(g, kp, (double*)ab, sdest);
     else
-      source_consts_kernel<double, 0><<<b, 256, 0, st>>>(g, kp, (double*)ab);
+      source_consts_kernel<double, 0><<<b, 256, 0, st>>>(g, kp, (double*)ab, sdest);
   }
   count();
   return cudaGetLastError();

@@ -392,7 +392,7 @@ int Plan::set_far_method(int precision, int method, const tree::Params* prm, cud
       return kErrArg;
     }
     auto t = std::make_unique<TreeFar>();
-    const int ier = t->build(g, p, kp.thresh, st);
+    const int ier = t->build(g, p, kp.thresh, st, &kp, precision);
     if (ier) return ier;
     tree_[precision] = std::move(t);
     if (precision == 1) {
@@ -613,9 +613,14 @@ int Plan::matvec_tree(int precision, int nd, const double* d_sigma, double* d_po
   a.weff_f32 = precision == 1;
   a.sdest = T.sdest();
   if (timing) BIE_CUDA(cudaEventRecord(ev_[0], st));
-  BIE_CUDA(dev::launch_strengths(g, kp, a, st));
+  // one density: (charge, dipole) strengths; several: oversampled densities
+  if (nd > 1)
+    BIE_CUDA(dev::launch_oversample(g, kp, a, st));
+  else
+    BIE_CUDA(dev::launch_strengths(g, kp, a, st));
   if (timing) BIE_CUDA(cudaEventRecord(ev_[1], st));
-  BIE_CUDA(T.run(precision, nd, kp, str_.p, partial_.p, st));
+  BIE_CUDA(T.run(precision, nd, kp, nd > 1 ? nullptr : str_.p, partial_.p, st,
+                 nd > 1 ? str_.p : nullptr));
   if (timing) BIE_CUDA(cudaEventRecord(ev_[2], st));
   BIE_CUDA(dev::launch_combine(g, nr, kp, a, st));
   if (timing) {

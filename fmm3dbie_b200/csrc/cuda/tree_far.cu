@@ -133,10 +133,14 @@ __device__ __forceinline__ void lagrange_d(int p, R u, R* L, R* D) {
 constexpr int kUpThreads = 128, kUpTile = 32;
 constexpr int64_t kUpChunk = 2048;
 
-template <int KIND, typename R>
+// SIG = false: str holds each source's (charge, dipole) strengths per
+// density; SIG = true: they are formed as (a_s sigma_m, b_s sigma_m) from
+// the oversampled densities sig and the per-source constants ab.
+template <int KIND, typename R, bool SIG>
 __global__ void __launch_bounds__(kUpThreads)
     tree_up_kernel(const UpItemD* __restrict__ items, TreeArgs ta, const R* __restrict__ str,
-                   int nd, double* __restrict__ up_part) {
+                   const R* __restrict__ sig, const R* __restrict__ ab, int nd,
+                   double* __restrict__ up_part) {
   constexpr int SW = KIND == 1 ? 4 : 2;
   constexpr int C = KIND == 1 ? 2 : 1;
   __shared__ R sL[3][kP][kUpTile];
@@ -186,8 +190,26 @@ __global__ void __launch_bounds__(kUpThreads)
             }
         }
       }
-      for (int q = tid; q < ns * SW; q += kUpThreads)
-        sS[q / SW][q % SW] = str[(size_t(sb + q / SW) * nd + m) * SW + q % SW];
+      if constexpr (SIG) {
+        for (int q = tid; q < ns; q += kUpThreads) {
+          const size_t si = size_t(sb + q);
+          const R* a = ab + si * SW;
+          const R* sg = sig + (si * nd + m) * C;
+          if constexpr (KIND == 1) {
+            const R sr = sg[0], sim = sg[1];
+            sS[q][0] = fma(a[0], sr, -a[1] * sim);
+            sS[q][1] = fma(a[0], sim, a[1] * sr);
+            sS[q][2] = fma(a[2], sr, -a[3] * sim);
+            sS[q][3] = fma(a[2], sim, a[3] * sr);
+          } else {
+            sS[q][0] = a[0] * sg[0];
+            sS[q][1] = a[1] * sg[0];
+          }
+        }
+      } else {
+        for (int q = tid; q < ns * SW; q += kUpThreads)
+          sS[q / SW][q % SW] = str[(size_t(sb + q / SW) * nd + m) * SW + q % SW];
+      }
       __syncthreads();
       if (nl > 0) {
         R tr[kP], ti[kP];
@@ -427,28 +449,33 @@ __global__ void __launch_bounds__(kEvThreads)
 }
 
 // Several densities per block (MD of them, densities m0 .. m0 + MD - 1 on
-// grid y): each pair's unit responses G and D (pair_helm_unit) are computed
-// once and applied to every density's charge and dipole strengths; proxy
-// charges use G alone.  Otherwise as tree_eval_kernel.
+// grid y).  The charge and dipole strengths of a layer potential are both
+// proportional to the oversampled density, c_m = a_s sigma_m and
+// d_m = b_s sigma_m (a_s = alpha w_s/(4 pi), b_s = beta w_s/(4 pi)), so each
+// pair's kernel value K = a_s G + b_s D is formed once from its unit
+// responses (pair_helm_unit) and applied to every density with one complex
+// multiply-add; proxy charges use G alone.  sig: sigma_over in tree order,
+// ab: (a_s, b_s) in tree order.  Otherwise as tree_eval_kernel.
 constexpr int kMdTile = 64;
 
 template <int KIND, typename R, bool CK, bool PROXYT, int MD>
 __global__ void __launch_bounds__(kEvThreads)
-    tree_eval_md_kernel(TreeArgs ta, KParams kp, const R* __restrict__ str,
-                        const R* __restrict__ qhat, R* __restrict__ phi,
-                        double* __restrict__ partial, int nd) {
+    tree_eval_md_kernel(TreeArgs ta, KParams kp, const R* __restrict__ sig,
+                        const R* __restrict__ ab, const R* __restrict__ qhat,
+                        R* __restrict__ phi, double* __restrict__ partial, int nd) {
   using R2 = typename Vec<R>::T2;
   using R4 = typename Vec<R>::T4;
   constexpr int SW = KIND == 1 ? 4 : 2;
   constexpr int C = KIND == 1 ? 2 : 1;
   __shared__ R4 sg0[kMdTile];
   __shared__ R2 sg1[kMdTile];
-  // the source strengths of the list phase and the proxy potentials of the
-  // downward phase share one buffer
-  constexpr size_t kSstBytes = sizeof(R) * kMdTile * MD * SW;
+  __shared__ R4 sab[kMdTile];  // (a_s, b_s) of particle sources
+  // the densities (or proxy charges) of the list phase and the proxy
+  // potentials of the downward phase share one buffer
+  constexpr size_t kSstBytes = sizeof(R) * kMdTile * MD * C;
   constexpr size_t kPhiBytes = PROXYT ? 0 : sizeof(R2) * tree::kMaxProxies;
   __shared__ __align__(16) unsigned char sbuf[kSstBytes > kPhiBytes ? kSstBytes : kPhiBytes];
-  R(*sst)[MD][SW] = reinterpret_cast<R(*)[MD][SW]>(sbuf);
+  R(*sst)[MD][C] = reinterpret_cast<R(*)[MD][C]>(sbuf);
   R2* sphi = reinterpret_cast<R2*>(sbuf);
   __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
   const double2* tab = nullptr;
@@ -514,20 +541,17 @@ __global__ void __launch_bounds__(kEvThreads)
           } else {
             sg0[qq] = R4{R(ta.sx[s] - cx), R(ta.sy[s] - cy), R(ta.sz[s] - cz), R(ta.snx[s])};
             sg1[qq] = R2{R(ta.sny[s]), R(ta.snz[s])};
+            const R* a = ab + size_t(s) * SW;
+            sab[qq] = SW == 4 ? R4{a[0], a[1], a[2], a[3]} : R4{a[0], R(0), a[1], R(0)};
           }
         }
-        for (int qq = tid; qq < ns * MD * SW; qq += kEvThreads) {
-          const int sj = qq / (MD * SW), rem = qq - sj * (MD * SW);
-          const int mm = rem / SW, c = rem - mm * SW;
-          R v = R(0);
-          if (mm < nm) {
-            if (en.kind == 2) {
-              if (c < C) v = qhat[(size_t(sb + sj) * nd + m0 + mm) * C + c];
-            } else {
-              v = str[(size_t(sb + sj) * nd + m0 + mm) * SW + c];
-            }
+        {
+          const R* src = en.kind == 2 ? qhat : sig;
+          for (int qq = tid; qq < ns * MD * C; qq += kEvThreads) {
+            const int sj = qq / (MD * C), rem = qq - sj * (MD * C);
+            const int mm = rem / C, c = rem - mm * C;
+            sst[sj][mm][c] = mm < nm ? src[(size_t(sb + sj) * nd + m0 + mm) * C + c] : R(0);
           }
-          sst[sj][mm][c] = v;
         }
         __syncthreads();
         if (!wact) continue;  // a warp without targets only helps load the tiles
@@ -553,17 +577,21 @@ __global__ void __launch_bounds__(kEvThreads)
         } else {
           const bool chk = en.kind == 0;
           for (int j = 0; j < ns; ++j) {
+            const R4 w = sab[j];  // (a_r, a_i, b_r, b_i); Laplace (a, 0, b, 0)
             if constexpr (KIND == 1) {
               R gr, gi, dr, di;
               if (chk)
                 pair_helm_unit<true>(tx, ty, tz, sg0[j], sg1[j], k, kim, thr2, CK, gr, gi, dr, di, tab);
               else
                 pair_helm_unit<false>(tx, ty, tz, sg0[j], sg1[j], k, kim, thr2, CK, gr, gi, dr, di, tab);
+              // K = a G + b D
+              const R kr_ = fma(w.x, gr, fma(-w.y, gi, fma(w.z, dr, -w.w * di)));
+              const R ki_ = fma(w.x, gi, fma(w.y, gr, fma(w.z, di, w.w * dr)));
 #pragma unroll
               for (int mm = 0; mm < MD; ++mm) {
-                const R4 sv = *reinterpret_cast<const R4*>(sst[j][mm]);
-                tr[mm] = fma(sv.x, gr, fma(-sv.y, gi, fma(sv.z, dr, fma(-sv.w, di, tr[mm]))));
-                ti[mm] = fma(sv.x, gi, fma(sv.y, gr, fma(sv.z, di, fma(sv.w, dr, ti[mm]))));
+                const R2 sv = *reinterpret_cast<const R2*>(sst[j][mm]);
+                tr[mm] = fma(sv.x, kr_, fma(-sv.y, ki_, tr[mm]));
+                ti[mm] = fma(sv.x, ki_, fma(sv.y, kr_, ti[mm]));
               }
             } else {
               R g, dd;
@@ -571,9 +599,9 @@ __global__ void __launch_bounds__(kEvThreads)
                 pair_lap_unit<R, true>(tx, ty, tz, sg0[j], sg1[j], thr2, g, dd);
               else
                 pair_lap_unit<R, false>(tx, ty, tz, sg0[j], sg1[j], thr2, g, dd);
+              const R kv = fma(w.x, g, w.z * dd);
 #pragma unroll
-              for (int mm = 0; mm < MD; ++mm)
-                tr[mm] = fma(sst[j][mm][0], g, fma(sst[j][mm][1], dd, tr[mm]));
+              for (int mm = 0; mm < MD; ++mm) tr[mm] = fma(sst[j][mm][0], kv, tr[mm]);
             }
           }
         }
@@ -658,41 +686,48 @@ __global__ void __launch_bounds__(kEvThreads)
 }
 
 template <int KIND, typename R, bool CK, int MD>
-void launch_md(const TreeArgs& ta, const KParams& kp, int npitems, int nleaf, const R* str,
-               const R* qhat, R* phi, double* partial, int nd, cudaStream_t st, int& launches) {
+void launch_md(const TreeArgs& ta, const KParams& kp, int npitems, int nleaf, const R* sig,
+               const R* ab, const R* qhat, R* phi, double* partial, int nd, cudaStream_t st,
+               int& launches) {
   const unsigned gy = unsigned((nd + MD - 1) / MD);
   if (npitems > 0) {
-    tree_eval_md_kernel<KIND, R, CK, true, MD>
-        <<<dim3(unsigned(npitems), gy), kEvThreads, 0, st>>>(ta, kp, str, qhat, phi, partial, nd);
+    tree_eval_md_kernel<KIND, R, CK, true, MD><<<dim3(unsigned(npitems), gy), kEvThreads, 0, st>>>(
+        ta, kp, sig, ab, qhat, phi, partial, nd);
     ++launches;
   }
   if (nleaf > 0) {
-    tree_eval_md_kernel<KIND, R, CK, false, MD>
-        <<<dim3(unsigned(nleaf), gy), kEvThreads, 0, st>>>(ta, kp, str, qhat, phi, partial, nd);
+    tree_eval_md_kernel<KIND, R, CK, false, MD><<<dim3(unsigned(nleaf), gy), kEvThreads, 0, st>>>(
+        ta, kp, sig, ab, qhat, phi, partial, nd);
     ++launches;
   }
 }
 
 template <int KIND, typename R, bool CK>
 cudaError_t run_t(const TreeArgs& ta, const KParams& kp, int nup, const UpItemD* up, int nred,
-                  const RedD* red, int npitems, int nleaf, const R* str, double* up_part, R* qhat,
-                  R* phi, double* partial, int nd, cudaStream_t st) {
+                  const RedD* red, int npitems, int nleaf, const R* str, const R* sig,
+                  const R* ab, double* up_part, R* qhat, R* phi, double* partial, int nd,
+                  cudaStream_t st) {
   constexpr int C = KIND == 1 ? 2 : 1;
   int launches = 0;
+  const bool md = nd >= 2;  // several densities: from sig and ab
   if (nup > 0) {
-    tree_up_kernel<KIND, R><<<dim3(unsigned(nup), unsigned(nd)), kUpThreads, 0, st>>>(up, ta, str, nd,
-                                                                                     up_part);
+    const dim3 grid{unsigned(nup), unsigned(nd), 1u};
+    if (md)
+      tree_up_kernel<KIND, R, true><<<grid, kUpThreads, 0, st>>>(up, ta, nullptr, sig, ab, nd, up_part);
+    else
+      tree_up_kernel<KIND, R, false><<<grid, kUpThreads, 0, st>>>(up, ta, str, nullptr, nullptr, nd,
+                                                                  up_part);
     tree_reduce_kernel<R, C><<<unsigned(nred), 256, 0, st>>>(red, up_part, nd, qhat);
     launches += 2;
   }
-  if (nd >= 2) {
-    // several densities: one kernel evaluation per pair for a group of them
+  if (md) {
+    // one kernel evaluation per pair for a group of densities
     if (nd <= 4)
-      launch_md<KIND, R, CK, 4>(ta, kp, npitems, nleaf, str, qhat, phi, partial, nd, st, launches);
+      launch_md<KIND, R, CK, 4>(ta, kp, npitems, nleaf, sig, ab, qhat, phi, partial, nd, st, launches);
     else if (nd <= 8)
-      launch_md<KIND, R, CK, 8>(ta, kp, npitems, nleaf, str, qhat, phi, partial, nd, st, launches);
+      launch_md<KIND, R, CK, 8>(ta, kp, npitems, nleaf, sig, ab, qhat, phi, partial, nd, st, launches);
     else
-      launch_md<KIND, R, CK, 16>(ta, kp, npitems, nleaf, str, qhat, phi, partial, nd, st, launches);
+      launch_md<KIND, R, CK, 16>(ta, kp, npitems, nleaf, sig, ab, qhat, phi, partial, nd, st, launches);
   } else {
     if (npitems > 0) {
       tree_eval_kernel<KIND, R, CK, true>
@@ -761,7 +796,7 @@ void grid_points(const tree::Node& nd, std::vector<double>& px, std::vector<doub
 }  // namespace
 
 int TreeFar::build(const dev::Geometry& g, const tree::Params& prm, double thresh,
-                   cudaStream_t st) {
+                   cudaStream_t st, const dev::KParams* kp, int precision) {
   const auto t0 = std::chrono::steady_clock::now();
   prm_ = prm;
   ntarg_ = g.ntarg;
@@ -1005,6 +1040,13 @@ int TreeFar::build(const dev::Geometry& g, const tree::Params& prm, double thres
   TF_CUDA(put_raw(cent_, cent, st));
   TF_CUDA(put_raw(upitems_, ups, st));
   TF_CUDA(put_raw(reds_, reds, st));
+  if (kp && g.sw) {
+    // per-source (a_s, b_s) in tree order for several densities at once
+    const size_t rs = precision == 1 ? sizeof(float) : sizeof(double);
+    TF_CUDA(ab_.alloc(size_t(nptso_) * (kp->kind == 1 ? 4 : 2) * rs));
+    TF_CUDA(dev::launch_source_consts(g, *kp, precision, ab_.p, st, sdest_.p));
+    ab_precision_ = precision;
+  }
   TF_CUDA(cudaStreamSynchronize(st));  // host vectors above feed async copies
   nleaf_ = int(leaves.size());
   npitems_ = int(pitems.size());
@@ -1036,8 +1078,9 @@ int TreeFar::ensure_scratch(int nd, int precision) {
 }
 
 cudaError_t TreeFar::run(int precision, int nd, const dev::KParams& kp, const void* str_sorted,
-                         double* partial, cudaStream_t st) {
+                         double* partial, cudaStream_t st, const void* sig_sorted) {
   if (nd < 1 || nd > 65535) return cudaErrorInvalidValue;
+  if (nd >= 2 && (!sig_sorted || !ab_.p || ab_precision_ != precision)) return cudaErrorInvalidValue;
   if (ensure_scratch(nd, precision) != kOk) return cudaErrorMemoryAllocation;
   dev::TreeArgs ta;
   ta.tn = reinterpret_cast<const dev::TNodeD*>(tnodes_.p);
@@ -1069,7 +1112,9 @@ cudaError_t TreeFar::run(int precision, int nd, const dev::KParams& kp, const vo
     constexpr int KIND = decltype(kind_c)::value;
     constexpr bool CK = decltype(ck_c)::value;
     return dev::run_t<KIND, R, CK>(ta, kp, nup_, up, nred_, red, npitems_, nleaf_,
-                                   static_cast<const R*>(str_sorted), up_part_.p,
+                                   static_cast<const R*>(str_sorted),
+                                   static_cast<const R*>(sig_sorted),
+                                   reinterpret_cast<const R*>(ab_.p), up_part_.p,
                                    reinterpret_cast<R*>(qhat_.p), reinterpret_cast<R*>(phi_.p),
                                    partial, nd, st);
   };

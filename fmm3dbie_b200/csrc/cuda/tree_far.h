@@ -32,12 +32,19 @@ class TreeFar {
   // closer than thresh plus 2^-12 of the coordinates' extent (a margin far
   // above the FP32 rounding of centred coordinates) keep the
   // self-interaction test r >= thresh.
-  int build(const dev::Geometry& g, const tree::Params& prm, double thresh, cudaStream_t st);
-  // Far field of per-source strengths stored in sorted source order
+  // kp and precision (optional, with g.sw set): also keep the per-source
+  // constants (alpha w_s/(4 pi), beta w_s/(4 pi)) in tree order and that
+  // precision, for several densities at once.
+  int build(const dev::Geometry& g, const tree::Params& prm, double thresh, cudaStream_t st,
+            const dev::KParams* kp = nullptr, int precision = 0);
+  // Far field into partial[(i * nd + m) * C] at original target index i.
+  // nd = 1: from per-source (charge, dipole) strengths in tree order
   // (str_sorted[(s * nd + m) * SW], SW = 4 Helmholtz / 2 Laplace, far
-  // precision) into partial[(i * nd + m) * C] at original target index i.
+  // precision).  nd >= 2: from the oversampled densities in tree order
+  // (sig_sorted[(s * nd + m) * C], C = 2 / 1) and the constants kept by
+  // build (which then needs kp and this precision).
   cudaError_t run(int precision, int nd, const dev::KParams& kp, const void* str_sorted,
-                  double* partial, cudaStream_t st);
+                  double* partial, cudaStream_t st, const void* sig_sorted = nullptr);
   // original oversampled source index -> sorted position
   const int32_t* sdest() const { return sdest_.p; }
   // per original target: centre of its leaf (3 doubles), the origin of the
@@ -60,7 +67,8 @@ class TreeFar {
   DBuf<int2> pitems_;
   DBuf<double> tpx_, tpy_, tpz_, spx_, spy_, spz_;
   DBuf<double> up_part_;
-  DBuf<char> qhat_, phi_;
+  DBuf<char> qhat_, phi_, ab_;
+  int ab_precision_ = -1;
   int64_t up_len_ = 0;
 };
 
