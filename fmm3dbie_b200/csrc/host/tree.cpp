@@ -102,6 +102,7 @@ void build_tree(int64_t n, const double* x, const double* y, const double* z, in
 void set_proxies(Tree& t, const Params& prm) {
   for (Node& nd : t.nodes) {
     nd.np[0] = nd.np[1] = nd.np[2] = 0;
+    nd.capped = false;
     if (nd.n() <= 1) continue;
     double ext[3], emax = 0.0;
     for (int d = 0; d < 3; ++d) {
@@ -126,11 +127,14 @@ void set_proxies(Tree& t, const Params& prm) {
           pd = int(std::ceil(prm.p * lmax / std::log(rho(ext[d])) - 1e-9));
           pd += int(std::ceil(prm.kscale * prm.k * 0.5 * ext[d] - 1e-9));
         }
-        np[d] = std::min(std::max(pd, 1), kMaxP);
+        np[d] = std::max(pd, 1);
       }
-      while (np[0] * np[1] * np[2] > kMaxProxies) {
-        const int d = int(std::max_element(np, np + 3) - np);
-        --np[d];
+      // a grid the caps cannot hold would miss the accuracy: no proxies,
+      // and the traversal splits the node instead of accepting its pairs
+      if (np[0] > kMaxP || np[1] > kMaxP || np[2] > kMaxP ||
+          int64_t(np[0]) * np[1] * np[2] > kMaxProxies) {
+        nd.capped = true;
+        continue;
       }
     }
     if (int64_t(np[0]) * np[1] * np[2] >= nd.n()) continue;
@@ -151,7 +155,10 @@ void traverse(const Tree& T, const Tree& S, const Params& prm, double sep_min,
     double d2 = 0.0;
     for (int d = 0; d < 3; ++d) d2 += (t.c[d] - s.c[d]) * (t.c[d] - s.c[d]);
     const double D = std::sqrt(d2);
-    if (t.r + s.r < prm.theta * D) {
+    const bool tleaf = t.nchild == 0, sleaf = s.nchild == 0;
+    // a pair with a node too large for an accurate grid is split further
+    const bool split_capped = (t.capped && !tleaf) || (s.capped && !sleaf);
+    if (t.r + s.r < prm.theta * D && !split_capped) {
       const double nt = double(t.n()), ns = double(s.n());
       const double pt = t.nprox(), ps = s.nprox();
       double best = nt * ns;
@@ -171,9 +178,14 @@ void traverse(const Tree& T, const Tree& S, const Params& prm, double sep_min,
       out.push_back({a, b, kind});
       continue;
     }
-    const bool tleaf = t.nchild == 0, sleaf = s.nchild == 0;
     if (tleaf && sleaf) {
       out.push_back({a, b, kPPCheck});
+    } else if (split_capped) {
+      if (t.capped && !tleaf && (!s.capped || sleaf || t.r >= s.r)) {
+        for (int c = 0; c < t.nchild; ++c) stack.push_back({t.child0 + c, b});
+      } else {
+        for (int c = 0; c < s.nchild; ++c) stack.push_back({a, s.child0 + c});
+      }
     } else if (sleaf || (!tleaf && t.r >= s.r)) {
       for (int c = 0; c < t.nchild; ++c) stack.push_back({t.child0 + c, b});
     } else {

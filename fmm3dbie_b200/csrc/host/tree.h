@@ -53,6 +53,7 @@ struct Node {
   double r = 0;                // half diagonal
   int parent = -1, child0 = -1, nchild = 0, level = 0;
   int np[3] = {0, 0, 0};       // proxy grid; all 0 when the node has none
+  bool capped = false;         // its grid would exceed kMaxP / kMaxProxies
   int64_t n() const { return e - b; }
   int nprox() const { return np[0] * np[1] * np[2]; }
 };
@@ -70,7 +71,10 @@ void build_tree(int64_t n, const double* x, const double* y, const double* z, in
 // Chebyshev interpolation error for a source at the smallest accepted
 // distance (r / theta) matches that of p nodes along the longest side,
 // plus kscale * k * side_d / 2 for the oscillation of e^{ikr}; a node whose
-// grid would hold as many points as the node itself gets none.
+// grid would hold as many points as the node itself gets none, and a node
+// whose grid would exceed kMaxP points per side or kMaxProxies points gets
+// none and is marked capped (the traversal then splits it rather than
+// accept its pairs).
 void set_proxies(Tree& t, const Params& prm);
 
 enum Kind { kPPCheck = 0, kPP = 1, kPC = 2, kCP = 3, kCC = 4 };

@@ -26,7 +26,7 @@ def _ellipsoid(rng, n):
 
 
 @pytest.mark.parametrize("theta,p,k", [(0.5, 8, 0.0), (0.7, 4, 0.0), (0.5, 10, 5.0),
-                                       (0.3, 6, 0.0)])
+                                       (0.3, 6, 0.0), (0.5, 10, 40.0)])
 def test_coverage_surface(theta, p, k):
     rng = np.random.default_rng(1)
     out = _check(_ellipsoid(rng, 6000), _ellipsoid(rng, 9000), theta, p, k)
@@ -59,3 +59,17 @@ def test_lists_cheaper_than_direct():
     frac = out[8] / out[9]
     print(f"\nkernel evaluations of the lists: {frac:.3f} of the direct sum")
     assert frac < 0.3
+
+
+def test_high_frequency_splits_capped_nodes():
+    """At k = 40 the grids of the large nodes would exceed 16 points per side:
+    those nodes get no proxies and their pairs are split until the grids fit
+    (on this point set down to the leaves: the lists become the direct sum,
+    exact rather than under-resolved), with coverage still exact."""
+    rng = np.random.default_rng(5)
+    t, s = _ellipsoid(rng, 60000), _ellipsoid(rng, 100000)
+    lo = _check(t, s, 0.5, 10, 2.0)
+    hi = _check(t, s, 0.5, 10, 40.0)
+    assert lo[0] == 0 and hi[0] == 0
+    print(f"\nkernel evaluations of the lists: k = 2 {lo[8] / lo[9]:.3f}, k = 40 {hi[8] / hi[9]:.3f}")
+    assert lo[8] < lo[9] and hi[8] <= hi[9]
