@@ -820,7 +820,8 @@ int TreeFar::build(const dev::Geometry& g, const tree::Params& prm, double thres
   tree::Tree T, S;
   tree::build_tree(ntarg_, htx.data(), hty.data(), htz.data(), prm.leaf_t, T);
   tree::build_tree(nptso_, hsx.data(), hsy.data(), hsz.data(), prm.leaf_s, S);
-  // target leaves must fit one thread block: split coincident targets by index
+  // target leaves must fit one thread block; only more than 128 coincident
+  // targets (which no split separates) exceed it
   for (const auto& nd : T.nodes)
     if (nd.nchild == 0 && nd.n() > dev::kEvThreads) {
       set_last_error("tree far field: more than 128 coincident targets");
