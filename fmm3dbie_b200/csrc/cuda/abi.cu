@@ -1224,7 +1224,7 @@ int bie_tree_check(int64_t nt, const double* targ, int64_t ns, const double* src
     bie::tree::set_proxies(S, prm);
     std::vector<bie::tree::Interaction> ia;
     bie::tree::traverse(T, S, prm, 0.0, ia);
-    for (int q = 0; q < 10; ++q) out[q] = 0.0;
+    for (int q = 0; q < 14; ++q) out[q] = 0.0;
     out[0] = bie::tree::check_coverage(T, S, ia);
     out[1] = double(T.nodes.size());
     out[2] = double(S.nodes.size());
@@ -1239,6 +1239,29 @@ int bie_tree_check(int64_t nt, const double* targ, int64_t ns, const double* src
     }
     out[8] = evals;
     out[9] = double(nt) * double(ns);
+    int64_t lmin = nt, lmax = 0, capped = 0, broken = 0;
+    for (const bie::tree::Tree* tr : {&T, &S})
+      for (const auto& nd : tr->nodes) {
+        capped += nd.capped ? 1 : 0;
+        if (nd.nchild == 0) continue;
+        // children are contiguous and tile the parent's range in order
+        int64_t pos = nd.b;
+        for (int c = 0; c < nd.nchild; ++c) {
+          const auto& ch = tr->nodes[nd.child0 + c];
+          if (ch.b != pos || ch.parent < 0 || &tr->nodes[ch.parent] != &nd) ++broken;
+          pos = ch.e;
+        }
+        if (pos != nd.e) ++broken;
+      }
+    for (const auto& nd : T.nodes)
+      if (nd.nchild == 0) {
+        lmin = std::min<int64_t>(lmin, nd.n());
+        lmax = std::max<int64_t>(lmax, nd.n());
+      }
+    out[10] = double(lmin);
+    out[11] = double(lmax);
+    out[12] = double(capped);
+    out[13] = double(broken);
     return int(bie::kOk);
   });
 }

@@ -377,10 +377,12 @@ int bie_plan_get_far_method(void* plan, int64_t iprec, double* out);
 /* Host-only check of the hierarchical far field's lists: builds the target
  * tree (leaves <= leaf_t points) and source tree (<= leaf_s) of the points
  * targ[3 nt] and src[3 ns] (xyz per point), the proxy grids for (theta, p,
- * wavenumber k) and the dual traversal.  out[10] = number of (target leaf,
+ * wavenumber k) and the dual traversal.  out[14] = number of (target leaf,
  * source leaf) pairs not covered exactly once (0 when correct), target
  * nodes, source nodes, interactions by form (5), kernel evaluations of the
- * lists, ntarg * nsrc.  No GPU is used. */
+ * lists, ntarg * nsrc, smallest and largest target leaf, nodes of either
+ * tree whose grid the caps could not hold, nodes whose point range is not
+ * the union of its children's (0 when correct).  No GPU is used. */
 int bie_tree_check(int64_t nt, const double* targ, int64_t ns, const double* src, double theta,
                    int64_t p, double k, int64_t leaf_t, int64_t leaf_s, double* out);
 

@@ -12,7 +12,7 @@ from fmm3dbie_b200 import _lib as L
 def _check(t, s, theta=0.5, p=8, k=0.0, leaf_t=128, leaf_s=256):
     t = np.ascontiguousarray(t, float)
     s = np.ascontiguousarray(s, float)
-    out = np.zeros(10)
+    out = np.zeros(14)
     st = L.lib().bie_tree_check(len(t), L.ptr(t), len(s), L.ptr(s), theta, p, k, leaf_t, leaf_s,
                                 L.ptr(out))
     assert st == 0
@@ -30,8 +30,10 @@ def _ellipsoid(rng, n):
 def test_coverage_surface(theta, p, k):
     rng = np.random.default_rng(1)
     out = _check(_ellipsoid(rng, 6000), _ellipsoid(rng, 9000), theta, p, k)
-    assert out[0] == 0
+    assert out[0] == 0 and out[13] == 0
     assert out[3:8].sum() > 0
+    # k-d splits at multiples of 32 near the median: target leaves of 64..128
+    assert 64 <= out[10] and out[11] <= 128
 
 
 def test_coverage_volume_and_small_leaves():
@@ -71,5 +73,6 @@ def test_high_frequency_splits_capped_nodes():
     lo = _check(t, s, 0.5, 10, 2.0)
     hi = _check(t, s, 0.5, 10, 40.0)
     assert lo[0] == 0 and hi[0] == 0
+    assert hi[12] > lo[12]  # more nodes too large for an accurate grid
     print(f"\nkernel evaluations of the lists: k = 2 {lo[8] / lo[9]:.3f}, k = 40 {hi[8] / hi[9]:.3f}")
     assert lo[8] < lo[9] and hi[8] <= hi[9]
