@@ -4,7 +4,7 @@
 
 The node tables for triangular patches are parsed from a reference checkout
 (DIR/src/tria_routs/koorn-*.txt) into fmm3dbie_b200/_data/ when they are not
-there yet; see tables.py.
+there yet (see tables.py); DIR comes from --reference or FMM3DBIE_REFERENCE.
 """
 from __future__ import annotations
 
@@ -56,9 +56,13 @@ def _run(cmd):
 def build(force: bool = False, reference: str | None = None, verbose: bool = False) -> str:
     from . import tables
     if not os.path.exists(tables.TABLE_PATH):
-        ref = reference or os.environ.get("FMM3DBIE_REFERENCE", "/root/reference")
-        if os.path.isdir(ref):
-            tables.generate(ref)
+        ref = reference or os.environ.get("FMM3DBIE_REFERENCE")
+        if not ref or not os.path.isdir(ref):
+            raise RuntimeError(
+                f"{tables.TABLE_PATH} is missing and no reference checkout was given to parse "
+                "the Vioreanu-Rokhlin node tables from: pass --reference DIR or set "
+                "FMM3DBIE_REFERENCE")
+        tables.generate(ref)
     os.makedirs(BUILD, exist_ok=True)
     deps = _headers()
     jobs = []

@@ -15,21 +15,32 @@
 // Limits and sharing rules:
 //  * the scratch is kNoAllocScratchBytes (48 MiB) of device memory that every
 //    GPU which loads this code keeps until the process exits;
-//  * ns <= kNoAllocMaxSources (1,048,576) sources, and nt <= 1,048,576
-//    targets (more targets than that leave no room for a single chunk of
-//    partial sums); larger calls are rejected with BIE_ERR_ARG and a message;
+//  * it always evaluates the direct sum (FP64 or FP32 pair sums, as iprec
+//    says): BIE_FAR_METHOD and BIE_TREE_PAIRS, which switch
+//    bie_farfield_dev to the hierarchical sum for large calls, are ignored;
+//  * ns <= kNoAllocMaxSources (1,048,576) sources, and at most 1,048,576
+//    targets for Helmholtz (kind 1) or 2,097,152 for Laplace (kind 0): one
+//    chunk of partial sums (one complex or real value per target) must fit
+//    in the 16 MiB left after the strengths; larger calls are rejected with
+//    BIE_ERR_ARG and a message;
 //  * all calls share the one array: two calls whose work overlaps on the GPU
 //    (different streams, or different host threads on the same device) race
 //    on it and give wrong results -- order them on one stream or serialise
 //    them;
 //  * the first call on each device looks up the array's device address with
 //    cudaGetSymbolAddress (with that device current) and caches it; make
-//    that first call before any stream capture begins on that device;
+//    that first call before any stream capture begins on that device.  The
+//    cached address belongs to the device's primary context: after
+//    cudaDeviceReset (or anything else that destroys that context) it is
+//    stale, and the process must not call this entry point on that device
+//    again;
 //  * nothing in the scratch needs to start at zero: each call writes every
 //    strength and every partial sum it later reads, so the contents left by
 //    the previous call are never used.
 #include <algorithm>
+#include <exception>
 #include <mutex>
+#include <new>
 #include <string>
 
 #include "../../../include/fmm3dbie_b200.h"
@@ -74,11 +85,12 @@ int scratch_address(int device, void** out) {
 
 }  // namespace
 
-extern "C" int bie_farfield_dev_noalloc(int64_t kind, const double* zk, int64_t ns,
-                                        const double* src_dev, const double* nrm_dev,
-                                        const double* charge_dev, const double* dipstr_dev,
-                                        int64_t nt, const double* targ_dev, double thresh,
-                                        int64_t iprec, double* pot_dev, void* stream) {
+namespace {
+
+int farfield_noalloc(int64_t kind, const double* zk, int64_t ns, const double* src_dev,
+                     const double* nrm_dev, const double* charge_dev, const double* dipstr_dev,
+                     int64_t nt, const double* targ_dev, double thresh, int64_t iprec,
+                     double* pot_dev, void* stream) {
   if ((kind != 0 && kind != 1) || (iprec != 0 && iprec != 1) || ns < 0 || nt < 0) {
     bie::set_last_error("bie_farfield_dev_noalloc: bad kind/iprec/sizes");
     return BIE_ERR_ARG;
@@ -104,7 +116,11 @@ extern "C" int bie_farfield_dev_noalloc(int64_t kind, const double* zk, int64_t 
     bie::set_last_error(cudaGetErrorString(e));
     return BIE_ERR_CUDA;
   }
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) {
+    bie::set_last_error(cudaGetErrorString(e));
+    return BIE_ERR_CUDA;
+  }
   void* base = nullptr;
   int ier = scratch_address(device, &base);
   if (ier) return ier;
@@ -148,4 +164,27 @@ extern "C" int bie_farfield_dev_noalloc(int64_t kind, const double* zk, int64_t 
     return BIE_ERR_CUDA;
   }
   return BIE_OK;
+}
+
+}  // namespace
+
+// The C-ABI entry: no exception (a failed string or lock operation) leaves
+// through it; those become an error status like every other failure.
+extern "C" int bie_farfield_dev_noalloc(int64_t kind, const double* zk, int64_t ns,
+                                        const double* src_dev, const double* nrm_dev,
+                                        const double* charge_dev, const double* dipstr_dev,
+                                        int64_t nt, const double* targ_dev, double thresh,
+                                        int64_t iprec, double* pot_dev, void* stream) {
+  try {
+    return farfield_noalloc(kind, zk, ns, src_dev, nrm_dev, charge_dev, dipstr_dev, nt, targ_dev,
+                            thresh, iprec, pot_dev, stream);
+  } catch (const std::bad_alloc&) {
+    bie::set_last_error("bie_farfield_dev_noalloc: host allocation failed");
+    return BIE_ERR_NOMEM;
+  } catch (const std::exception& ex) {
+    bie::set_last_error(ex.what());
+    return BIE_ERR_ARG;
+  } catch (...) {
+    return BIE_ERR_ARG;
+  }
 }

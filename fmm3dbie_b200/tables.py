@@ -109,5 +109,8 @@ def generate(reference_root: str, path: str = TABLE_PATH) -> str:
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FMM3DBIE_REFERENCE")
+    if not root:
+        sys.exit("usage: python -m fmm3dbie_b200.tables REFERENCE_DIR "
+                 "(or set FMM3DBIE_REFERENCE to a reference checkout)")
     print(generate(root))

@@ -406,16 +406,20 @@ int bie_farfield_dev(int64_t kind, const double* zk, int64_t ns, const double* s
                      const double* nrm_dev, const double* charge_dev, const double* dipstr_dev,
                      int64_t nt, const double* targ_dev, double thresh, int64_t iprec,
                      double* pot_dev, void* stream);
-/* Same sum as bie_farfield_dev, allocating nothing: for callers that cannot
- * allocate device memory at this point (their memory belongs to their own
- * pool or to a budget fixed at start-up, or a cudaMalloc/cudaFree here would
- * stall their other streams).  No counterpart in the reference.  Its scratch
- * is a fixed 48 MiB array inside the library that every GPU loading the
- * library keeps until exit; ns <= 1,048,576 and nt <= 1,048,576, larger
- * calls return BIE_ERR_ARG.  All calls share that array: calls that overlap
- * on the GPU race and must be ordered (one stream) by the caller.  The first
- * call on a device resolves the array's address and should come before any
- * stream capture on that device.  Returns without synchronising. */
+/* The direct far-field sum of bie_farfield_dev, allocating nothing: for
+ * callers that cannot allocate device memory at this point (their memory
+ * belongs to their own pool or to a budget fixed at start-up, or a
+ * cudaMalloc/cudaFree here would stall their other streams).  No counterpart
+ * in the reference.  It always evaluates the direct sum and ignores
+ * BIE_FAR_METHOD / BIE_TREE_PAIRS (bie_farfield_dev may switch to the
+ * hierarchical sum from ns * nt >= 1.5e10 on).  Its scratch is a fixed
+ * 48 MiB array inside the library that every GPU loading the library keeps
+ * until exit; ns <= 1,048,576, nt <= 1,048,576 (Helmholtz) or 2,097,152
+ * (Laplace), larger calls return BIE_ERR_ARG.  All calls share that array:
+ * calls that overlap on the GPU race and must be ordered (one stream) by the
+ * caller.  The first call on a device resolves the array's address and should
+ * come before any stream capture on that device; the address is not valid
+ * after cudaDeviceReset.  Returns without synchronising. */
 int bie_farfield_dev_noalloc(int64_t kind, const double* zk, int64_t ns, const double* src_dev,
                              const double* nrm_dev, const double* charge_dev,
                              const double* dipstr_dev, int64_t nt, const double* targ_dev,

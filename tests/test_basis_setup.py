@@ -168,8 +168,13 @@ def test_go3_roundtrip(tmp_path, sphere4):
 
 
 def test_reference_go3_mesh_if_present(built):
+    """Reads a mesh shipped with the reference (geometries/sphere_192_o03.go3)
+    when FMM3DBIE_REFERENCE names a reference checkout."""
     import os
-    path = "/root/reference/geometries/sphere_192_o03.go3"
+    root = os.environ.get("FMM3DBIE_REFERENCE")
+    if not root:
+        pytest.skip("FMM3DBIE_REFERENCE is not set")
+    path = os.path.join(root, "geometries", "sphere_192_o03.go3")
     if not os.path.exists(path):
         pytest.skip("reference geometry not present")
     s = S.read_go3(path)
