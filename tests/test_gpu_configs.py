@@ -1,0 +1,227 @@
+"""GPU parity against the FP64 oracle on the five workload configurations, at
+the sizes the workloads name (reduced only where stated):
+
+* the Helmholtz ellipsoid (1,2,3), 1280 order-6 patches, npts 35,840, zk 2,
+  zpars (2, -2i, 1), eps 1e-7: FP64 and FP32 matvecs against oracle.lpcomp;
+  the mixed-precision solve to FP64 residual 1e-10 checked by the oracle's
+  operator and by the analytic exterior field at 100 seeded points on the
+  radius-5 sphere (examples/helmholtz/helm_dir_iter_example.f);
+* the same surface at zk 5 with 64 plane-wave right-hand sides: several
+  columns of the multi-density matvec (FP64, FP32 CUDA-core and FP32
+  tensor-core far fields) against the oracle, and the batched mixed solve;
+* an order-8 ellipsoid of the uneven batch (Laplace and Helmholtz);
+* the quad torus (iptype 11, 6 x 6 Gauss-Legendre nodes), reduced to 32 x 16
+  patches, at k = 8 (the top of the warm-start wavenumber range).
+
+The oracle (oracle.lpcomp: lpcomp_*_comb_dir_addsub restated, exact direct
+far-field sum) takes the same surface, near quadrature and oversampling as
+the device plan.  Tolerances (w-weighted relative L2): FP64 1e-12; FP32 as
+stated per case, next to the eps of the configuration.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from fmm3dbie_b200 import Plan
+from fmm3dbie_b200 import surface as S
+from conftest import wnorm
+
+pytestmark = pytest.mark.gpu
+
+X0 = np.array([0.1, -0.2, 0.3])
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+def _rel(w, a, b):
+    return wnorm(w, a - b) / wnorm(w, b)
+
+
+def _exterior_field(s, soln, zp, targ):
+    """Smooth-rule potential (alpha S + beta D) soln at far targets."""
+    k = zp[0]
+    w = s.qwts()
+    out = np.zeros(len(targ), complex)
+    for i, t in enumerate(targ):
+        dx = t[None, :] - s.xyz
+        r = np.linalg.norm(dx, axis=1)
+        dn = np.sum(dx * s.normals, 1)
+        ker = (zp[1] / r + zp[2] * dn * (1 - 1j * k * r) / r ** 3) * np.exp(1j * k * r) / (4 * np.pi)
+        out[i] = np.sum(ker * w * soln)
+    return out
+
+
+def _sphere_targets(n, radius, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n, 3))
+    return radius * v / np.linalg.norm(v, axis=1)[:, None]
+
+
+@pytest.fixture(scope="module")
+def ellipsoid_full(torch):
+    return S.icosa_ellipsoid(3, 6, (1.0, 2.0, 3.0))
+
+
+@pytest.fixture(scope="module")
+def helm2(ellipsoid_full):
+    zp = (2.0, -2.0j, 1.0)
+    st = S.setup(ellipsoid_full, 1, 1e-7, zp)
+    P = Plan(1, zp, ellipsoid_full, st.near, st.over)
+    yield zp, st, P
+    P.close()
+
+
+def test_headline_surface_matvec(torch, ellipsoid_full, helm2):
+    s = ellipsoid_full
+    zp, st, P = helm2
+    assert s.npts == 35840 and P.nptso > 60000
+    rng = np.random.default_rng(2)
+    sigma = rng.normal(size=s.npts) + 1j * rng.normal(size=s.npts)
+    ref = oracle.lpcomp(1, s, zp, st.near, st.over, sigma)
+    x = torch.tensor(sigma, device="cuda")
+    w = s.qwts()
+    e64 = _rel(w, P.matvec(x, 0).cpu().numpy(), ref)
+    e32 = _rel(w, P.matvec(x, 1).cpu().numpy(), ref)
+    print(f"\nellipsoid 35840, zk 2: FP64 {e64:.2e}, FP32 {e32:.2e} (eps 1e-7)")
+    assert e64 < 1e-12
+    assert e32 < 2e-7
+
+
+def test_headline_mixed_solve(torch, ellipsoid_full, helm2):
+    """The timed solve of the benchmark: mixed precision to FP64 residual
+    1e-10; its residual under the oracle's operator and its exterior field
+    against the analytic point-source field."""
+    s = ellipsoid_full
+    zp, st, P = helm2
+    r = np.linalg.norm(s.xyz - X0, axis=1)
+    rhs = np.exp(2j * r) / (4 * np.pi * r)
+    x, info = P.solve(torch.tensor(rhs, device="cuda"), 0.5, mode=1, numit=300, eps_gmres=1e-10)
+    assert info["status"] == 0 and info["rres"][0] <= 1e-10
+    xs = x.cpu().numpy()
+    w = s.qwts()
+    res = rhs - (0.5 * xs + oracle.lpcomp(1, s, zp, st.near, st.over, xs))
+    rres_oracle = wnorm(w, res) / wnorm(w, rhs)
+    targ = _sphere_targets(100, 5.0, 2)
+    u = _exterior_field(s, xs, zp, targ)
+    d = np.linalg.norm(targ - X0, axis=1)
+    uex = np.exp(2j * d) / (4 * np.pi * d)
+    e_ext = float(np.max(np.abs(u - uex)) / np.max(np.abs(uex)))
+    print(f"\nmixed solve: rres {info['rres'][0]:.2e}, oracle residual {rres_oracle:.2e}, "
+          f"exterior field error {e_ext:.2e}")
+    assert rres_oracle < 2e-10
+    assert e_ext < 1e-6
+
+
+@pytest.fixture(scope="module")
+def helm5(ellipsoid_full):
+    zk = 5.0
+    zp = (zk, -1j * zk, 1.0)
+    s = ellipsoid_full
+    st = S.setup(s, 1, 1e-7, zp)
+    rng = np.random.default_rng(3)
+    d = rng.normal(size=(64, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    rhs = -np.exp(1j * zk * (s.xyz @ d.T))
+    P = Plan(1, zp, s, st.near, st.over)
+    yield zp, st, P, np.ascontiguousarray(rhs)
+    P.close()
+
+
+def test_plane_waves_multi_density_matvec(torch, ellipsoid_full, helm5):
+    """64 densities in one matvec (FP64; FP32 on CUDA cores and on the tensor
+    cores) against the oracle column by column."""
+    s = ellipsoid_full
+    zp, st, P, rhs = helm5
+    rng = np.random.default_rng(30)
+    sig = rhs * (1 + 0.3 * rng.normal(size=rhs.shape))       # 64 plane-wave-like densities
+    X = torch.tensor(sig, device="cuda")
+    w = s.qwts()
+    y64 = P.matvec(X, 0).cpu().numpy()
+    P.set_far(1, 64, 0, 2)
+    ysimt = P.matvec(X, 1).cpu().numpy()
+    P.set_far(1, 64, 4, 1)
+    ytc = P.matvec(X, 1).cpu().numpy()
+    torch.cuda.synchronize()
+    assert P.get_far(1, 64)[2] == 0, "tensor-core completion wait timed out"
+    for m in (0, 31, 63):
+        ref = oracle.lpcomp(1, s, zp, st.near, st.over, sig[:, m])
+        e64, es, et = (_rel(w, y[:, m], ref) for y in (y64, ysimt, ytc))
+        print(f"\nzk 5 density {m}: FP64 {e64:.2e}, FP32 CUDA cores {es:.2e}, "
+              f"FP32 tensor cores {et:.2e}")
+        assert e64 < 1e-12
+        assert es < 3e-7
+        assert et < 1e-6
+
+
+def test_plane_waves_batched_solve(torch, ellipsoid_full, helm5):
+    s = ellipsoid_full
+    zp, st, P, rhs = helm5
+    R = torch.tensor(rhs, device="cuda")
+    X, info = P.solve(R, 0.5, mode=1, numit=300, eps_gmres=1e-10)
+    assert info["status"] == 0 and np.all(info["rres"] <= 1e-10)
+    w = s.qwts()
+    for m in (5, 47):
+        xs = X[:, m].cpu().numpy()
+        res = rhs[:, m] - (0.5 * xs + oracle.lpcomp(1, s, zp, st.near, st.over, xs))
+        rr = wnorm(w, res) / wnorm(w, rhs[:, m])
+        print(f"\nzk 5 batched mixed solve, system {m}: oracle residual {rr:.2e}")
+        assert rr < 2e-10
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_order8_uneven_surface(torch, kind):
+    from fmm3dbie_b200.batch import uneven_ellipsoids
+    items, rhs, _ = uneven_ellipsoids(kind)
+    cand = [(it.surf.npts, q) for q, it in enumerate(items)
+            if int(it.surf.norders[0]) == 8 and it.surf.npts <= 15000]
+    assert cand, "the uneven batch has no order-8 surface of <= 320 patches"
+    it = items[max(cand)[1]]          # a 320-patch order-8 surface (14,400 nodes)
+    s = it.surf
+    st = S.setup(s, kind, 1e-7, it.params)
+    P = Plan(kind, it.params, s, st.near, st.over)
+    rng = np.random.default_rng(40 + kind)
+    sigma = rng.normal(size=s.npts) if kind == 0 else rng.normal(size=s.npts) + 1j * rng.normal(size=s.npts)
+    ref = oracle.lpcomp(kind, s, it.params, st.near, st.over, sigma)
+    x = torch.tensor(sigma, device="cuda")
+    w = s.qwts()
+    e64 = _rel(w, P.matvec(x, 0).cpu().numpy(), ref)
+    e32 = _rel(w, P.matvec(x, 1).cpu().numpy(), ref)
+    print(f"\norder-8 ellipsoid npts {s.npts} kind {kind} params {it.params}: FP64 {e64:.2e}, "
+          f"FP32 {e32:.2e}")
+    P.close()
+    assert e64 < 1e-12
+    assert e32 < 3e-7
+
+
+def test_quad_torus_k8(torch):
+    from fmm3dbie_b200.warmstart import torus_surface
+    s = torus_surface(32, 16, 5)
+    assert np.all(s.iptype == 11) and s.npts == 32 * 16 * 36
+    zk = 8.0
+    zp = (zk, -1j * zk, 1.0)
+    st = S.setup(s, 1, 1e-7, zp)
+    P = Plan(1, zp, s, st.near, st.over)
+    rng = np.random.default_rng(5)
+    d = rng.normal(size=3)
+    d /= np.linalg.norm(d)
+    rhs = -np.exp(1j * zk * (s.xyz @ d))
+    w = s.qwts()
+    x = torch.tensor(rhs, device="cuda")
+    ref = oracle.lpcomp(1, s, zp, st.near, st.over, rhs)
+    e64 = _rel(w, P.matvec(x, 0).cpu().numpy(), ref)
+    e32 = _rel(w, P.matvec(x, 1).cpu().numpy(), ref)
+    X, info = P.solve(x, 0.5, mode=1, numit=400, eps_gmres=1e-10)
+    xs = X.cpu().numpy()
+    res = rhs - (0.5 * xs + oracle.lpcomp(1, s, zp, st.near, st.over, xs))
+    rr = wnorm(w, res) / wnorm(w, rhs)
+    print(f"\ntorus 32x16 quads, k 8: FP64 {e64:.2e}, FP32 {e32:.2e}; mixed solve rres "
+          f"{info['rres'][0]:.2e}, oracle residual {rr:.2e}, FP32/FP64 matvecs "
+          f"{info['fp32_matvecs']}/{info['fp64_matvecs']}")
+    P.close()
+    assert e64 < 1e-12
+    assert e32 < 1e-6
+    assert info["status"] == 0 and rr < 2e-10
