@@ -23,65 +23,55 @@ inline double norm3(const double* a) { return std::sqrt(a[0] * a[0] + a[1] * a[1
 using V3 = std::array<double, 3>;
 using Tri = std::array<V3, 3>;
 
-// Regular icosahedron with vertices on the unit sphere; faces oriented so
-// that (v1-v0)x(v2-v0) points outward.
+// The icosahedron of xtri_rsolid (itype 4, xtri_parameterizations.f90:1674-1829):
+// a ring of five vertices at angles 2 pi i / 5 lifted to the height that
+// makes the apex (0, 0, d) equidistant, the apex, and the point reflections
+// of those six; faces in the reference's order and orientation, so that
+// (v1-v0)x(v2-v0) points outward; vertices scaled to the unit sphere.
 std::vector<Tri> icosahedron() {
-  const double phi = 0.5 * (1.0 + std::sqrt(5.0));
-  std::vector<V3> v;
-  for (int s1 : {-1, 1})
-    for (int s2 : {-1, 1}) {
-      v.push_back({0.0, double(s1), s2 * phi});
-      v.push_back({double(s1), s2 * phi, 0.0});
-      v.push_back({s2 * phi, 0.0, double(s1)});
-    }
-  for (auto& p : v) {
-    const double r = norm3(p.data());
-    for (auto& c : p) c /= r;
+  const double pi = 4.0 * std::atan(1.0);
+  std::array<V3, 12> v{};
+  for (int i = 0; i < 5; ++i) v[i] = {std::cos(2 * pi * (i + 1) / 5.0), std::sin(2 * pi * (i + 1) / 5.0), 0.0};
+  const double edge = std::hypot(v[1][0] - v[0][0], v[1][1] - v[0][1]);
+  const double apex = std::sqrt(edge * edge - 1.0);
+  v[5] = {0.0, 0.0, apex};
+  const double lift = (1.0 - apex * apex) / (2.0 * apex);
+  for (int i = 0; i < 6; ++i) {
+    v[i][2] += lift;
+    v[i + 6] = {-v[i][0], -v[i][1], -v[i][2]};
   }
-  auto d2 = [&](int a, int b) {
-    double s = 0;
-    for (int k = 0; k < 3; ++k) s += (v[a][k] - v[b][k]) * (v[a][k] - v[b][k]);
-    return s;
-  };
-  double emin = 1e30;
-  for (int a = 0; a < 12; ++a)
-    for (int b = a + 1; b < 12; ++b) emin = std::min(emin, d2(a, b));
+  const double scale = 1.0 / norm3(v[0].data());
+  for (auto& p : v)
+    for (auto& c : p) c *= scale;
+  static const int faces[20][3] = {{0, 1, 5},  {1, 2, 5}, {2, 3, 5},  {3, 4, 5},  {4, 0, 5},
+                                   {7, 6, 11}, {8, 7, 11}, {9, 8, 11}, {10, 9, 11}, {6, 10, 11},
+                                   {1, 0, 9},  {2, 1, 10}, {3, 2, 6},  {4, 3, 7},  {0, 4, 8},
+                                   {7, 8, 4},  {8, 9, 0},  {9, 10, 1}, {10, 6, 2}, {6, 7, 3}};
   std::vector<Tri> out;
-  for (int a = 0; a < 12; ++a)
-    for (int b = a + 1; b < 12; ++b)
-      for (int c = b + 1; c < 12; ++c) {
-        if (d2(a, b) > emin * 1.01 || d2(b, c) > emin * 1.01 || d2(a, c) > emin * 1.01) continue;
-        Tri t{v[a], v[b], v[c]};
-        double e1[3], e2[3], n[3];
-        for (int k = 0; k < 3; ++k) {
-          e1[k] = t[1][k] - t[0][k];
-          e2[k] = t[2][k] - t[0][k];
-        }
-        cross3(e1, e2, n);
-        const double dot = n[0] * (t[0][0] + t[1][0] + t[2][0]) + n[1] * (t[0][1] + t[1][1] + t[2][1]) +
-                           n[2] * (t[0][2] + t[1][2] + t[2][2]);
-        if (dot < 0) std::swap(t[1], t[2]);
-        out.push_back(t);
-      }
+  for (const auto& f : faces) out.push_back({v[f[0]], v[f[1]], v[f[2]]});
   return out;
 }
 
-// Flat 4-way refinement: children (v0,m01,m20), (m01,v1,m12), (m20,m12,v2),
-// (m01,m12,m20), all keeping the parent orientation.
+// Flat 4-way refinement in xtri_platonic's order (xtri_parameterizations.f90:
+// 1335-1413, xtri_refine4_flat :1864-1949): triangle i becomes its corner
+// child (v0, m01, m02) in place and the other three children
+// (m12, m02, m01), (m01, v1, m12), (m02, m12, v2) are appended, so patch
+// numbering matches the reference's at every level.
 std::vector<Tri> refine4(const std::vector<Tri>& in) {
-  std::vector<Tri> out;
+  std::vector<Tri> out(in);
   out.reserve(in.size() * 4);
-  for (const auto& t : in) {
-    V3 m01, m12, m20;
+  for (size_t i = 0; i < in.size(); ++i) {
+    const Tri& t = in[i];
+    V3 m01, m12, m02;
     for (int k = 0; k < 3; ++k) {
       m01[k] = 0.5 * (t[0][k] + t[1][k]);
       m12[k] = 0.5 * (t[1][k] + t[2][k]);
-      m20[k] = 0.5 * (t[2][k] + t[0][k]);
+      m02[k] = 0.5 * (t[0][k] + t[2][k]);
     }
-    out.push_back({t[0], m01, m20});
+    out[i] = {t[0], m01, m02};
+    out.push_back({m12, m02, m01});
     out.push_back({m01, t[1], m12});
-    out.push_back({m20, m12, t[2]});
-    out.push_back({m01, m12, m20});
+    out.push_back({m02, m12, t[2]});
   }
   return out;
 }

@@ -26,20 +26,19 @@
  * tests (sphere spectra of S and D, Green's identity, point-source solves)
  * evaluated in tests/.
  */
-#include <complex.h>
-#include <math.h>
-#include <stdint.h>
-#include <stdlib.h>
-#include <string.h>
-
-#define OVER4PI 0.07957747154594767
+#include "oracle_common.h"
 
 /* ---------------- node tables -------------------------------------------- */
-static double* g_vr_uvs[21];
-static int64_t g_vr_np[21];
+double* g_vr_uvs[21];
+double* g_vr_wts[21];
+int64_t g_vr_np[21];
+double g_koorn_abc[KOORN_NMAX + 1][KOORN_NMAX + 1][3];
+double g_koorn_sc[KOORN_NMAX + 1][KOORN_NMAX + 1];
+int g_koorn_ready;
 
 int oracle_set_vr_nodes(int64_t norder, int64_t npols, const double* uvs) {
   if (norder < 0 || norder > 20 || npols != (norder + 1) * (norder + 2) / 2) return 1;
+  koorn_init();
   free(g_vr_uvs[norder]);
   g_vr_uvs[norder] = (double*)malloc(sizeof(double) * 2 * npols);
   memcpy(g_vr_uvs[norder], uvs, sizeof(double) * 2 * npols);
@@ -47,126 +46,14 @@ int oracle_set_vr_nodes(int64_t norder, int64_t npols, const double* uvs) {
   return 0;
 }
 
-static int64_t npols_of(int64_t iptype, int64_t norder) {
-  if (iptype == 1) return (norder + 1) * (norder + 2) / 2;
-  return (norder + 1) * (norder + 1);
-}
-
-/* koorn_pols, koornexps.f90:206-330 (same recurrences and scaling) */
-static void koorn_pols(const double* uv, int64_t nmax, double* pols) {
-  double legpols[64], jacpols[64][64];
-  const double u = uv[0], v = uv[1];
-  const double z = 2 * u + v - 1, y = 1 - v;
-  legpols[0] = 1;
-  legpols[1] = z;
-  for (int64_t k = 1; k <= nmax; ++k)
-    legpols[k + 1] = ((2 * k + 1) * z * legpols[k] - k * legpols[k - 1] * y * y) / (k + 1);
-  const double x = 1 - 2 * v;
-  for (int64_t k = 0; k <= nmax; ++k) {
-    const double beta = 2 * k + 1;
-    jacpols[0][k] = 1;
-    jacpols[1][k] = (-beta + (2 + beta) * x) / 2;
-    for (int64_t n = 1; n <= nmax - k - 1; ++n) {
-      const double an = (2 * n + beta + 1) * (2 * n + beta + 2) / 2 / (n + 1) / (n + beta + 1);
-      const double bn = (-beta * beta) * (2 * n + beta + 1) / 2 / (n + 1) / (n + beta + 1) / (2 * n + beta);
-      const double cn = n * (n + beta) * (2 * n + beta + 2) / (n + 1) / (n + beta + 1) / (2 * n + beta);
-      jacpols[n + 1][k] = (an * x + bn) * jacpols[n][k] - cn * jacpols[n - 1][k];
-    }
-  }
-  int64_t iii = 0;
-  for (int64_t n = 0; n <= nmax; ++n)
-    for (int64_t k = 0; k <= n; ++k) {
-      const double sc = sqrt(1.0 / (2 * k + 1) / (2 * n + 2));
-      pols[iii++] = legpols[k] * jacpols[n - k][k] / sc;
-    }
-}
-
-/* legepols: P_0..P_n */
-static void legepols(double x, int64_t n, double* p) {
-  p[0] = 1;
-  if (n >= 1) p[1] = x;
-  for (int64_t k = 1; k < n; ++k) p[k + 1] = ((2 * k + 1) * x * p[k] - k * p[k - 1]) / (k + 1);
-}
-
-/* Gauss-Legendre nodes (ascending), Newton on P_n */
-static void legendre_nodes(int64_t n, double* x) {
-  double p[128];
-  for (int64_t i = 0; i < n; ++i) {
-    double t = cos(M_PI * (i + 0.75) / (n + 0.5));
-    for (int it = 0; it < 100; ++it) {
-      legepols(t, n, p);
-      /* derivative from (1-t^2) P_n' = n (P_{n-1} - t P_n) */
-      const double dp = n * (p[n - 1] - t * p[n]) / (1 - t * t);
-      const double d = p[n] / dp;
-      t -= d;
-      if (fabs(d) < 1e-16) break;
-    }
-    x[n - 1 - i] = t;
-  }
-}
-
-static void basis_pols(int64_t iptype, int64_t norder, const double* uv, double* pols) {
-  if (iptype == 1) {
-    koorn_pols(uv, norder, pols);
-    return;
-  }
-  double px[64], py[64];
-  legepols(uv[0], norder, px);
-  legepols(uv[1], norder, py);
-  const int64_t n = norder + 1;
-  for (int64_t i = 0; i < n; ++i)
-    for (int64_t j = 0; j < n; ++j) pols[j + n * i] = px[j] * py[i];
-}
-
-static int disc_nodes(int64_t iptype, int64_t norder, double* uvs) {
-  if (iptype == 1) {
-    if (!g_vr_uvs[norder]) return 6;
-    memcpy(uvs, g_vr_uvs[norder], sizeof(double) * 2 * g_vr_np[norder]);
-    return 0;
-  }
-  if (iptype != 11) return 1;
-  const int64_t n = norder + 1;
-  double x[64];
-  legendre_nodes(n, x);
-  for (int64_t i = 0; i < n; ++i)
-    for (int64_t j = 0; j < n; ++j) {
-      uvs[2 * (j + n * i)] = x[j];
-      uvs[2 * (j + n * i) + 1] = x[i];
-    }
-  return 0;
-}
-
-/* dinverse via Gauss-Jordan with partial pivoting; a is overwritten */
-static int inverse(int64_t n, double* a, double* b) {
-  for (int64_t i = 0; i < n * n; ++i) b[i] = 0;
-  for (int64_t i = 0; i < n; ++i) b[i * n + i] = 1;
-  for (int64_t c = 0; c < n; ++c) {
-    int64_t piv = c;
-    for (int64_t r = c + 1; r < n; ++r)
-      if (fabs(a[r * n + c]) > fabs(a[piv * n + c])) piv = r;
-    if (a[piv * n + c] == 0) return 7;
-    for (int64_t j = 0; j < n; ++j) {
-      double t = a[c * n + j];
-      a[c * n + j] = a[piv * n + j];
-      a[piv * n + j] = t;
-      t = b[c * n + j];
-      b[c * n + j] = b[piv * n + j];
-      b[piv * n + j] = t;
-    }
-    const double inv = 1 / a[c * n + c];
-    for (int64_t j = 0; j < n; ++j) {
-      a[c * n + j] *= inv;
-      b[c * n + j] *= inv;
-    }
-    for (int64_t r = 0; r < n; ++r) {
-      if (r == c) continue;
-      const double f = a[r * n + c];
-      for (int64_t j = 0; j < n; ++j) {
-        a[r * n + j] -= f * a[c * n + j];
-        b[r * n + j] -= f * b[c * n + j];
-      }
-    }
-  }
+/* Nodes and weights of the Vioreanu-Rokhlin rule of one order
+ * (get_vioreanu_nodes / get_vioreanu_wts, koornexps.f90:57,90). */
+int oracle_set_vr_table(int64_t norder, int64_t npols, const double* uvs, const double* wts) {
+  const int ier = oracle_set_vr_nodes(norder, npols, uvs);
+  if (ier) return ier;
+  free(g_vr_wts[norder]);
+  g_vr_wts[norder] = (double*)malloc(sizeof(double) * npols);
+  memcpy(g_vr_wts[norder], wts, sizeof(double) * npols);
   return 0;
 }
 
@@ -309,6 +196,23 @@ int oracle_eval_addsub(int64_t kind, int64_t npatches, const int64_t* norders, c
   }
   const double thresh = oracle_fmm_thresh(nptso, srcover, 12, ntarg, targs, ndtarg);
   const double th2 = thresh * thresh;
+  /* far field: this file's scalar direct sum (method 0, the parity oracle)
+   * or oracle_far.c's vectorised direct sum / treecode (methods 1, 2: the
+   * timed stand-ins for the FMM) */
+  double* farpot = NULL;
+  if (oracle_get_far_method() != 0) {
+    double* cd = malloc(sizeof(double) * 4 * nptso);
+    for (int64_t s = 0; s < nptso; ++s) {
+      cd[2 * s] = creal(ch[s]) * OVER4PI;
+      cd[2 * s + 1] = cimag(ch[s]) * OVER4PI;
+      cd[2 * nptso + 2 * s] = creal(dp[s]) * OVER4PI;
+      cd[2 * nptso + 2 * s + 1] = cimag(dp[s]) * OVER4PI;
+    }
+    const double zz[2] = {creal(zk), cimag(zk)};
+    farpot = malloc(sizeof(double) * 2 * ntarg);
+    oracle_farfield(nptso, srcover, cd, cd + 2 * nptso, zz, thresh, ndtarg, ntarg, targs, farpot);
+    free(cd);
+  }
 #pragma omp parallel
   {
     int64_t* idx = malloc(sizeof(int64_t) * (nptso > 0 ? nptso : 1));
@@ -316,7 +220,8 @@ int oracle_eval_addsub(int64_t kind, int64_t npatches, const int64_t* norders, c
     for (int64_t i = 0; i < ntarg; ++i) {
       const double* t = targs + ndtarg * i;
       /* "FMM": every oversampled source */
-      double complex val = direct_one(t, nptso, NULL, srcover, ch, dp, zk, th2);
+      double complex val = farpot ? farpot[2 * i] + I * farpot[2 * i + 1]
+                                  : direct_one(t, nptso, NULL, srcover, ch, dp, zk, th2);
       /* near add: wnear . sigma */
       for (int64_t j = row_ptr[i] - 1; j < row_ptr[i + 1] - 1; ++j) {
         const int64_t jp = col_ind[j] - 1;
@@ -349,6 +254,7 @@ int oracle_eval_addsub(int64_t kind, int64_t npatches, const int64_t* norders, c
   free(sover);
   free(ch);
   free(dp);
+  free(farpot);
   return 0;
 }
 

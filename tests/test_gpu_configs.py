@@ -225,3 +225,49 @@ def test_quad_torus_k8(torch):
     assert e64 < 1e-12
     assert e32 < 1e-6
     assert info["status"] == 0 and rr < 2e-10
+
+
+def _independent(kind, params, eps, osurf, psurf):
+    """The oracle's pipeline (its surface, setup and near quadrature) and the
+    product's (device setup, device matvec) from the same surface
+    description."""
+    so = oracle.setup(osurf, kind, eps, params)
+    sp = S.setup(psurf, kind, eps, params)
+    P = Plan(kind, params, psurf, sp.near, sp.over)
+    rng = np.random.default_rng(77)
+    n = osurf.npts
+    sig = rng.normal(size=n) if kind == 0 else rng.normal(size=n) + 1j * rng.normal(size=n)
+    ref = oracle.lpcomp(kind, osurf, params, so.near, so.over, sig)
+    import torch
+    x = torch.tensor(sig, device="cuda")
+    w = oracle.qwts(osurf)
+    out = (_rel(w, P.matvec(x, 0).cpu().numpy(), ref), _rel(w, P.matvec(x, 1).cpu().numpy(), ref))
+    P.close()
+    return out
+
+
+def test_sphere_independent_pipeline(torch):
+    """Config 1 end to end: the oracle builds the 320-patch order-4 sphere,
+    its near list, far orders, oversampling and near quadrature itself; the
+    product builds its own on the device.  Laplace alpha = beta = 1, eps 1e-6."""
+    e64, e32 = _independent(0, (1.0, 1.0), 1e-6, oracle.icosa_ellipsoid(2, 4),
+                            S.icosa_sphere(2, 4))
+    print(f"\nsphere 4800, independent setups: FP64 {e64:.2e}, FP32 {e32:.2e} (eps 1e-6)")
+    assert e64 < 1e-6 and e32 < 1e-6
+
+
+def test_headline_independent_pipeline(torch):
+    """Config 2 end to end with independent setups (npts 35,840, eps 1e-7)."""
+    e64, e32 = _independent(1, (2.0, -2.0j, 1.0), 1e-7, oracle.icosa_ellipsoid(3, 6, (1.0, 2.0, 3.0)),
+                            S.icosa_ellipsoid(3, 6, (1.0, 2.0, 3.0)))
+    print(f"\nellipsoid 35840, independent setups: FP64 {e64:.2e}, FP32 {e32:.2e} (eps 1e-7)")
+    assert e64 < 1e-7 and e32 < 2e-7
+
+
+def test_torus_independent_pipeline(torch):
+    """Quad torus (32 x 16 patches, iptype 11) at k = 8 with independent setups."""
+    from fmm3dbie_b200.warmstart import torus_surface
+    e64, e32 = _independent(1, (8.0, -8.0j, 1.0), 1e-7, oracle.torus_quad(32, 16, 5),
+                            torus_surface(32, 16, 5))
+    print(f"\ntorus 18432 k 8, independent setups: FP64 {e64:.2e}, FP32 {e32:.2e} (eps 1e-7)")
+    assert e64 < 1e-6 and e32 < 1e-6
