@@ -197,6 +197,7 @@ class PlaneWaveProblem:
                                        device=self.device).contiguous()
         self.ks = [float(k) for k in ks]
         self.plans = {}
+        self.setups = {}      # host copies of each wavenumber's setup arrays
         self.setup_s = 0.0
         for k in self.ks:
             t = time.perf_counter()
@@ -204,7 +205,7 @@ class PlaneWaveProblem:
             st = setup(surf, 1, eps, zp)
             self.setup_s += time.perf_counter() - t
             self.plans[k] = Plan(1, zp, surf, st.near, st.over)
-            del st
+            self.setups[k] = st
 
     def close(self):
         for p in self.plans.values():

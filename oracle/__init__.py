@@ -464,3 +464,83 @@ def setup(s, kind, eps, params, targs=None, ipatch_id=None, uvs_targ=None) -> OS
                              iquad)
     return OSetup(ONear(row_ptr, col_ind, iquad, wnear), OOver(novers, ixyzso, srcover, wover),
                   rfac, rfac0, cms, rads, nev)
+
+
+class GmresSolver:
+    """zgmres_guru / dgmres_guru (src/common/gmres_routs.f90:13-375) one
+    Arnoldi step at a time, with the oracle's matvec: (zid I + K) x = rhs,
+    unrestarted, modified Gram-Schmidt in the w-weighted inner product,
+    Givens rotations (rotmat_gmres.f:15-100), stop when the recurrence
+    residual |s_{m+1}|/||rhs|| <= eps_gmres; finish() back-substitutes and
+    takes the true residual with one more matvec, as the reference does.
+    The same algorithm as oracle_gmres in oracle.c, stepwise so that a
+    caller can time its iterations."""
+
+    def __init__(self, kind, surf, params, near, over, zid, rhs, numit=200, eps_gmres=1e-10,
+                 wts=None):
+        self.kind, self.surf, self.params, self.near, self.over = kind, surf, params, near, over
+        self.zid = complex(zid)
+        self.w = qwts(surf) if wts is None else wts
+        self.rhs = np.asarray(rhs, complex)
+        self.numit, self.eps = numit, eps_gmres
+        self.rb = float(np.sqrt(np.sum(self.w * np.abs(self.rhs) ** 2)))
+        self.V = [self.rhs / self.rb]
+        self.H = np.zeros((numit + 1, numit), complex)
+        self.cs = np.zeros(numit, complex)
+        self.sn = np.zeros(numit, complex)
+        self.s = np.zeros(numit + 1, complex)
+        self.s[0] = self.rb
+        self.it = 0
+        self.errs = []
+        self.done = False
+
+    def _apply(self, x):
+        y = lpcomp(self.kind, self.surf, self.params, self.near, self.over,
+                   x.real if self.kind == 0 else x)
+        return np.asarray(y, complex)
+
+    def step(self) -> bool:
+        """One Arnoldi iteration; True once the residual test is met (or
+        numit is reached)."""
+        it = self.it
+        wv = self._apply(self.V[it])
+        for k in range(it + 1):
+            z = np.sum(wv * np.conj(self.V[k]) * self.w)
+            self.H[k, it] = z
+            wv = wv - z * self.V[k]
+        self.H[it, it] += self.zid
+        wn = float(np.sqrt(np.sum(self.w * np.abs(wv) ** 2)))
+        self.V.append(wv / wn)
+        for k in range(it):
+            t = self.cs[k] * self.H[k, it] + np.conj(self.sn[k]) * self.H[k + 1, it]
+            self.H[k + 1, it] = -self.sn[k] * self.H[k, it] + self.cs[k] * self.H[k + 1, it]
+            self.H[k, it] = t
+        a, b = self.H[it, it], wn
+        if a == 0:
+            c, sgiv = 0.0, 1.0
+        else:
+            t = b / a
+            c = 1.0 / np.sqrt(1.0 + abs(t) ** 2)
+            sgiv = t * c
+        self.cs[it], self.sn[it] = c, sgiv
+        self.H[it, it] = c * self.H[it, it] + np.conj(sgiv) * wn
+        self.s[it + 1] = -sgiv * self.s[it]
+        self.s[it] = c * self.s[it]
+        err = abs(self.s[it + 1]) / self.rb
+        self.errs.append(err)
+        self.it += 1
+        self.done = err <= self.eps or self.it == self.numit
+        return self.done
+
+    def finish(self):
+        """Back-substitution, solution and true relative residual (one
+        matvec).  Returns (soln, niter, errs, rres)."""
+        m = self.it
+        y = np.zeros(m, complex)
+        for j in range(m - 1, -1, -1):
+            y[j] = (self.s[j] - np.dot(self.H[j, j + 1:m], y[j + 1:m])) / self.H[j, j]
+        x = sum(y[i] * self.V[i] for i in range(m))
+        r = self.zid * x + self._apply(x) - self.rhs
+        rres = float(np.sqrt(np.sum(self.w * np.abs(r) ** 2)) / self.rb)
+        soln = x.real if self.kind == 0 else x
+        return soln, m, np.array(self.errs), rres

@@ -119,3 +119,24 @@ def test_oracle_pipeline_known_answers(built):
     # Laplace eigenvalue 1/3 - 1/6 is the smaller one, so its relative error
     # is the larger)
     assert e_lap < 5e-6 and e_helm < 2e-6
+
+
+def test_stepwise_gmres_matches_oracle_gmres(built):
+    """The oracle's stepwise GMRES (timed by the benchmark's CPU legs) is
+    the oracle's C GMRES: same iterations, residuals and solution."""
+    s = oracle.icosa_ellipsoid(1, 4, (1.0, 2.0, 3.0))
+    zp = (2.0, -2.0j, 1.0)
+    st = oracle.setup(s, 1, 1e-6, zp)
+    r = np.linalg.norm(s.xyz - np.array([0.1, -0.2, 0.3]), axis=1)
+    rhs = np.exp(2j * r) / (4 * np.pi * r)
+    ref, nit, errs, rres, status = oracle.gmres(1, s, zp, st.near, st.over, 0.5, rhs, numit=60,
+                                                eps_gmres=1e-10)
+    g = oracle.GmresSolver(1, s, zp, st.near, st.over, 0.5, rhs, numit=60, eps_gmres=1e-10)
+    while not g.step():
+        pass
+    x, m, errs2, rres2 = g.finish()
+    assert status == 0 and m == nit
+    assert np.allclose(errs2, errs, rtol=1e-8, atol=0)
+    assert abs(rres2 - rres) <= 1e-3 * rres + 1e-15
+    w = oracle.qwts(s)
+    assert wnorm(w, x - ref) / wnorm(w, ref) < 1e-12
