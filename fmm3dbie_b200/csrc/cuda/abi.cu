@@ -1316,6 +1316,24 @@ int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
   });
 }
 
+int bie_set_mixed_residual(int64_t mode) {
+  if (mode != 0 && mode != 1) return BIE_ERR_ARG;
+  bie::set_mixed_residual_mode(int(mode));
+  return BIE_OK;
+}
+
+int bie_get_mixed_residual(void) { return bie::mixed_residual_mode(); }
+
+int bie_last_mixed_stats(double* out) {
+  if (!out) return BIE_ERR_ARG;
+  const bie::MixedOut& m = bie::last_mixed_out();
+  out[0] = m.fp64_matvecs;
+  out[1] = m.fp32_matvecs;
+  out[2] = m.incr_matvecs;
+  out[3] = m.max_incr_ratio;
+  return BIE_OK;
+}
+
 int bie_plan_timing(void* plan, int64_t enable, double* times) {
   if (!plan) return BIE_ERR_ARG;
   bie::Plan& P = *static_cast<bie::Plan*>(plan);

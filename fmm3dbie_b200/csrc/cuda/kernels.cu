@@ -11,6 +11,7 @@
 //   (c) combine   : pot_i = sum of far partials + sum_k W_eff(k) . sigma,
 //                   W_eff = wnear - smooth near part (folded once per plan,
 //                   replacing the per-call l3ddirectcdp/h3ddirectcdp subtraction).
+#include <cstdlib>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -462,7 +463,7 @@ constexpr int kCombineUnroll = 4;     // W_eff entries per lane in flight
 
 // Rows 8*bx .. 8*bx+7 (one warp each) of the near correction plus the far
 // partial sums.
-template <int CPLX, typename W>
+template <int CPLX, typename W, bool PAIRS = false>
 __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
                                              const W* __restrict__ weff,
                                              const double* __restrict__ sigma,
@@ -516,7 +517,45 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
       }
       const int np0 = __shfl_sync(kFull, np, 0);
       const int64_t e0 = __shfl_sync(kFull, wb, 0);
-      if (__all_sync(kFull, lane >= nkc || np == np0)) {
+      if (PAIRS && __all_sync(kFull, lane >= nkc || np == np0)) {
+        // FP32 complex W_eff read as 16-byte pairs of entries from an even
+        // global entry index (the array is 256-byte aligned): twice the bytes
+        // per load instruction, kU pairs per lane in flight.  Pair p covers
+        // global entries a0 + 2p and a0 + 2p + 1; entries outside this
+        // group's span [e0, e0 + ne) are masked.
+        const int ne = nkc * np0;
+        const float inv = 1.0f / float(np0);
+        const int64_t a0 = e0 & ~int64_t(1);
+        const int npairs = int((e0 + ne - a0 + 1) >> 1);
+        for (int pb = 0; pb < npairs; pb += 32 * kU) {
+          float4 wv[kU];
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            const int pp = pb + 32 * u + lane;
+            wv[u] = pp < npairs ? reinterpret_cast<const float4*>(weff)[(a0 >> 1) + pp]
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            const int pp = pb + 32 * u + lane;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int e = int(a0 + 2 * pp + h - e0);
+              const bool ok = pp < npairs && e >= 0 && e < ne;
+              const int kk = ok ? int((float(e) + 0.5f) * inv) : 0;
+              const int psk = __shfl_sync(kFull, ps, kk);
+              if (ok) {
+                const int node = psk + (e - kk * np0);
+                const double2 sv = reinterpret_cast<const double2*>(sigma)[node];
+                const double wr = double(h ? wv[u].z : wv[u].x);
+                const double wi = double(h ? wv[u].w : wv[u].y);
+                ar = fma(wr, sv.x, fma(-wi, sv.y, ar));
+                ai = fma(wr, sv.y, fma(wi, sv.x, ai));
+              }
+            }
+          }
+        }
+      } else if (__all_sync(kFull, lane >= nkc || np == np0)) {
         // every patch of this group has np0 nodes: entry e belongs to patch
         // e / np0 (exact in FP32: the fraction stays >= 0.5/np0 from an integer)
         const int ne = nkc * np0;
@@ -631,12 +670,12 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
   }
 }
 
-template <int CPLX, typename W>
+template <int CPLX, typename W, bool PAIRS = false>
 __global__ void __launch_bounds__(kCombineThreads)
     combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
                    const double* __restrict__ sigma, const double* __restrict__ partial,
                    int nchunks, double* __restrict__ pot, int nd) {
-  combine_rows<CPLX, W>(g, nr, weff, sigma, partial, nchunks, pot, nd, blockIdx.x);
+  combine_rows<CPLX, W, PAIRS>(g, nr, weff, sigma, partial, nchunks, pot, nd, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1580,6 +1619,16 @@ int far_chunks_for_waves(int64_t ntarg, int64_t nptso, int precision, int varian
   return int((nptso + chunk - 1) / chunk);
 }
 
+// FP32 Helmholtz near correction with 16-byte pair loads of W_eff (default;
+// BIE_COMBINE_PAIRS=0 selects the one-entry loads)
+static bool combine_pairs() {
+  static const bool on = [] {
+    const char* e = std::getenv("BIE_COMBINE_PAIRS");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
                            const MatvecArgs& a, cudaStream_t st) {
   if (g.ntarg == 0) return cudaSuccess;
@@ -1587,7 +1636,9 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
   const int64_t blocks = (g.ntarg * 32 + threads - 1) / threads;
   const dim3 grid(static_cast<unsigned>(blocks)), block(threads);
   if (kp.kind == 1) {
-    if (a.weff_f32)
+    if (a.weff_f32 && combine_pairs())
+      combine_kernel<1, float, true><<<grid, block, 0, st>>>(g, nr, (const float*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+    else if (a.weff_f32)
       combine_kernel<1, float><<<grid, block, 0, st>>>(g, nr, (const float*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
     else
       combine_kernel<1, double><<<grid, block, 0, st>>>(g, nr, (const double*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);

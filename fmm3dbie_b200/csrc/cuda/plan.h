@@ -127,7 +127,7 @@ struct GmresWorkspace {
 };
 
 struct MixedWorkspace {
-  DBuf<double> r, d, partial, nrm;
+  DBuf<double> r, d, partial, nrm, kx;
 };
 
 // Per-precision stage totals (index 0 = f64 matvecs, 1 = f32 matvecs).
@@ -328,14 +328,34 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
 // Mixed-precision solve: FP64 residuals and iterative refinement around
 // FP32-matvec GMRES inner solves.  Stops when the FP64 relative residual
 // is <= eps_target (per system) or max_outer refinements were done.
+//
+// The refinement residual r = b - (zid x + K x) needs K x to about 1e-11 of
+// ||b||.  With increments on (the default), K x is kept in FP64: the first
+// refinement step applies the FP64 operator to the whole x, and a later
+// step whose correction d is small, kFp32OpErr ||d||_w / ||x||_w <=
+// eps_target / 4 for every active system, adds the FP32 operator's K d to
+// it instead (FP32 error on a correction of relative size ||d||/||x||); any
+// other step applies the FP64 operator to x again.
 struct MixedOut {
   std::vector<int64_t> inner_iters;  // total inner GMRES iterations per system
   std::vector<double> rres;          // final FP64 relative residual per system
   std::vector<int64_t> outer;        // refinement steps per system
   std::vector<int64_t> x0_dropped;   // 1 where the initial guess was replaced by 0
   int fp64_matvecs = 0, fp32_matvecs = 0;
+  int incr_matvecs = 0;              // FP32 applications to corrections (in fp32_matvecs)
+  double max_incr_ratio = 0.0;       // largest ||d||_w / ||x||_w of an increment step
   int status = kOk;
 };
+// Relative error assumed for the FP32 operator in the increment test (the
+// measured FP32 matvec errors are 2.6e-7 to 9.3e-7 of the FP64 result).
+constexpr double kFp32OpErr = 1e-6;
+// Refinement residual: 1 = increments (default), 0 = the FP64 operator on x
+// at every step.  BIE_MIXED_RESIDUAL=full|increment sets the initial value.
+int mixed_residual_mode();
+void set_mixed_residual_mode(int mode);
+// statistics of the calling thread's last mixed solve: fp64 and fp32
+// matvecs, increment matvecs, largest increment ratio
+const MixedOut& last_mixed_out();
 int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, const double* d_x0,
                 int64_t numit, double eps_target, double inner_floor, int max_outer,
                 double* d_soln, MixedOut& out, cudaStream_t st);

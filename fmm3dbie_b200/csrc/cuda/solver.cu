@@ -3,7 +3,9 @@
 // system (segment, density) has its own inner products, Hessenberg matrix,
 // Givens rotations and stopping test; all systems share every launch.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -283,9 +285,43 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
   return out.status;
 }
 
+namespace {
+std::atomic<int> g_mixed_mode{-1};
+thread_local MixedOut t_last_mixed;
+}  // namespace
+
+int mixed_residual_mode() {
+  int m = g_mixed_mode.load();
+  if (m < 0) {
+    const char* e = std::getenv("BIE_MIXED_RESIDUAL");
+    m = (e && std::string(e) == "full") ? 0 : 1;
+    g_mixed_mode.store(m);
+  }
+  return m;
+}
+
+void set_mixed_residual_mode(int mode) { g_mixed_mode.store(mode ? 1 : 0); }
+
+const MixedOut& last_mixed_out() { return t_last_mixed; }
+
+static int solve_mixed_impl(Operator& P, int nd, const cdouble* zid, const double* d_rhs,
+                            const double* d_x0, int64_t numit, double eps_target,
+                            double inner_floor, int max_outer, double* d_soln, MixedOut& out,
+                            cudaStream_t st);
+
 int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, const double* d_x0,
                 int64_t numit, double eps_target, double inner_floor, int max_outer,
                 double* d_soln, MixedOut& out, cudaStream_t st) {
+  const int s = solve_mixed_impl(P, nd, zid, d_rhs, d_x0, numit, eps_target, inner_floor,
+                                 max_outer, d_soln, out, st);
+  t_last_mixed = out;
+  return s;
+}
+
+static int solve_mixed_impl(Operator& P, int nd, const cdouble* zid, const double* d_rhs,
+                            const double* d_x0, int64_t numit, double eps_target,
+                            double inner_floor, int max_outer, double* d_soln, MixedOut& out,
+                            cudaStream_t st) {
   if (!P.square()) {
     set_last_error("the solver needs an operator whose targets are its nodes");
     return kErrArg;
@@ -302,10 +338,12 @@ int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, co
   DBuf<double>& d = P.mws.d;
   DBuf<double>& partial = P.mws.partial;
   DBuf<double>& nrm = P.mws.nrm;
+  DBuf<double>& kx = P.mws.kx;  // K x in FP64 (see MixedOut)
   BIE_CUDA(r.alloc(ldv));
   BIE_CUDA(d.alloc(ldv));
+  BIE_CUDA(kx.alloc(ldv));
   BIE_CUDA(partial.alloc(size_t(2) * nd * sg.nchunk));
-  BIE_CUDA(nrm.alloc(size_t(6) * nsys));
+  BIE_CUDA(nrm.alloc(size_t(8) * nsys));
   double* d_zid = nrm.p + 4 * nsys;  // zid per system
   {
     std::vector<cdouble> zv(zid, zid + nsys);
@@ -315,8 +353,11 @@ int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, co
   out.inner_iters.assign(nsys, 0);
   out.outer.assign(nsys, 0);
   out.rres.assign(nsys, 1.0);
-  out.fp64_matvecs = out.fp32_matvecs = 0;
+  out.fp64_matvecs = out.fp32_matvecs = out.incr_matvecs = 0;
+  out.max_incr_ratio = 0.0;
   out.status = kOk;
+  const bool increments = mixed_residual_mode() == 1;
+  bool kx_valid = false;
   const double* wts = P.d_node_wts;
   // r = rhs - (zid x + K x) from K x already in r
   auto finish_residual = [&]() -> int {
@@ -406,8 +447,10 @@ int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, co
     if (!r_is_f64 && all_done) {
       // the guess already meets the target in FP32: confirm it in FP64
       if ((ier = P.set_active(std::vector<uint8_t>(sg.nseg, 1), st))) return ier;
-      if ((ier = P.apply(0, nd, d_soln, r.p, st))) return ier;
+      if ((ier = P.apply(0, nd, d_soln, kx.p, st))) return ier;
       ++out.fp64_matvecs;
+      kx_valid = true;
+      BIE_CUDA(cudaMemcpyAsync(r.p, kx.p, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
       if ((ier = finish_residual())) return ier;
       r_is_f64 = true;
       continue;
@@ -448,14 +491,48 @@ int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, co
       maxit = std::max(maxit, go.niter[q]);
     }
     out.fp32_matvecs += int(maxit);
-    // x += d ; r = rhs - (zid x + K x) in f64 for the systems still refined
+    // x += d ; r = rhs - (zid x + K x) for the systems still refined
     // (frozen surfaces of a batch skip the matvec; their r is not read again)
     BIE_CUDA(dev::launch_axpby(d.p, d_soln, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+    bool incr = false;
+    double ratio_max = 0.0;
+    if (increments && kx_valid) {
+      // ||d||_w and ||x||_w per system decide whether K x may be updated
+      // with the FP32 operator applied to d
+      std::vector<double> hd(2 * nsys), hx(2 * nsys);
+      BIE_CUDA(dev::launch_mdot(d.p, ldv, 1, d.p, wts, nd, cplx, sg, partial.p, nrm.p, st));
+      BIE_CUDA(cudaMemcpyAsync(hd.data(), nrm.p, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+      BIE_CUDA(dev::launch_mdot(d_soln, ldv, 1, d_soln, wts, nd, cplx, sg, partial.p,
+                                nrm.p + 6 * nsys, st));
+      BIE_CUDA(cudaMemcpyAsync(hx.data(), nrm.p + 6 * nsys, 2 * nsys * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
+      BIE_CUDA(cudaStreamSynchronize(st));
+      incr = true;
+      for (int q = 0; q < nsys; ++q) {
+        if (frozen[q]) continue;
+        const double xn = std::sqrt(std::max(hx[2 * q], 0.0));
+        const double dn = std::sqrt(std::max(hd[2 * q], 0.0));
+        const double ratio = xn > 0 ? dn / xn : (dn > 0 ? 1.0 : 0.0);
+        ratio_max = std::max(ratio_max, ratio);
+        if (kFp32OpErr * ratio > 0.25 * eps_target) incr = false;
+      }
+    }
     if ((ier = P.set_active(seg_mask(), st))) return ier;
-    ier = P.apply(0, nd, d_soln, r.p, st);
-    if (ier) return ier;
+    if (incr) {
+      ier = P.apply(1, nd, d.p, r.p, st);  // r = K32 d
+      if (ier) return ier;
+      BIE_CUDA(dev::launch_axpby(r.p, kx.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
+      ++out.fp32_matvecs;
+      ++out.incr_matvecs;
+      out.max_incr_ratio = std::max(out.max_incr_ratio, ratio_max);
+    } else {
+      ier = P.apply(0, nd, d_soln, kx.p, st);
+      if (ier) return ier;
+      ++out.fp64_matvecs;
+      kx_valid = true;
+    }
     if ((ier = P.set_active(std::vector<uint8_t>(sg.nseg, 1), st))) return ier;
-    ++out.fp64_matvecs;
+    BIE_CUDA(cudaMemcpyAsync(r.p, kx.p, ldv * sizeof(double), cudaMemcpyDeviceToDevice, st));
     if ((ier = finish_residual())) return ier;
     r_is_f64 = true;
   }

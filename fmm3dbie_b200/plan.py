@@ -167,9 +167,21 @@ class Plan:
         else:
             info["fp64_matvecs"] = int(errs[0])
             info["fp32_matvecs"] = int(errs[1])
+            ms = np.zeros(4)
+            L.lib().bie_last_mixed_stats(L.ptr(ms))
+            info["increment_matvecs"] = int(ms[2])
+            info["max_increment_ratio"] = float(ms[3])
             if x0 is not None:
                 info["x0_dropped"] = errs[2:2 + nd].astype(bool)
         return out, info
+
+    @staticmethod
+    def set_mixed_residual(mode: str) -> None:
+        """Refinement residual of the mixed solvers, process wide: "increment"
+        (default: FP32 operator on small corrections, FP64 on the first
+        step) or "full" (FP64 operator on x after every inner solve)."""
+        L.check(L.lib().bie_set_mixed_residual({"full": 0, "increment": 1}[mode]),
+                "bie_set_mixed_residual")
 
     def timing(self, enable: bool | None = None):
         t = np.zeros(8)

@@ -348,6 +348,20 @@ int bie_plan_solve(void* plan, int64_t mode, int64_t nd, const double* zid,
  * strengths, far, combine (ms totals), calls for the f64 matvecs, then the
  * same four for the f32 matvecs. */
 int bie_plan_timing(void* plan, int64_t enable, double* times);
+/* Refinement residual of the mixed-precision solvers (mode 1 of
+ * bie_plan_solve / bie_batch_solve, iprec 1 of *_solver_guru_ext), process
+ * wide: 1 (default; BIE_MIXED_RESIDUAL=increment) keeps K x in FP64 from the
+ * first refinement step's FP64 matvec and adds the FP32 operator's K d for a
+ * later correction d whose FP32 error cannot reach the target
+ * (1e-6 ||d||_w / ||x||_w <= eps_gmres / 4 for every active system), else
+ * applies the FP64 operator to x again; 0 (BIE_MIXED_RESIDUAL=full) applies
+ * the FP64 operator to x after every inner solve.  bie_last_mixed_stats:
+ * the calling thread's last mixed solve: out[0] FP64 matvecs, out[1] FP32
+ * matvecs (increments included), out[2] increment matvecs, out[3] largest
+ * ||d||_w / ||x||_w of an increment.  No reference counterpart. */
+int bie_set_mixed_residual(int64_t mode);
+int bie_get_mixed_residual(void);
+int bie_last_mixed_stats(double* out);
 /* Far-field shape of (iprec, nd): bie_plan_set_far pins it (variant 0-2:
  * CUDA-core block shapes; 3-4: tensor-core kernel of the FP32 Helmholtz
  * multi-density path, 16/32 or 64 densities per CTA, nd >= 4; nchunks source

@@ -20,11 +20,19 @@
  * target pairs with r < thresh skipped (the FMM3D self-interaction rule that
  * l3ddirectcdp / h3ddirectcdp share).
  *
+ * oracle_setup.c builds what this matvec consumes (surface, near list, far
+ * orders, oversampled geometry, weights, near quadrature) independently of
+ * the product; oracle_far.c holds the faster CPU far fields used only when
+ * the CPU path is timed (oracle_set_far_method); the scalar direct sum here
+ * is the parity oracle.
+ *
  * Parity status: the reference cannot be compiled here (no Fortran
  * compiler, FMM3D absent, GGQ tables missing), and its tests carry no
  * golden vectors.  The oracle is pinned by the reference's own known-answer
- * tests (sphere spectra of S and D, Green's identity, point-source solves)
- * evaluated in tests/.
+ * tests (sphere spectra of S and D through the oracle's own pipeline,
+ * Green's identity, point-source solves) evaluated in tests/; element-level
+ * parity of the near quadrature with the reference's GGQ generator is
+ * unpinned.
  */
 #include "oracle_common.h"
 

@@ -278,3 +278,32 @@ def test_torus_independent_pipeline(torch):
                             torus_surface(32, 16, 5))
     print(f"\ntorus 18432 k 8, independent setups: FP64 {e64:.2e}, FP32 {e32:.2e} (eps 1e-7)")
     assert e64 < 1e-6 and e32 < 1.5e-6
+
+
+def test_refinement_residual_modes(torch, ellipsoid_full, helm2):
+    """The mixed solver's refinement residual: the FP64 operator on x after
+    every inner solve ("full") or FP32 increments on small corrections once
+    K x is known in FP64 ("increment", the default).  Both reach FP64
+    residual 1e-10; the oracle's operator confirms the true residual of each
+    solution; increments replace FP64 matvecs."""
+    s = ellipsoid_full
+    zp, st, P = helm2
+    r = np.linalg.norm(s.xyz - X0, axis=1)
+    rhs = np.exp(2j * r) / (4 * np.pi * r)
+    rd = torch.tensor(rhs, device="cuda")
+    w = s.qwts()
+    out = {}
+    for mode in ("full", "increment"):
+        Plan.set_mixed_residual(mode)
+        x, info = P.solve(rd, 0.5, mode=1, numit=300, eps_gmres=1e-10)
+        xs = x.cpu().numpy()
+        res = rhs - (0.5 * xs + oracle.lpcomp(1, s, zp, st.near, st.over, xs))
+        out[mode] = (info, wnorm(w, res) / wnorm(w, rhs))
+    Plan.set_mixed_residual("increment")
+    for mode, (info, rr) in out.items():
+        print(f"\n{mode}: rres {info['rres'][0]:.2e}, oracle residual {rr:.2e}, FP64/FP32 "
+              f"matvecs {info['fp64_matvecs']}/{info['fp32_matvecs']}, increments "
+              f"{info['increment_matvecs']} (largest |d|/|x| {info['max_increment_ratio']:.1e})")
+        assert info["status"] == 0 and info["rres"][0] <= 1e-10 and rr < 2e-10
+    assert out["full"][0]["increment_matvecs"] == 0
+    assert out["increment"][0]["fp64_matvecs"] <= out["full"][0]["fp64_matvecs"]
