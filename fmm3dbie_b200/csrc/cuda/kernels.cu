@@ -11,7 +11,6 @@
 //   (c) combine   : pot_i = sum of far partials + sum_k W_eff(k) . sigma,
 //                   W_eff = wnear - smooth near part (folded once per plan,
 //                   replacing the per-call l3ddirectcdp/h3ddirectcdp subtraction).
-#include <cstdlib>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -102,10 +101,16 @@ __device__ __forceinline__ void far_block(const Geometry& g, const KParams& kp,
   const int64_t ntarg = g.ntarg, nptso = g.nptso;
   const int64_t tbase = int64_t(bx) * NT * TPT;
   const int m = bz;  // density index
-  // Coordinates are shifted by the block's first target so that nearby
-  // pairs keep their relative accuracy in single precision.
+  // FP32: coordinates are shifted by the block's first target so that nearby
+  // pairs keep their relative accuracy in single precision.  FP64 keeps the
+  // absolute coordinates: t - s of two nearby points is then exact, which the
+  // double-layer numerator n.(t - s) = O(r^2) of a close pair needs (a shift
+  // would leave t - s with rounding of the shifted magnitudes, up to 5e-10 of
+  // n.(t - s) on a curved surface).
   const int64_t tc = tbase < ntarg ? tbase : ntarg - 1;
-  const double cx = g.tx[tc], cy = g.ty[tc], cz = g.tz[tc];
+  constexpr bool kShift = sizeof(R) == 4;
+  const double cx = kShift ? g.tx[tc] : 0.0, cy = kShift ? g.ty[tc] : 0.0,
+               cz = kShift ? g.tz[tc] : 0.0;
   R tx[TPT], ty[TPT], tz[TPT];
   double accr[TPT], acci[TPT];
 #pragma unroll
@@ -120,12 +125,16 @@ __device__ __forceinline__ void far_block(const Geometry& g, const KParams& kp,
   }
   const R thr2 = R(kp.thresh * kp.thresh);
   const R k = R(kp.kr), kim = R(kp.ki);
-  // bounding box of this block's targets (FP32 blocks of kFarBlockTargets32)
+  // bounding box of this block's targets: the box of the kFarBlockTargets32
+  // block that contains them (the block itself in FP32; FP64 blocks of 256 or
+  // fewer targets lie inside one, which only makes the test conservative)
   double tbx[6] = {0, 0, 0, 0, 0, 0};
-  const bool boxes = sizeof(R) == 4 && NT * TPT == kFarBlockTargets32 && g.sbox && g.tbox;
+  const bool boxes = (sizeof(R) == 4 ? NT * TPT == kFarBlockTargets32
+                                     : kFarBlockTargets32 % (NT * TPT) == 0) &&
+                     g.sbox && g.tbox && TILE == kFarTileSources;
   if (boxes)
 #pragma unroll
-    for (int c = 0; c < 6; ++c) tbx[c] = g.tbox[6 * bx + c];
+    for (int c = 0; c < 6; ++c) tbx[c] = g.tbox[6 * (tbase / kFarBlockTargets32) + c];
   const int64_t s0 = int64_t(by) * chunk_len;
   const int64_t s1 = min(s0 + chunk_len, nptso);
   for (int64_t sb = s0; sb < s1; sb += TILE) {
@@ -149,8 +158,8 @@ __device__ __forceinline__ void far_block(const Geometry& g, const KParams& kp,
     R pr[TPT], pi[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) pr[t] = pi[t] = R(0);
-    // FP32: a full tile whose bounding box stays farther than the margin from
-    // the block's targets cannot hold an excluded pair, so it skips the test.
+    // A full tile whose bounding box stays farther than the margin from the
+    // block's targets cannot hold an excluded pair, so it skips the test.
     // A partial tile keeps it: its zero padding sits at the block centre,
     // which is the block's first target.
     bool check = true;
@@ -269,7 +278,10 @@ __device__ __forceinline__ void far_md_block(const Geometry& g, const KParams& k
   const int m0 = bz * MD;
   const int64_t tcen = (tbase / kMdCentre) * kMdCentre;
   const int64_t tc = tcen < ntarg ? tcen : ntarg - 1;
-  const double cx = g.tx[tc], cy = g.ty[tc], cz = g.tz[tc];
+  // shifted coordinates in FP32 only (see far_block)
+  constexpr bool kShift = sizeof(R) == 4;
+  const double cx = kShift ? g.tx[tc] : 0.0, cy = kShift ? g.ty[tc] : 0.0,
+               cz = kShift ? g.tz[tc] : 0.0;
   R tx[TPT], ty[TPT], tz[TPT];
   double acc[TPT][MD][C];
 #pragma unroll
@@ -463,7 +475,7 @@ constexpr int kCombineUnroll = 4;     // W_eff entries per lane in flight
 
 // Rows 8*bx .. 8*bx+7 (one warp each) of the near correction plus the far
 // partial sums.
-template <int CPLX, typename W, bool PAIRS = false>
+template <int CPLX, typename W>
 __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
                                              const W* __restrict__ weff,
                                              const double* __restrict__ sigma,
@@ -517,45 +529,7 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
       }
       const int np0 = __shfl_sync(kFull, np, 0);
       const int64_t e0 = __shfl_sync(kFull, wb, 0);
-      if (PAIRS && __all_sync(kFull, lane >= nkc || np == np0)) {
-        // FP32 complex W_eff read as 16-byte pairs of entries from an even
-        // global entry index (the array is 256-byte aligned): twice the bytes
-        // per load instruction, kU pairs per lane in flight.  Pair p covers
-        // global entries a0 + 2p and a0 + 2p + 1; entries outside this
-        // group's span [e0, e0 + ne) are masked.
-        const int ne = nkc * np0;
-        const float inv = 1.0f / float(np0);
-        const int64_t a0 = e0 & ~int64_t(1);
-        const int npairs = int((e0 + ne - a0 + 1) >> 1);
-        for (int pb = 0; pb < npairs; pb += 32 * kU) {
-          float4 wv[kU];
-#pragma unroll
-          for (int u = 0; u < kU; ++u) {
-            const int pp = pb + 32 * u + lane;
-            wv[u] = pp < npairs ? reinterpret_cast<const float4*>(weff)[(a0 >> 1) + pp]
-                                : make_float4(0.f, 0.f, 0.f, 0.f);
-          }
-#pragma unroll
-          for (int u = 0; u < kU; ++u) {
-            const int pp = pb + 32 * u + lane;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const int e = int(a0 + 2 * pp + h - e0);
-              const bool ok = pp < npairs && e >= 0 && e < ne;
-              const int kk = ok ? int((float(e) + 0.5f) * inv) : 0;
-              const int psk = __shfl_sync(kFull, ps, kk);
-              if (ok) {
-                const int node = psk + (e - kk * np0);
-                const double2 sv = reinterpret_cast<const double2*>(sigma)[node];
-                const double wr = double(h ? wv[u].z : wv[u].x);
-                const double wi = double(h ? wv[u].w : wv[u].y);
-                ar = fma(wr, sv.x, fma(-wi, sv.y, ar));
-                ai = fma(wr, sv.y, fma(wi, sv.x, ai));
-              }
-            }
-          }
-        }
-      } else if (__all_sync(kFull, lane >= nkc || np == np0)) {
+      if (__all_sync(kFull, lane >= nkc || np == np0)) {
         // every patch of this group has np0 nodes: entry e belongs to patch
         // e / np0 (exact in FP32: the fraction stays >= 0.5/np0 from an integer)
         const int ne = nkc * np0;
@@ -670,12 +644,12 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
   }
 }
 
-template <int CPLX, typename W, bool PAIRS = false>
+template <int CPLX, typename W>
 __global__ void __launch_bounds__(kCombineThreads)
     combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
                    const double* __restrict__ sigma, const double* __restrict__ partial,
                    int nchunks, double* __restrict__ pot, int nd) {
-  combine_rows<CPLX, W, PAIRS>(g, nr, weff, sigma, partial, nchunks, pot, nd, blockIdx.x);
+  combine_rows<CPLX, W>(g, nr, weff, sigma, partial, nchunks, pot, nd, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1619,16 +1593,6 @@ int far_chunks_for_waves(int64_t ntarg, int64_t nptso, int precision, int varian
   return int((nptso + chunk - 1) / chunk);
 }
 
-// FP32 Helmholtz near correction with 16-byte pair loads of W_eff (default;
-// BIE_COMBINE_PAIRS=0 selects the one-entry loads)
-static bool combine_pairs() {
-  static const bool on = [] {
-    const char* e = std::getenv("BIE_COMBINE_PAIRS");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
-
 cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
                            const MatvecArgs& a, cudaStream_t st) {
   if (g.ntarg == 0) return cudaSuccess;
@@ -1636,9 +1600,7 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
   const int64_t blocks = (g.ntarg * 32 + threads - 1) / threads;
   const dim3 grid(static_cast<unsigned>(blocks)), block(threads);
   if (kp.kind == 1) {
-    if (a.weff_f32 && combine_pairs())
-      combine_kernel<1, float, true><<<grid, block, 0, st>>>(g, nr, (const float*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-    else if (a.weff_f32)
+    if (a.weff_f32)
       combine_kernel<1, float><<<grid, block, 0, st>>>(g, nr, (const float*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
     else
       combine_kernel<1, double><<<grid, block, 0, st>>>(g, nr, (const double*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);

@@ -303,8 +303,12 @@ __global__ void __launch_bounds__(kEvThreads)
     node = ta.leaves[blockIdx.x];
   }
   const TNodeD tn = ta.tn[node];
-  const double cx = 0.5 * (tn.lo[0] + tn.hi[0]), cy = 0.5 * (tn.lo[1] + tn.hi[1]),
-               cz = 0.5 * (tn.lo[2] + tn.hi[2]);
+  // FP32 shifts coordinates to the node centre; FP64 keeps them absolute so
+  // that t - s of a close pair stays exact (as the direct far kernels do)
+  constexpr bool kShift = sizeof(R) == 4;
+  const double cx = kShift ? 0.5 * (tn.lo[0] + tn.hi[0]) : 0.0,
+               cy = kShift ? 0.5 * (tn.lo[1] + tn.hi[1]) : 0.0,
+               cz = kShift ? 0.5 * (tn.lo[2] + tn.hi[2]) : 0.0;
   bool act, wact;  // this thread's / this warp's targets exist
   double x = cx, y = cy, z = cz;
   if constexpr (PROXYT) {
@@ -496,8 +500,12 @@ __global__ void __launch_bounds__(kEvThreads)
     node = ta.leaves[blockIdx.x];
   }
   const TNodeD tn = ta.tn[node];
-  const double cx = 0.5 * (tn.lo[0] + tn.hi[0]), cy = 0.5 * (tn.lo[1] + tn.hi[1]),
-               cz = 0.5 * (tn.lo[2] + tn.hi[2]);
+  // FP32 shifts coordinates to the node centre; FP64 keeps them absolute so
+  // that t - s of a close pair stays exact (as the direct far kernels do)
+  constexpr bool kShift = sizeof(R) == 4;
+  const double cx = kShift ? 0.5 * (tn.lo[0] + tn.hi[0]) : 0.0,
+               cy = kShift ? 0.5 * (tn.lo[1] + tn.hi[1]) : 0.0,
+               cz = kShift ? 0.5 * (tn.lo[2] + tn.hi[2]) : 0.0;
   bool act, wact;
   double x = cx, y = cy, z = cz;
   if constexpr (PROXYT) {
