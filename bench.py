@@ -741,6 +741,20 @@ def batched_leg(dev, steps=1):
     out["fp64_single"] = {"solves_per_s": 1000.0 / float(np.mean(ts)), "ms_per_solve": float(np.mean(ts)),
                           "niter": its, "sample": "2 of the 64 systems, one at a time"}
     out["speedup_vs_fp64_single"] = out["mixed"]["solves_per_s"] / out["fp64_single"]["solves_per_s"]
+    # stage times of one FP32 matvec of the 64 densities (CUDA events); the
+    # oversampling stage against its bytes: sigma read (c128) and the
+    # oversampled densities written (c64)
+    P.matvec(R, 1)
+    torch.cuda.synchronize()
+    P.timing(True)
+    P.matvec(R, 1)
+    torch.cuda.synchronize()
+    tm = P.timing(False)["f32"]
+    ob = float(s.npts) * 64 * 16 + float(P.nptso) * 64 * 8
+    out["fp32_matvec_nd64_ms"] = {"strengths": tm["strengths_ms"], "far": tm["far_ms"],
+                                  "combine": tm["combine_ms"],
+                                  "strengths_gbs": ob / (tm["strengths_ms"] * 1e-3) / 1e9,
+                                  "strengths_bytes": ob}
     # error against the oracle: residual of two mixed solutions under the
     # oracle's matvec on the same inputs
     xs = xsol["mixed"].cpu().numpy()

@@ -145,6 +145,19 @@ int BatchPlan::build_config(int precision, int nd, int variant, int64_t chunk, C
     vofs += p.npts;
     sofs += p.nptso;
   }
+  // largest items first: the far kernels draw items in list order as blocks
+  // become free, so the cheap ones (partial chunks, short target blocks of
+  // small surfaces) fill the tail
+  {
+    auto cost = [&](const int4& it) {
+      const Plan& p = *plans[size_t(it.x)];
+      const int64_t nt = std::min<int64_t>(tpb, p.ntarg - int64_t(it.y) * tpb);
+      const int64_t ns = std::min<int64_t>(chunk, p.nptso - int64_t(it.z) * chunk);
+      return nt * ns;
+    };
+    std::stable_sort(far_items.begin(), far_items.end(),
+                     [&](const int4& a, const int4& b) { return cost(a) > cost(b); });
+  }
   if (far_items.size() > size_t(INT32_MAX)) {
     set_last_error("batch work list too long");
     return kErrArg;
@@ -158,6 +171,7 @@ int BatchPlan::build_config(int precision, int nd, int variant, int64_t chunk, C
   BIE_CUDA(c.str.alloc(sbytes));
   BIE_CUDA(c.partial.alloc(size_t(std::max<int64_t>(pofs, 1))));
   BIE_CUDA(c.refs.alloc(2));
+  BIE_CUDA(c.counter.alloc(1));
   c.variant = variant;
   c.chunk = chunk;
   dev::BatchArgs& a = c.args;
@@ -177,6 +191,7 @@ int BatchPlan::build_config(int precision, int nd, int variant, int64_t chunk, C
   a.yref = reinterpret_cast<double* const*>(c.refs.p + 1);
   a.str = c.str.p;
   a.partial = c.partial.p;
+  a.far_counter = c.counter.p;
   const int bps = std::max(1, dev::batch_far_blocks_per_sm(kind, precision, variant, nd, ck));
   a.grid_far = int(std::min<int64_t>(int64_t(far_items.size()), int64_t(num_sms) * bps));
   a.grid_patch = int(std::min<int64_t>(int64_t(patch_items.size()), int64_t(num_sms) * 8));

@@ -217,6 +217,7 @@ struct BatchArgs {
   double* partial = nullptr;
   int grid_patch = 1, grid_far = 1, grid_row = 1;  // persistent grid sizes
   int max_np = 0;
+  int* far_counter = nullptr;              // device work counter of the far-field launch
 };
 // Strengths/oversampling, far field and combine of every surface: three
 // persistent launches, each walking its work list.  Reads the vector

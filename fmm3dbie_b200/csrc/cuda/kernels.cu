@@ -1275,10 +1275,24 @@ __global__ void batch_strengths_kernel(const BatchSurf* __restrict__ bs,
   }
 }
 
+// Next work item of a persistent batch kernel, taken from a counter that the
+// launch sequence zeroes before the kernel: thread 0 draws, the block reads
+// it, and the second barrier keeps thread 0's next draw from overwriting the
+// slot before every thread has read it (items are then handed out in list
+// order, largest first, as blocks become free).
+__device__ __forceinline__ int next_item(int* counter, int* slot) {
+  if (threadIdx.x == 0) *slot = atomicAdd(counter, 1);
+  __syncthreads();
+  const int w = *slot;
+  __syncthreads();
+  return w;
+}
+
 template <int KIND, typename R, int NT, int TPT, int TILE, bool CK>
 __global__ void __launch_bounds__(NT)
     batch_far_kernel(const BatchSurf* __restrict__ bs, const int4* __restrict__ items, int nitems,
-                     const R* __restrict__ str, double* __restrict__ partial, int nd, int prec) {
+                     const R* __restrict__ str, double* __restrict__ partial, int nd, int prec,
+                     int* __restrict__ counter) {
   constexpr int SW = (KIND == 1) ? 4 : 2;
   __shared__ typename Vec<R>::T4 sg0[TILE];
   __shared__ typename Vec<R>::T2 sg1[TILE];
@@ -1290,7 +1304,10 @@ __global__ void __launch_bounds__(NT)
     tab = stab;
   }
   __syncthreads();
-  for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+  __shared__ int s_w;
+  for (;;) {
+    const int w = next_item(counter, &s_w);
+    if (w >= nitems) break;
     const int4 it = items[w];
     const BatchSurf& S = bs[it.x];
     if (S.live && *S.live == 0) continue;  // uniform over the block
@@ -1307,7 +1324,7 @@ template <int KIND, typename R, int NT, int TPT, int MD, int TILE, bool CK>
 __global__ void __launch_bounds__(NT)
     batch_far_md_kernel(const BatchSurf* __restrict__ bs, const int4* __restrict__ items,
                         int nitems, const R* __restrict__ sig, double* __restrict__ partial,
-                        int nd, int prec) {
+                        int nd, int prec, int* __restrict__ counter) {
   constexpr int C = (KIND == 1) ? 2 : 1;
   __shared__ typename Vec<R>::T4 sg0[TILE];
   __shared__ typename Vec<R>::T2 sg1[TILE];
@@ -1320,7 +1337,10 @@ __global__ void __launch_bounds__(NT)
     tab = stab;
   }
   __syncthreads();
-  for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+  __shared__ int s_w;
+  for (;;) {
+    const int w = next_item(counter, &s_w);
+    if (w >= nitems) break;
     const int4 it = items[w];
     const BatchSurf& S = bs[it.x];
     if (S.live && *S.live == 0) continue;  // uniform over the block
@@ -1371,7 +1391,8 @@ cudaError_t batch_far_dispatch(const BatchArgs& a, cudaStream_t st, int* occ) {
   auto kern = batch_far_kernel<KIND, R, NT, TPT, kFarTile, CK>;
   if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, NT, 0);
   kern<<<a.grid_far, NT, 0, st>>>(a.surfs, a.far_items, a.nfar_items,
-                                  static_cast<const R*>(a.str), a.partial, a.nd, a.precision);
+                                  static_cast<const R*>(a.str), a.partial, a.nd, a.precision,
+                                  a.far_counter);
   return cudaGetLastError();
 }
 
@@ -1381,7 +1402,8 @@ cudaError_t batch_far_md_dispatch(const BatchArgs& a, cudaStream_t st, int* occ)
   auto kern = batch_far_md_kernel<KIND, R, NT, TPT, MD, kFarTile, CK>;
   if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, NT, 0);
   kern<<<a.grid_far, NT, 0, st>>>(a.surfs, a.far_items, a.nfar_items,
-                                  static_cast<const R*>(a.str), a.partial, a.nd, a.precision);
+                                  static_cast<const R*>(a.str), a.partial, a.nd, a.precision,
+                                  a.far_counter);
   return cudaGetLastError();
 }
 
@@ -1468,6 +1490,8 @@ cudaError_t launch_batch_matvec(const BatchArgs& a, cudaStream_t st) {
   else
     e = cplx ? strengths(batch_strengths_kernel<double, 1>, static_cast<double*>(a.str))
              : strengths(batch_strengths_kernel<double, 0>, static_cast<double*>(a.str));
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(a.far_counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   e = batch_far_any(a, st, nullptr);
   if (e != cudaSuccess) return e;

@@ -293,6 +293,7 @@ class BatchPlan : public Operator {
     DBuf<char> str;
     DBuf<double> partial;
     DBuf<void*> refs;  // [0] input vector, [1] output vector (device pointer slots)
+    DBuf<int> counter;  // far-field work counter
     dev::BatchArgs args;
     cudaGraphExec_t graph = nullptr;
   };
