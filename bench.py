@@ -495,7 +495,6 @@ def main():
     mixed = lambda: P.solve(r_d, 0.5, mode=1, numit=300, eps_gmres=TOL_RES)  # noqa: E731
     for _ in range(args.warmup):
         mixed()
-    P.timing(True)
     if args.clock_sampler == "nvml":
         try:
             clocks = NvmlClockSampler(local)
@@ -508,6 +507,12 @@ def main():
     tsm, (xm, infom) = timed(mixed, args.steps, 0)
     launches = int(lib.bie_launch_count() - n0)
     ck = clocks.stop()
+    # stage times (CUDA events per matvec stage; the stage timing synchronises
+    # after every matvec, so it runs after the timed region, on two more solves)
+    P.timing(True)
+    for _ in range(2):
+        mixed()
+    torch.cuda.synchronize()
     stages = P.timing(False)
     pinfo = P.info()
     tm = float(np.mean(tsm))

@@ -486,6 +486,20 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
   const int64_t ntarg = g.ntarg;
   if (nd == 1) {
     __shared__ double sred[32][8][2];
+    // the row's range and its first 32 near pairs are loaded before the
+    // partial-sum phase and its barrier, so their latency overlaps it
+    int64_t k0 = 0, k1 = 0;
+    if (i < ntarg) {
+      k0 = nr.row_ptr[i];
+      k1 = nr.row_ptr[i + 1];
+    }
+    int ps_pre = 0, np_pre = 0;
+    int64_t wb_pre = 0;
+    if (i < ntarg && lane < k1 - k0) {
+      ps_pre = nr.nps[k0 + lane];
+      wb_pre = nr.wofs[k0 + lane];
+      np_pre = int(nr.wofs[k0 + lane + 1] - wb_pre);
+    }
     // far-field partial sums of the block's 8 rows, read cooperatively: thread
     // t takes row t % 8 of chunks t / 8, t / 8 + 32, ..., so every warp load
     // covers four whole 8-row segments
@@ -509,7 +523,6 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
     }
     __syncthreads();
     if (i >= ntarg) return;
-    const int64_t k0 = nr.row_ptr[i], k1 = nr.row_ptr[i + 1];
     const int wrow = threadIdx.x >> 5;
     double ar = sred[lane][wrow][0], ai = sred[lane][wrow][1];
     // Near patches of the row, 32 at a time: one lane-parallel load of their
@@ -520,12 +533,16 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
     constexpr int kU = kCombineUnroll;
     for (int64_t kc = k0; kc < k1; kc += 32) {
       const int nkc = int(k1 - kc < 32 ? k1 - kc : 32);
-      int ps = 0, np = 0;
-      int64_t wb = 0;
-      if (lane < nkc) {
-        ps = nr.nps[kc + lane];
-        wb = nr.wofs[kc + lane];
-        np = int(nr.wofs[kc + lane + 1] - wb);
+      int ps = ps_pre, np = np_pre;
+      int64_t wb = wb_pre;
+      if (kc != k0) {
+        ps = np = 0;
+        wb = 0;
+        if (lane < nkc) {
+          ps = nr.nps[kc + lane];
+          wb = nr.wofs[kc + lane];
+          np = int(nr.wofs[kc + lane + 1] - wb);
+        }
       }
       const int np0 = __shfl_sync(kFull, np, 0);
       const int64_t e0 = __shfl_sync(kFull, wb, 0);
