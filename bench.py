@@ -760,6 +760,25 @@ def batched_leg(dev, steps=1):
                                   "combine": tm["combine_ms"],
                                   "strengths_gbs": ob / (tm["strengths_ms"] * 1e-3) / 1e9,
                                   "strengths_bytes": ob}
+    # the oversampling alone on each engine (CUDA cores, tensor cores), 64
+    # densities, mean of 10 launches by CUDA events
+    import ctypes as C
+    from fmm3dbie_b200 import _lib as L
+    osv = torch.empty((P.nptso, 64), dtype=torch.complex64, device=dev)
+    eng = {}
+    for e in (0, 1):
+        args = (P._h, e, 64, C.c_void_p(R.data_ptr()), C.c_void_p(osv.data_ptr()), C.c_void_p(0))
+        L.check(L.lib().bie_plan_oversample(*args), "bie_plan_oversample")
+        a_ = torch.cuda.Event(enable_timing=True)
+        b_ = torch.cuda.Event(enable_timing=True)
+        a_.record()
+        for _ in range(10):
+            L.lib().bie_plan_oversample(*args)
+        b_.record()
+        b_.synchronize()
+        ms = a_.elapsed_time(b_) / 10
+        eng["cuda_cores" if e == 0 else "tensor_cores"] = {"ms": ms, "gbs": ob / (ms * 1e-3) / 1e9}
+    out["oversample_nd64"] = eng
     # error against the oracle: residual of two mixed solutions under the
     # oracle's matvec on the same inputs
     xs = xsol["mixed"].cpu().numpy()

@@ -119,6 +119,9 @@ _SIGS = {
     "bie_plan_matvec": (C.c_int, [VP, I64, I64, VP, VP, VP]),
     "bie_plan_solve": (C.c_int, [VP, I64, I64, PDBL, VP, VP, I64, DBL, VP, PI64, PDBL, PDBL, VP]),
     "bie_plan_timing": (C.c_int, [VP, I64, PDBL]),
+    "bie_set_oversample_engine": (C.c_int, [I64]),
+    "bie_get_oversample_engine": (C.c_int, []),
+    "bie_plan_oversample": (C.c_int, [VP, I64, I64, VP, VP, VP]),
     "bie_set_mixed_residual": (C.c_int, [I64]),
     "bie_get_mixed_residual": (C.c_int, []),
     "bie_last_mixed_stats": (C.c_int, [PDBL]),

@@ -1147,6 +1147,45 @@ int bie_plan_set_far(void* plan, int64_t iprec, int64_t nd, int64_t variant, int
   });
 }
 
+int bie_set_oversample_engine(int64_t engine) {
+  if (engine != 0 && engine != 1) return BIE_ERR_ARG;
+  bie::dev::set_oversample_engine(int(engine));
+  return BIE_OK;
+}
+
+int bie_get_oversample_engine(void) { return bie::dev::oversample_engine(); }
+
+int bie_plan_oversample(void* plan, int64_t engine, int64_t nd, const double* sigma_dev,
+                        float* out_dev, void* stream) {
+  if (!plan || !sigma_dev || !out_dev || nd < 1 || (engine != 0 && engine != 1)) return BIE_ERR_ARG;
+  return guarded([&] {
+    bie::Plan& P = *static_cast<bie::Plan*>(plan);
+    if (!P.cplx) {
+      bie::set_last_error("bie_plan_oversample: complex (Helmholtz) plans only");
+      return BIE_ERR_ARG;
+    }
+    if (engine == 1 && !bie::dev::oversample_tc_fits(P.g, P.kp, 1, int(nd))) {
+      bie::set_last_error("bie_plan_oversample: the tensor-core engine takes nd a multiple of 8 "
+                          "up to 128 and patches of at most 64 nodes and 128 far nodes");
+      return BIE_ERR_ARG;
+    }
+    bie::dev::MatvecArgs a;
+    a.precision = 1;
+    a.nd = int(nd);
+    a.sigma = sigma_dev;
+    a.strengths = out_dev;
+    a.tc_err = P.tc_err_ptr();
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const cudaError_t e = engine == 1 ? bie::dev::launch_oversample_tc(P.g, P.kp, a, st)
+                                      : bie::dev::launch_oversample(P.g, P.kp, a, st);
+    if (e != cudaSuccess) {
+      bie::set_last_error(cudaGetErrorString(e));
+      return BIE_ERR_CUDA;
+    }
+    return BIE_OK;
+  });
+}
+
 int bie_plan_get_far(void* plan, int64_t iprec, int64_t nd, int64_t* out) {
   if (!plan || !out || (iprec != 0 && iprec != 1) || nd < 1) return BIE_ERR_ARG;
   const bie::Plan* P = static_cast<bie::Plan*>(plan);

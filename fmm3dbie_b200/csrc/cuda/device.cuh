@@ -143,6 +143,18 @@ cudaError_t launch_far_md(const Geometry& g, const KParams& kp, const MatvecArgs
                           cudaStream_t st);
 cudaError_t launch_oversample(const Geometry& g, const KParams& kp, const MatvecArgs& a,
                               cudaStream_t st);
+// The same oversampled densities by the tensor cores (3xTF32 products, FP32
+// accumulator; oversample_tc.cu): complex densities, FP32 path, nd a
+// multiple of 8 up to 128, at most 128 far nodes and 64 nodes per patch
+// (oversample_tc_fits); cudaErrorNotSupported otherwise.  a.tc_err receives
+// a completion-wait timeout.
+bool oversample_tc_fits(const Geometry& g, const KParams& kp, int precision, int nd);
+cudaError_t launch_oversample_tc(const Geometry& g, const KParams& kp, const MatvecArgs& a,
+                                 cudaStream_t st);
+// Engine of the several-density oversampling in the plans' matvecs: 0 CUDA
+// cores (default), 1 tensor cores where oversample_tc_fits (BIE_OVERSAMPLE_ENGINE).
+int oversample_engine();
+void set_oversample_engine(int engine);
 // sdest (optional): source s is stored at position sdest[s].
 cudaError_t launch_source_consts(const Geometry& g, const KParams& kp, int precision, void* ab,
                                  cudaStream_t st, const int32_t* sdest = nullptr);

@@ -537,6 +537,15 @@ int Plan::tune_far(int precision, int nd, dev::MatvecArgs& a, cudaStream_t st, F
   return kOk;
 }
 
+cudaError_t Plan::oversample(const dev::MatvecArgs& a, cudaStream_t st) {
+  if (dev::oversample_engine() == 1 && dev::oversample_tc_fits(g, kp, a.precision, a.nd)) {
+    dev::MatvecArgs b = a;
+    b.tc_err = tc_err_.p;
+    return dev::launch_oversample_tc(g, kp, b, st);
+  }
+  return dev::launch_oversample(g, kp, a, st);
+}
+
 int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cudaStream_t st) {
   if (nd < 1) return kErrArg;
   if (precision == 1 && !weff32_.p) {
@@ -562,7 +571,7 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
   a.tc_err = tc_err_.p;
   if (timing) BIE_CUDA(cudaEventRecord(ev_[0], st));
   if (nd > 1)
-    BIE_CUDA(dev::launch_oversample(g, kp, a, st));
+    BIE_CUDA(oversample(a, st));
   else
     BIE_CUDA(dev::launch_strengths(g, kp, a, st));
   if (far_cfg_.find({precision, nd}) == far_cfg_.end()) {
@@ -615,7 +624,7 @@ int Plan::matvec_tree(int precision, int nd, const double* d_sigma, double* d_po
   if (timing) BIE_CUDA(cudaEventRecord(ev_[0], st));
   // one density: (charge, dipole) strengths; several: oversampled densities
   if (nd > 1)
-    BIE_CUDA(dev::launch_oversample(g, kp, a, st));
+    BIE_CUDA(oversample(a, st));
   else
     BIE_CUDA(dev::launch_strengths(g, kp, a, st));
   if (timing) BIE_CUDA(cudaEventRecord(ev_[1], st));

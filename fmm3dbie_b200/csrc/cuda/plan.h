@@ -214,6 +214,10 @@ class Plan : public Operator {
   int set_far_config(int precision, int nd, int variant, int nchunks);
   // Nonzero once a tensor-core far-field launch timed out waiting for its MMAs.
   int tc_error() const;
+  int* tc_err_ptr() { return tc_err_.p; }
+  // several-density oversampling of a matvec on the engine of
+  // dev::oversample_engine() (a.tc_err is the plan's flag)
+  cudaError_t oversample(const dev::MatvecArgs& a, cudaStream_t st);
   // Far-field method of a precision: 0 = direct sum over all pairs (the
   // kernels above), 1 = hierarchical (dual-tree barycentric Lagrange
   // interpolation, tree_far.h).  Chosen at build from the problem size

@@ -362,6 +362,21 @@ int bie_plan_timing(void* plan, int64_t enable, double* times);
 int bie_set_mixed_residual(int64_t mode);
 int bie_get_mixed_residual(void);
 int bie_last_mixed_stats(double* out);
+/* Oversampling of several complex densities (oversample_fun_guru,
+ * surf_routs.f90:511-591, nd at once) on the tensor cores: per patch the
+ * interpolation matrix times the patch densities as a tcgen05.mma kind::tf32
+ * GEMM with 3xTF32 products and an FP32 accumulator.  Engine 0: CUDA cores
+ * (FP64 sums, the default in the plans' FP32 matvecs); 1: tensor cores where
+ * they apply (Helmholtz, FP32 path, nd a multiple of 8 up to 128, patches of
+ * at most 64 nodes and 128 far nodes; BIE_OVERSAMPLE_ENGINE=1).
+ * bie_plan_oversample writes the FP32 oversampled densities of the plan's
+ * surface, out_dev[2 (s nd + m) + re/im] for oversampled node s (1..nptso)
+ * and density m, from sigma_dev (npts x nd complex, point-major), with the
+ * engine given; stream-ordered.  No reference counterpart. */
+int bie_set_oversample_engine(int64_t engine);
+int bie_get_oversample_engine(void);
+int bie_plan_oversample(void* plan, int64_t engine, int64_t nd, const double* sigma_dev,
+                        float* out_dev, void* stream);
 /* Far-field shape of (iprec, nd): bie_plan_set_far pins it (variant 0-2:
  * CUDA-core block shapes; 3-4: tensor-core kernel of the FP32 Helmholtz
  * multi-density path, 16/32 or 64 densities per CTA, nd >= 4; nchunks source
