@@ -190,6 +190,19 @@ cudaError_t launch_axpby(const double* x, double* y, double ar, double ai, doubl
 // y[e] = a[sys(e)] x[e] + b y[e], a complex per system on device
 cudaError_t launch_axpbys(const double* x, double* y, const double* a, double br, double bi,
                           int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st);
+// GMRES least squares on the device, FP64, one thread per system: the
+// Givens step of iteration it (Hessenberg column from the two Gram-Schmidt
+// passes h1, h2 and the new vector's squared norm nrm, rotations, residual
+// estimate, stopping test, scale = 1/||w|| for the systems that go on), and
+// the back-substitution into the combination coefficients.  H (M+1) x M per
+// system, column-major; cs, sn M, sv M+1 per system; all complex (re, im).
+cudaError_t launch_gmres_givens(int it, int M, int nsys, const double* h1, const double* h2,
+                                const double* nrm, const double* zid, double* H, double* cs,
+                                double* sn, double* sv, const double* bnorm, const double* eps,
+                                int64_t* done, int* brk, double* errs, double* scale,
+                                cudaStream_t st);
+cudaError_t launch_gmres_backsolve(int M, int nsys, int mused, const double* H, const double* sv,
+                                   const int64_t* done, double* coef, cudaStream_t st);
 // y[e] = sum_k c[k, sys(e)] V_k[e]
 cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
                          int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st);

@@ -1775,6 +1775,134 @@ cudaError_t launch_axpbys(const double* x, double* y, const double* a, double br
   return cudaGetLastError();
 }
 
+// ---- GMRES least squares on the device (FP64) -------------------------------
+// Complex values as (re, im) pairs; one thread per system.
+struct Z {
+  double r, i;
+};
+__device__ __forceinline__ Z zmul(Z a, Z b) { return {a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
+__device__ __forceinline__ Z zadd(Z a, Z b) { return {a.r + b.r, a.i + b.i}; }
+__device__ __forceinline__ Z zconj(Z a) { return {a.r, -a.i}; }
+__device__ __forceinline__ Z zdiv(Z a, Z b) {
+  const double d = b.r * b.r + b.i * b.i;
+  return {(a.r * b.r + a.i * b.i) / d, (a.i * b.r - a.r * b.i) / d};
+}
+__device__ __forceinline__ Z zld(const double* p) { return {p[0], p[1]}; }
+__device__ __forceinline__ void zst(double* p, Z v) {
+  p[0] = v.r;
+  p[1] = v.i;
+}
+
+// Iteration it of every active system: the new Hessenberg column
+// H(0..it, it) = h1 + h2 (the two Gram-Schmidt passes) with zid on the
+// diagonal, the previous Givens rotations applied, the new rotation
+// (zrotmat_gmres, rotmat_gmres.f:60-100) against the norm of the new
+// vector, the rotated residual vector s, the residual estimate
+// |s(it+1)| / ||rhs||, and the stopping test; scale = 1/||w|| for the
+// systems that go on (0 for the others).  done[q]: 0 active, > 0 iterations
+// taken, < 0 zero right-hand side; brk[q] = 1 on a NaN (breakdown).
+__global__ void gmres_givens_kernel(int it, int M, int nsys, const double* __restrict__ h1,
+                                    const double* __restrict__ h2,
+                                    const double* __restrict__ nrm,
+                                    const double* __restrict__ zid, double* __restrict__ H,
+                                    double* __restrict__ cs, double* __restrict__ sn,
+                                    double* __restrict__ sv, const double* __restrict__ bnorm,
+                                    const double* __restrict__ eps, int64_t* __restrict__ done,
+                                    int* __restrict__ brk, double* __restrict__ errs,
+                                    double* __restrict__ scale) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsys) return;
+  scale[2 * q] = 0.0;
+  scale[2 * q + 1] = 0.0;
+  if (done[q] != 0) return;
+  double* Hq = H + 2 * (size_t(q) * M + it) * (M + 1);  // column it of system q
+  for (int k = 0; k <= it; ++k)
+    zst(Hq + 2 * k, zadd(zld(h1 + 2 * (size_t(k) * nsys + q)), zld(h2 + 2 * (size_t(k) * nsys + q))));
+  zst(Hq + 2 * it, zadd(zld(Hq + 2 * it), zld(zid + 2 * q)));
+  const double wnrm = sqrt(fmax(nrm[2 * q], 0.0));
+  double* cq = cs + 2 * size_t(q) * M;
+  double* sq = sn + 2 * size_t(q) * M;
+  double* vq = sv + 2 * size_t(q) * (M + 1);
+  for (int k = 0; k < it; ++k) {
+    const Z c = zld(cq + 2 * k), s = zld(sq + 2 * k);
+    const Z a = zld(Hq + 2 * k), b = zld(Hq + 2 * (k + 1));
+    zst(Hq + 2 * k, zadd(zmul(c, a), zmul(zconj(s), b)));
+    const Z ms = {-s.r, -s.i};
+    zst(Hq + 2 * (k + 1), zadd(zmul(ms, a), zmul(c, b)));
+  }
+  const Z a = zld(Hq + 2 * it);
+  Z c, s;
+  if (a.r == 0.0 && a.i == 0.0) {
+    c = {0.0, 0.0};
+    s = {1.0, 0.0};
+  } else {
+    const Z t = zdiv(Z{wnrm, 0.0}, a);
+    const double cr = 1.0 / sqrt(1.0 + t.r * t.r + t.i * t.i);
+    c = {cr, 0.0};
+    s = {t.r * cr, t.i * cr};
+  }
+  zst(cq + 2 * it, c);
+  zst(sq + 2 * it, s);
+  zst(Hq + 2 * it, zadd(zmul(c, a), zmul(zconj(s), Z{wnrm, 0.0})));
+  const Z v = zld(vq + 2 * it);
+  zst(vq + 2 * (it + 1), Z{-(s.r * v.r - s.i * v.i), -(s.r * v.i + s.i * v.r)});
+  zst(vq + 2 * it, zmul(c, v));
+  const Z vn = zld(vq + 2 * (it + 1));
+  const double err = bnorm[q] > 0.0 ? sqrt(vn.r * vn.r + vn.i * vn.i) / bnorm[q] : 0.0;
+  errs[size_t(q) * (M + 1) + it] = err;
+  if (!(err == err) || !(wnrm == wnrm)) {
+    brk[q] = 1;
+    done[q] = it + 1;
+    return;
+  }
+  if (err <= eps[q] || it == M - 1 || wnrm == 0.0) {
+    done[q] = it + 1;
+    return;
+  }
+  scale[2 * q] = 1.0 / wnrm;
+}
+
+// y = triu(H)^-1 s over the done[q] iterations of system q, written as the
+// combination coefficients coef[2 (j nsys + q)], j < mused (zero past done[q]).
+__global__ void gmres_backsolve_kernel(int M, int nsys, int mused, const double* __restrict__ H,
+                                       const double* __restrict__ sv,
+                                       const int64_t* __restrict__ done,
+                                       double* __restrict__ coef) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsys) return;
+  const int k = done[q] > 0 ? int(done[q]) : 0;
+  for (int j = k; j < mused; ++j) zst(coef + 2 * (size_t(j) * nsys + q), Z{0.0, 0.0});
+  const double* Hq = H + 2 * size_t(q) * M * (M + 1);
+  const double* vq = sv + 2 * size_t(q) * (M + 1);
+  for (int j = k - 1; j >= 0; --j) {
+    Z acc = zld(vq + 2 * j);
+    for (int l = j + 1; l < k; ++l) {
+      const Z h = zld(Hq + 2 * (size_t(l) * (M + 1) + j));
+      const Z y = zld(coef + 2 * (size_t(l) * nsys + q));
+      acc = {acc.r - (h.r * y.r - h.i * y.i), acc.i - (h.r * y.i + h.i * y.r)};
+    }
+    zst(coef + 2 * (size_t(j) * nsys + q), zdiv(acc, zld(Hq + 2 * (size_t(j) * (M + 1) + j))));
+  }
+}
+
+cudaError_t launch_gmres_givens(int it, int M, int nsys, const double* h1, const double* h2,
+                                const double* nrm, const double* zid, double* H, double* cs,
+                                double* sn, double* sv, const double* bnorm, const double* eps,
+                                int64_t* done, int* brk, double* errs, double* scale,
+                                cudaStream_t st) {
+  gmres_givens_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(it, M, nsys, h1, h2, nrm, zid, H, cs, sn, sv,
+                                                       bnorm, eps, done, brk, errs, scale);
+  count();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gmres_backsolve(int M, int nsys, int mused, const double* H, const double* sv,
+                                   const int64_t* done, double* coef, cudaStream_t st) {
+  gmres_backsolve_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(M, nsys, mused, H, sv, done, coef);
+  count();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
                          int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st) {
   if (cplx)

@@ -124,6 +124,11 @@ struct PlanSpec {
 
 struct GmresWorkspace {
   DBuf<double> V, w, partial, dots, coef, scale;
+  // least squares on the device: Hessenberg columns, rotations, residual
+  // vector, norms, tolerances and error history per system
+  DBuf<double> ls;
+  DBuf<int64_t> done;
+  DBuf<int> brk;
 };
 
 struct MixedWorkspace {

@@ -24,18 +24,6 @@ namespace {
     }                                                                              \
   } while (0)
 
-// zrotmat_gmres (rotmat_gmres.f:60-100)
-inline void rotmat(cdouble a, cdouble b, cdouble& c, cdouble& s) {
-  if (a == cdouble(0)) {
-    s = 1.0;
-    c = 0.0;
-  } else {
-    const cdouble t = b / a;
-    c = 1.0 / std::sqrt(1.0 + std::norm(t));
-    s = t * c;
-  }
-}
-
 // host complex per system -> interleaved doubles
 std::vector<double> interleave(const std::vector<cdouble>& v) {
   std::vector<double> o(2 * v.size());
@@ -156,25 +144,44 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
   }
   BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
   BIE_CUDA(dev::launch_dscale(V, V, ws.scale.p, n, nd, cplx, sg, st));
-  // per-system Hessenberg columns, rotations and residual vector
+  // Per-system Hessenberg columns, rotations and residual vector live on the
+  // device; the Givens step and the back-substitution run there in FP64, and
+  // the host reads back only the per-system stop flags each iteration.
   const int64_t M = numit;
-  std::vector<cdouble> H(size_t(nsys) * (M + 1) * M), cs(size_t(nsys) * M), sn(size_t(nsys) * M),
-      sv(size_t(nsys) * (M + 1));
+  const size_t nH = size_t(2) * nsys * (M + 1) * M, nR = size_t(2) * nsys * M,
+               nS = size_t(2) * nsys * (M + 1), nE = size_t(nsys) * (M + 1);
+  BIE_CUDA(ws.ls.alloc(nH + 2 * nR + nS + 2 * size_t(nsys) + nE));
+  BIE_CUDA(ws.done.alloc(nsys));
+  BIE_CUDA(ws.brk.alloc(nsys));
+  double* d_H = ws.ls.p;
+  double* d_cs = d_H + nH;
+  double* d_sn = d_cs + nR;
+  double* d_sv = d_sn + nR;
+  double* d_bnorm = d_sv + nS;
+  double* d_eps = d_bnorm + nsys;
+  double* d_errs = d_eps + nsys;
   std::vector<int64_t> done(nsys, 0);
-  out.niter.assign(nsys, 0);
-  out.errs.assign(size_t(nsys) * (M + 1), 0.0);
-  out.rres.assign(nsys, 0.0);
-  out.status = kOk;
+  std::vector<double> sv0(2 * nsys, 0.0), epsv(nsys);
   int nactive = 0;
   for (int q = 0; q < nsys; ++q) {
-    sv[size_t(q) * (M + 1)] = rb[q];
+    sv0[2 * q] = rb[q];
+    epsv[q] = eps_sys ? eps_sys[q] : eps_gmres;
     if (rb[q] == 0.0) done[q] = -1;  // zero right-hand side: solution 0
     else ++nactive;
   }
-  auto Hc = [&](int q, int64_t row, int64_t col) -> cdouble& {
-    return H[(size_t(q) * M + col) * (M + 1) + row];
-  };
-  std::vector<double> hh1(2 * (M + 1) * nsys), hh2(2 * (M + 1) * nsys), hn(2 * nsys);
+  // s(0) of system q = ||r0||; the rest of s is written as the rotations go
+  BIE_CUDA(cudaMemcpy2DAsync(d_sv, 2 * (M + 1) * sizeof(double), sv0.data(), 2 * sizeof(double),
+                             2 * sizeof(double), nsys, cudaMemcpyHostToDevice, st));
+  BIE_CUDA(cudaMemcpyAsync(d_bnorm, bnorm.data(), nsys * sizeof(double), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(cudaMemcpyAsync(d_eps, epsv.data(), nsys * sizeof(double), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(cudaMemcpyAsync(ws.done.p, done.data(), nsys * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  BIE_CUDA(cudaMemsetAsync(d_errs, 0, nE * sizeof(double), st));
+  BIE_CUDA(cudaMemsetAsync(ws.brk.p, 0, nsys * sizeof(int), st));
+  out.niter.assign(nsys, 0);
+  out.errs.assign(nE, 0.0);
+  out.rres.assign(nsys, 0.0);
+  out.status = kOk;
+  std::vector<double> hn(2 * nsys);
   int64_t it = 0;
   for (; it < M && nactive > 0; ++it) {
     double* vit = V + size_t(it) * ldv;
@@ -193,76 +200,36 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
     BIE_CUDA(dev::launch_mdot(V, ldv, m, ws.w.p, wts, nd, cplx, sg, ws.partial.p, d_h2, st));
     BIE_CUDA(dev::launch_maxpy(V, ldv, m, d_h2, ws.w.p, n, nd, cplx, sg, st));
     BIE_CUDA(dev::launch_mdot(ws.w.p, ldv, 1, ws.w.p, wts, nd, cplx, sg, ws.partial.p, d_nrm, st));
-    BIE_CUDA(cudaMemcpyAsync(hh1.data(), d_h1, 2 * m * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaMemcpyAsync(hh2.data(), d_h2, 2 * m * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaMemcpyAsync(hn.data(), d_nrm, 2 * nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
-    BIE_CUDA(cudaStreamSynchronize(st));
-    for (int q = 0; q < nsys; ++q) {
-      hscale[2 * q] = 0.0;
-      hscale[2 * q + 1] = 0.0;
-      if (done[q] != 0) continue;
-      for (int k = 0; k < m; ++k)
-        Hc(q, k, it) = cdouble(hh1[2 * (k * nsys + q)] + hh2[2 * (k * nsys + q)],
-                               hh1[2 * (k * nsys + q) + 1] + hh2[2 * (k * nsys + q) + 1]);
-      Hc(q, it, it) += zv[q];
-      const double wnrm = std::sqrt(std::max(hn[2 * q], 0.0));
-      cdouble* c = cs.data() + size_t(q) * M;
-      cdouble* s = sn.data() + size_t(q) * M;
-      cdouble* svq = sv.data() + size_t(q) * (M + 1);
-      for (int64_t k = 0; k < it; ++k) {
-        const cdouble t = c[k] * Hc(q, k, it) + std::conj(s[k]) * Hc(q, k + 1, it);
-        Hc(q, k + 1, it) = -s[k] * Hc(q, k, it) + c[k] * Hc(q, k + 1, it);
-        Hc(q, k, it) = t;
-      }
-      rotmat(Hc(q, it, it), cdouble(wnrm), c[it], s[it]);
-      Hc(q, it, it) = c[it] * Hc(q, it, it) + std::conj(s[it]) * wnrm;
-      svq[it + 1] = -s[it] * svq[it];
-      svq[it] = c[it] * svq[it];
-      const double err = bnorm[q] > 0 ? std::abs(svq[it + 1]) / bnorm[q] : 0.0;
-      out.errs[size_t(q) * (M + 1) + it] = err;
-      if (!(err == err) || !(wnrm == wnrm)) {
-        out.status = kBreakdown;
-        done[q] = it + 1;
-        --nactive;
-        continue;
-      }
-      if (err <= (eps_sys ? eps_sys[q] : eps_gmres) || it == M - 1 || wnrm == 0.0) {
-        done[q] = it + 1;
-        --nactive;
-        continue;
-      }
-      hscale[2 * q] = 1.0 / wnrm;
-    }
-    BIE_CUDA(cudaMemcpyAsync(ws.scale.p, hscale.data(), 2 * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
+    BIE_CUDA(dev::launch_gmres_givens(int(it), int(M), nsys, d_h1, d_h2, d_nrm, d_zid, d_H, d_cs,
+                                      d_sn, d_sv, d_bnorm, d_eps, ws.done.p, ws.brk.p, d_errs,
+                                      ws.scale.p, st));
     BIE_CUDA(dev::launch_dscale(ws.w.p, vnext, ws.scale.p, n, nd, cplx, sg, st));
+    BIE_CUDA(cudaMemcpyAsync(done.data(), ws.done.p, nsys * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    BIE_CUDA(cudaStreamSynchronize(st));
+    nactive = 0;
+    for (int q = 0; q < nsys; ++q) nactive += done[q] == 0 ? 1 : 0;
   }
   {
     int ier = P.set_active(std::vector<uint8_t>(sg.nseg, 1), st);
     if (ier) return ier;
   }
-  // back-substitution per system: y = triu(H)\s, soln = V y (+ x0)
-  std::vector<double> hc(size_t(2) * (M + 1) * nsys, 0.0);
+  // back-substitution per system on the device: y = triu(H)\s, soln = V y (+ x0)
+  const int mused = int(std::max<int64_t>(it, 1));
+  BIE_CUDA(dev::launch_gmres_backsolve(int(M), nsys, mused, d_H, d_sv, ws.done.p, ws.coef.p, st));
+  BIE_CUDA(dev::launch_combo(V, ldv, mused, ws.coef.p, d_soln, n, nd, cplx, sg, st));
+  std::vector<int> brk(nsys);
+  BIE_CUDA(cudaMemcpyAsync(out.errs.data(), d_errs, nE * sizeof(double), cudaMemcpyDeviceToHost, st));
+  BIE_CUDA(cudaMemcpyAsync(brk.data(), ws.brk.p, nsys * sizeof(int), cudaMemcpyDeviceToHost, st));
+  BIE_CUDA(cudaStreamSynchronize(st));
+  for (int q = 0; q < nsys; ++q)
+    if (brk[q]) out.status = kBreakdown;
   for (int q = 0; q < nsys; ++q) {
     if (done[q] <= 0) continue;
     const int64_t k = done[q];
-    std::vector<cdouble> y(k);
-    const cdouble* svq = sv.data() + size_t(q) * (M + 1);
-    for (int64_t j = k - 1; j >= 0; --j) {
-      cdouble acc = svq[j];
-      for (int64_t l = j + 1; l < k; ++l) acc -= Hc(q, j, l) * y[l];
-      y[j] = acc / Hc(q, j, j);
-    }
-    for (int64_t j = 0; j < k; ++j) {
-      hc[2 * (j * nsys + q)] = y[j].real();
-      hc[2 * (j * nsys + q) + 1] = y[j].imag();
-    }
     out.niter[q] = k;
-    if (out.errs[size_t(q) * (M + 1) + k - 1] > (eps_sys ? eps_sys[q] : eps_gmres) && out.status == kOk)
+    if (out.errs[size_t(q) * (M + 1) + k - 1] > epsv[q] && out.status == kOk)
       out.status = kNotConverged;
   }
-  const int mused = int(std::max<int64_t>(it, 1));
-  BIE_CUDA(cudaMemcpyAsync(ws.coef.p, hc.data(), 2 * mused * nsys * sizeof(double), cudaMemcpyHostToDevice, st));
-  BIE_CUDA(dev::launch_combo(V, ldv, mused, ws.coef.p, d_soln, n, nd, cplx, sg, st));
   if (d_x0) BIE_CUDA(dev::launch_axpby(d_x0, d_soln, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
   // rres = || zid x + K x - rhs ||_w / ||rhs||_w   (one more matvec)
   if (rres_precision >= 0) {
