@@ -203,6 +203,15 @@ cudaError_t launch_gmres_givens(int it, int M, int nsys, const double* h1, const
                                 cudaStream_t st);
 cudaError_t launch_gmres_backsolve(int M, int nsys, int mused, const double* H, const double* sv,
                                    const int64_t* done, double* coef, cudaStream_t st);
+// Krylov-basis coefficients (mcols per system) of each system's GMRES
+// residual vector r0 - A V y.
+cudaError_t launch_gmres_resvec(int M, int nsys, int mcols, const double* cs, const double* sn,
+                                const double* sv, const int64_t* done, double* z,
+                                cudaStream_t st);
+// kx += r - rn - zid[sys] d
+cudaError_t launch_kx_update(double* kx, const double* r, const double* rn, const double* d,
+                             const double* zid, int64_t n, int nd, int cplx, const Segs& sg,
+                             cudaStream_t st);
 // y[e] = sum_k c[k, sys(e)] V_k[e]
 cudaError_t launch_combo(const double* V, int64_t ldv, int m, const double* c, double* y,
                          int64_t n, int nd, int cplx, const Segs& sg, cudaStream_t st);

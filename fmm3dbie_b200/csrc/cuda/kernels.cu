@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <atomic>
 #include <mutex>
+#include <type_traits>
 #include <cmath>
 
 #include "device.cuh"
@@ -227,22 +228,183 @@ __device__ __forceinline__ void far_block(const Geometry& g, const KParams& kp,
 }
 
 
+// FP32 far field with two targets per packed instruction (pair_helm_x2,
+// pair_lap_x2): the work, the coordinate shift, the tile boxes and the
+// threshold test of far_block<float>, with the source tile in shared memory
+// holding every value twice (kFarX2Words float4 per source, source-major, so
+// the threads of a warp read one source as a broadcast).
+template <int KIND>
+constexpr int kFarX2Words = KIND == 1 ? 6 : 4;
+
+template <int KIND, int NT, int TPT, int TILE, bool CK>
+__device__ __forceinline__ void far_block_x2(const Geometry& g, const KParams& kp,
+                                             const float* __restrict__ str,
+                                             double* __restrict__ partial, int64_t chunk_len,
+                                             int nd, int64_t bx, int64_t by, int bz,
+                                             float4* tile) {
+  static_assert(TPT % 2 == 0, "targets are taken in pairs");
+  constexpr int SW = (KIND == 1) ? 4 : 2;  // strength reals per source
+  constexpr int W = kFarX2Words<KIND>;
+  constexpr int TP = TPT / 2;  // target pairs per thread
+  const int64_t ntarg = g.ntarg, nptso = g.nptso;
+  const int64_t tbase = int64_t(bx) * NT * TPT;
+  const int m = bz;
+  const int64_t tc = tbase < ntarg ? tbase : ntarg - 1;
+  const double cx = g.tx[tc], cy = g.ty[tc], cz = g.tz[tc];
+  float2 tx[TP], ty[TP], tz[TP];
+  double accr[TPT], acci[TPT];
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    const int64_t it = tbase + threadIdx.x + int64_t(t) * NT;
+    const int64_t ic = it < ntarg ? it : ntarg - 1;
+    const float x = float(g.tx[ic] - cx), y = float(g.ty[ic] - cy), z = float(g.tz[ic] - cz);
+    if (t % 2 == 0) {
+      tx[t / 2].x = x;
+      ty[t / 2].x = y;
+      tz[t / 2].x = z;
+    } else {
+      tx[t / 2].y = x;
+      ty[t / 2].y = y;
+      tz[t / 2].y = z;
+    }
+    accr[t] = 0.0;
+    acci[t] = 0.0;
+  }
+  const float thr2 = float(kp.thresh * kp.thresh);
+  const float2 k2 = make_float2(float(kp.kr), float(kp.kr)),
+               kim2 = make_float2(float(kp.ki), float(kp.ki));
+  double tbx[6] = {0, 0, 0, 0, 0, 0};
+  const bool boxes = NT * TPT == kFarBlockTargets32 && g.sbox && g.tbox && TILE == kFarTileSources;
+  if (boxes)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tbx[c] = g.tbox[6 * (tbase / kFarBlockTargets32) + c];
+  const int64_t s0 = int64_t(by) * chunk_len;
+  const int64_t s1 = min(s0 + chunk_len, nptso);
+  for (int64_t sb = s0; sb < s1; sb += TILE) {
+    const int ns = int((s1 - sb) < TILE ? (s1 - sb) : TILE);
+    __syncthreads();
+    for (int q = threadIdx.x; q < TILE; q += NT) {
+      float4* T = tile + q * W;
+      if (q < ns) {
+        const int64_t s = sb + q;
+        const float x = -float(g.sx[s] - cx), y = -float(g.sy[s] - cy), z = -float(g.sz[s] - cz);
+        const float nx = float(g.snx[s]), ny = float(g.sny[s]), nz = float(g.snz[s]);
+        T[0] = make_float4(x, x, y, y);
+        T[1] = make_float4(z, z, nx, nx);
+        T[2] = make_float4(ny, ny, nz, nz);
+        const float* st = str + (size_t(s) * nd + m) * SW;
+        if constexpr (KIND == 1) {
+          const float4 v = *reinterpret_cast<const float4*>(st);
+          T[3] = make_float4(v.x, v.x, v.y, v.y);
+          T[4] = make_float4(v.z, v.z, v.w, v.w);
+          T[5] = make_float4(-v.z, -v.z, 0.f, 0.f);
+        } else {
+          T[3] = make_float4(st[0], st[0], st[1], st[1]);
+        }
+      } else {
+#pragma unroll
+        for (int w = 0; w < W; ++w) T[w] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+    __syncthreads();
+    float2 pa[TP], pb[TP], pi[TP];
+#pragma unroll
+    for (int t = 0; t < TP; ++t) pa[t] = pb[t] = pi[t] = make_float2(0.f, 0.f);
+    bool check = true;
+    if (boxes && ns == TILE) {
+      const double* sbx = g.sbox + 6 * (sb / kFarTileSources);
+      double gap2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double gap = fmax(fmax(sbx[c] - tbx[c + 3], tbx[c] - sbx[c + 3]), 0.0);
+        gap2 += gap * gap;
+      }
+      check = gap2 <= g.box_margin2;
+    }
+    auto sweep = [&](auto chk) {
+      constexpr bool C = decltype(chk)::value;
+#pragma unroll 2
+      for (int j = 0; j < TILE; ++j) {
+        const float4* T = tile + j * W;
+        const float4 q0 = T[0], q1 = T[1], q2 = T[2], q3 = T[3];
+        const float2 msx = make_float2(q0.x, q0.y), msy = make_float2(q0.z, q0.w),
+                     msz = make_float2(q1.x, q1.y), nx = make_float2(q1.z, q1.w),
+                     ny = make_float2(q2.x, q2.y), nz = make_float2(q2.z, q2.w);
+        if constexpr (KIND == 1) {
+          const float4 q4 = T[4];
+          const float2 q5 = *reinterpret_cast<const float2*>(T + 5);
+          const float2 cr = make_float2(q3.x, q3.y), ci = make_float2(q3.z, q3.w),
+                       dr = make_float2(q4.x, q4.y), di = make_float2(q4.z, q4.w);
+#pragma unroll
+          for (int t = 0; t < TP; ++t)
+            pair_helm_x2<C>(tx[t], ty[t], tz[t], msx, msy, msz, nx, ny, nz, cr, ci, dr, di, q5, k2,
+                            kim2, thr2, CK, pa[t], pb[t], pi[t]);
+        } else {
+          const float2 c = make_float2(q3.x, q3.y), d = make_float2(q3.z, q3.w);
+#pragma unroll
+          for (int t = 0; t < TP; ++t)
+            pair_lap_x2<C>(tx[t], ty[t], tz[t], msx, msy, msz, nx, ny, nz, c, d, thr2, pa[t]);
+        }
+      }
+    };
+    if (check)
+      sweep(std::true_type{});
+    else
+      sweep(std::false_type{});
+#pragma unroll
+    for (int t = 0; t < TP; ++t) {
+      accr[2 * t] += double(pa[t].x) - double(pb[t].x);
+      accr[2 * t + 1] += double(pa[t].y) - double(pb[t].y);
+      acci[2 * t] += double(pi[t].x);
+      acci[2 * t + 1] += double(pi[t].y);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < TPT; ++t) {
+    const int64_t it = tbase + threadIdx.x + int64_t(t) * NT;
+    if (it >= ntarg) continue;
+    const size_t o = (size_t(by) * ntarg + it) * nd + m;
+    if (KIND == 1) {
+      partial[2 * o] = accr[t];
+      partial[2 * o + 1] = acci[t];
+    } else {
+      partial[o] = accr[t];
+    }
+  }
+}
+
+
+// Blocks per SM the 128-thread shapes are compiled for.  FP32: a register
+// budget of 96 (5 blocks, 20 warps per SM) measured 2 % faster on the
+// 35,840-node Helmholtz matvec than the unconstrained 123 registers (4
+// blocks), with no spills; 80 and 64 registers measured no faster.  FP64: 128
+// registers (4 blocks) measured 2 % faster than the unconstrained 146 (3
+// blocks).
+template <typename R, int NT>
+constexpr int kFarMinBlocks = NT == 128 ? (sizeof(R) == 4 ? 5 : 4) : 1;
+
 template <int KIND, typename R, int NT, int TPT, int TILE, bool CK>
-__global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R* __restrict__ str,
+__global__ void __launch_bounds__(NT, (kFarMinBlocks<R, NT>)) far_kernel(Geometry g, KParams kp, const R* __restrict__ str,
                                                  double* __restrict__ partial, int64_t chunk_len,
                                                  int nd) {
   constexpr int SW = (KIND == 1) ? 4 : 2;
-  __shared__ typename Vec<R>::T4 sg0[TILE];
-  __shared__ typename Vec<R>::T2 sg1[TILE];
-  __shared__ R sst[TILE * SW];
-  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
-  const double2* tab = nullptr;
-  if constexpr (sizeof(R) == 8 && KIND == 1) {
-    fill_trig_table(stab);  // published by the first __syncthreads of the tile loop
-    tab = stab;
+  if constexpr (sizeof(R) == 4) {
+    __shared__ float4 tile[TILE * kFarX2Words<KIND>];
+    far_block_x2<KIND, NT, TPT, TILE, CK>(g, kp, str, partial, chunk_len, nd, blockIdx.x,
+                                          blockIdx.y, blockIdx.z, tile);
+  } else {
+    __shared__ typename Vec<R>::T4 sg0[TILE];
+    __shared__ typename Vec<R>::T2 sg1[TILE];
+    __shared__ R sst[TILE * SW];
+    __shared__ double2 stab[KIND == 1 ? kFarTrigN : 1];
+    const double2* tab = nullptr;
+    if constexpr (KIND == 1) {
+      fill_far_trig_table(stab);  // published by the first __syncthreads of the tile loop
+      tab = stab;
+    }
+    far_block<KIND, R, NT, TPT, TILE, CK>(g, kp, str, partial, chunk_len, nd, blockIdx.x,
+                                          blockIdx.y, blockIdx.z, tab, sg0, sg1, sst);
   }
-  far_block<KIND, R, NT, TPT, TILE, CK>(g, kp, str, partial, chunk_len, nd, blockIdx.x, blockIdx.y,
-                                        blockIdx.z, tab, sg0, sg1, sst);
 }
 
 // ---------------------------------------------------------------------------
@@ -258,6 +420,7 @@ __global__ void __launch_bounds__(NT) far_kernel(Geometry g, KParams kp, const R
 // ab: per source (a, b) (complex: 4 reals, real: 2); sig: sigma_over[s][nd].
 // ---------------------------------------------------------------------------
 constexpr int kMdCentre = 512;
+
 
 // One block's work of the multi-density far field: target block bx, source
 // chunk by, density group bz (MD densities).  Shared tiles and the FP64 trig
@@ -320,51 +483,87 @@ __device__ __forceinline__ void far_md_block(const Geometry& g, const KParams& k
         ssig[q * C + c] = ok ? sig[(size_t(sb + qs) * nd + m0 + mm) * C + c] : R(0);
     }
     __syncthreads();
-    R tr[TPT][MD][C];
+    if constexpr (sizeof(R) == 4 && KIND == 0) {
+      // FP32 Laplace: two densities per packed multiply-add (fma.rn.f32x2,
+      // each lane rounded as the scalar form).  (The Helmholtz densities stay
+      // scalar: a packed complex multiply-add needs the density twice in
+      // shared memory, (re, im) and (im, re), and with MD = 16 that layout
+      // and its registers measured 20 % slower.)
+      constexpr int NP = MD / 2;
+      float2 tr2[TPT][NP];
 #pragma unroll
-    for (int t = 0; t < TPT; ++t)
+      for (int t = 0; t < TPT; ++t)
 #pragma unroll
-      for (int m = 0; m < MD; ++m)
-#pragma unroll
-        for (int c = 0; c < C; ++c) tr[t][m][c] = R(0);
+        for (int m = 0; m < NP; ++m) tr2[t][m] = make_float2(0.f, 0.f);
 #pragma unroll 2
-    for (int j = 0; j < TILE; ++j) {
-      const R4 a = sg0[j];
-      const R2 b = sg1[j];
-      if constexpr (KIND == 1) {
-        const R4 s = reinterpret_cast<const R4*>(sab)[j];
+      for (int j = 0; j < TILE; ++j) {
+        const R4 a = sg0[j];
+        const R2 b = sg1[j];
+        const R2 sv2 = reinterpret_cast<const R2*>(sab)[j];
+        const float2* sv = reinterpret_cast<const float2*>(ssig + j * MD);
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
-          R kr_ = R(0), ki_ = R(0);
-          pair_helm(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, kr_, ki_, tab);
-          const R4* sv = reinterpret_cast<const R4*>(ssig) + j * (MD / 2);
+          float kv = 0.f;
+          pair_lap<R>(tx[t], ty[t], tz[t], a, b, sv2, thr2, kv);
+          const float2 kk = make_float2(kv, kv);
 #pragma unroll
-          for (int m2 = 0; m2 < MD / 2; ++m2) {
-            const R4 x = sv[m2];  // densities 2*m2 and 2*m2+1
-            tr[t][2 * m2][0] = fma(kr_, x.x, fma(-ki_, x.y, tr[t][2 * m2][0]));
-            tr[t][2 * m2][1] = fma(kr_, x.y, fma(ki_, x.x, tr[t][2 * m2][1]));
-            tr[t][2 * m2 + 1][0] = fma(kr_, x.z, fma(-ki_, x.w, tr[t][2 * m2 + 1][0]));
-            tr[t][2 * m2 + 1][1] = fma(kr_, x.w, fma(ki_, x.z, tr[t][2 * m2 + 1][1]));
-          }
-        }
-      } else {
-        const R2 s = reinterpret_cast<const R2*>(sab)[j];
-#pragma unroll
-        for (int t = 0; t < TPT; ++t) {
-          R kv = R(0);
-          pair_lap<R>(tx[t], ty[t], tz[t], a, b, s, thr2, kv);
-          const R* sv = ssig + j * MD;
-#pragma unroll
-          for (int m = 0; m < MD; ++m) tr[t][m][0] = fma(kv, sv[m], tr[t][m][0]);
+          for (int m = 0; m < NP; ++m) tr2[t][m] = __ffma2_rn(kk, sv[m], tr2[t][m]);
         }
       }
+#pragma unroll
+      for (int t = 0; t < TPT; ++t)
+#pragma unroll
+        for (int m = 0; m < NP; ++m) {
+          acc[t][2 * m][0] += double(tr2[t][m].x);
+          acc[t][2 * m + 1][0] += double(tr2[t][m].y);
+        }
+    } else {
+      R tr[TPT][MD][C];
+#pragma unroll
+      for (int t = 0; t < TPT; ++t)
+#pragma unroll
+        for (int m = 0; m < MD; ++m)
+#pragma unroll
+          for (int c = 0; c < C; ++c) tr[t][m][c] = R(0);
+#pragma unroll 2
+      for (int j = 0; j < TILE; ++j) {
+        const R4 a = sg0[j];
+        const R2 b = sg1[j];
+        if constexpr (KIND == 1) {
+          const R4 s = reinterpret_cast<const R4*>(sab)[j];
+#pragma unroll
+          for (int t = 0; t < TPT; ++t) {
+            R kr_ = R(0), ki_ = R(0);
+            pair_helm(tx[t], ty[t], tz[t], a, b, s, k, kim, thr2, CK, kr_, ki_, tab);
+            const R4* sv = reinterpret_cast<const R4*>(ssig) + j * (MD / 2);
+#pragma unroll
+            for (int m2 = 0; m2 < MD / 2; ++m2) {
+              const R4 x = sv[m2];  // densities 2*m2 and 2*m2+1
+              tr[t][2 * m2][0] = fma(kr_, x.x, fma(-ki_, x.y, tr[t][2 * m2][0]));
+              tr[t][2 * m2][1] = fma(kr_, x.y, fma(ki_, x.x, tr[t][2 * m2][1]));
+              tr[t][2 * m2 + 1][0] = fma(kr_, x.z, fma(-ki_, x.w, tr[t][2 * m2 + 1][0]));
+              tr[t][2 * m2 + 1][1] = fma(kr_, x.w, fma(ki_, x.z, tr[t][2 * m2 + 1][1]));
+            }
+          }
+        } else {
+          const R2 s = reinterpret_cast<const R2*>(sab)[j];
+#pragma unroll
+          for (int t = 0; t < TPT; ++t) {
+            R kv = R(0);
+            pair_lap<R>(tx[t], ty[t], tz[t], a, b, s, thr2, kv);
+            const R* sv = ssig + j * MD;
+#pragma unroll
+            for (int m = 0; m < MD; ++m) tr[t][m][0] = fma(kv, sv[m], tr[t][m][0]);
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < TPT; ++t)
+#pragma unroll
+        for (int m = 0; m < MD; ++m)
+#pragma unroll
+          for (int c = 0; c < C; ++c) acc[t][m][c] += double(tr[t][m][c]);
     }
-#pragma unroll
-    for (int t = 0; t < TPT; ++t)
-#pragma unroll
-      for (int m = 0; m < MD; ++m)
-#pragma unroll
-        for (int c = 0; c < C; ++c) acc[t][m][c] += double(tr[t][m][c]);
   }
 #pragma unroll
   for (int t = 0; t < TPT; ++t) {
@@ -391,10 +590,10 @@ __global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
   __shared__ typename Vec<R>::T2 sg1[TILE];
   __shared__ __align__(16) R sab[TILE * 2 * C];
   __shared__ __align__(16) R ssig[TILE * MD * C];
-  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kFarTrigN : 1];
   const double2* tab = nullptr;
   if constexpr (sizeof(R) == 8 && KIND == 1) {
-    fill_trig_table(stab);  // published by the first __syncthreads of the tile loop
+    fill_far_trig_table(stab);  // published by the first __syncthreads of the tile loop
     tab = stab;
   }
   far_md_block<KIND, R, NT, TPT, MD, TILE, CK>(g, kp, ab, sig, nd, partial, chunk_len, blockIdx.x,
@@ -1311,13 +1510,15 @@ __global__ void __launch_bounds__(NT)
                      const R* __restrict__ str, double* __restrict__ partial, int nd, int prec,
                      int* __restrict__ counter) {
   constexpr int SW = (KIND == 1) ? 4 : 2;
-  __shared__ typename Vec<R>::T4 sg0[TILE];
-  __shared__ typename Vec<R>::T2 sg1[TILE];
-  __shared__ R sst[TILE * SW];
-  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  constexpr bool X2 = sizeof(R) == 4;
+  __shared__ float4 tile[X2 ? TILE * kFarX2Words<KIND> : 1];
+  __shared__ typename Vec<R>::T4 sg0[X2 ? 1 : TILE];
+  __shared__ typename Vec<R>::T2 sg1[X2 ? 1 : TILE];
+  __shared__ R sst[X2 ? 1 : TILE * SW];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kFarTrigN : 1];
   const double2* tab = nullptr;
   if constexpr (sizeof(R) == 8 && KIND == 1) {
-    fill_trig_table(stab);
+    fill_far_trig_table(stab);
     tab = stab;
   }
   __syncthreads();
@@ -1330,9 +1531,13 @@ __global__ void __launch_bounds__(NT)
     if (S.live && *S.live == 0) continue;  // uniform over the block
     const Geometry g = S.g;
     const KParams kp = S.kp;
-    far_block<KIND, R, NT, TPT, TILE, CK>(g, kp, str + S.sofs * nd * SW, partial + S.pofs[prec],
-                                          S.chunk_len[prec], nd, it.y, it.z, it.w, tab, sg0, sg1,
-                                          sst);
+    if constexpr (X2)
+      far_block_x2<KIND, NT, TPT, TILE, CK>(g, kp, str + S.sofs * nd * SW, partial + S.pofs[prec],
+                                            S.chunk_len[prec], nd, it.y, it.z, it.w, tile);
+    else
+      far_block<KIND, R, NT, TPT, TILE, CK>(g, kp, str + S.sofs * nd * SW,
+                                            partial + S.pofs[prec], S.chunk_len[prec], nd, it.y,
+                                            it.z, it.w, tab, sg0, sg1, sst);
     __syncthreads();
   }
 }
@@ -1347,10 +1552,10 @@ __global__ void __launch_bounds__(NT)
   __shared__ typename Vec<R>::T2 sg1[TILE];
   __shared__ __align__(16) R sab[TILE * 2 * C];
   __shared__ __align__(16) R ssig[TILE * MD * C];
-  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kFarTrigN : 1];
   const double2* tab = nullptr;
   if constexpr (sizeof(R) == 8 && KIND == 1) {
-    fill_trig_table(stab);
+    fill_far_trig_table(stab);
     tab = stab;
   }
   __syncthreads();
@@ -1855,11 +2060,10 @@ __global__ void gmres_givens_kernel(int it, int M, int nsys, const double* __res
     done[q] = it + 1;
     return;
   }
-  if (err <= eps[q] || it == M - 1 || wnrm == 0.0) {
-    done[q] = it + 1;
-    return;
-  }
-  scale[2 * q] = 1.0 / wnrm;
+  // the new Krylov vector is normalised also when the system stops here: it
+  // is the last vector of the basis that carries the residual vector
+  if (wnrm > 0.0) scale[2 * q] = 1.0 / wnrm;
+  if (err <= eps[q] || it == M - 1 || wnrm == 0.0) done[q] = it + 1;
 }
 
 // y = triu(H)^-1 s over the done[q] iterations of system q, written as the
@@ -1883,6 +2087,73 @@ __global__ void gmres_backsolve_kernel(int M, int nsys, int mused, const double*
     }
     zst(coef + 2 * (size_t(j) * nsys + q), zdiv(acc, zld(Hq + 2 * (size_t(j) * (M + 1) + j))));
   }
+}
+
+// Coefficients z (j = 0..done[q], zero up to mcols) of the GMRES residual
+// vector r0 - A V y = V Q^H (0, ..., 0, g_k)^T in the Krylov basis: the
+// last rotated residual entry g_k carried back through the rotations
+// (G_i^H on entries i, i+1, last rotation first).
+__global__ void gmres_resvec_kernel(int M, int nsys, int mcols, const double* __restrict__ cs,
+                                    const double* __restrict__ sn,
+                                    const double* __restrict__ sv,
+                                    const int64_t* __restrict__ done, double* __restrict__ z) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsys) return;
+  const int k = done[q] > 0 ? int(done[q]) : 0;
+  for (int j = k + 1; j < mcols; ++j) zst(z + 2 * (size_t(j) * nsys + q), Z{0.0, 0.0});
+  if (k == 0) {
+    zst(z + 2 * size_t(q), Z{0.0, 0.0});
+    return;
+  }
+  const double* cq = cs + 2 * size_t(q) * M;
+  const double* sq = sn + 2 * size_t(q) * M;
+  Z hi = zld(sv + 2 * (size_t(q) * (M + 1) + k));  // z_k = g_k
+  for (int i = k - 1; i >= 0; --i) {
+    // (z_i, z_{i+1}) <- (c z_i - conj(s) z_{i+1}, s z_i + c z_{i+1}), z_i = 0
+    const Z c = zld(cq + 2 * i), s = zld(sq + 2 * i);
+    zst(z + 2 * (size_t(i + 1) * nsys + q), zmul(c, hi));
+    hi = Z{-(s.r * hi.r + s.i * hi.i), -(s.r * hi.i - s.i * hi.r)};
+  }
+  zst(z + 2 * size_t(q), hi);
+}
+
+cudaError_t launch_gmres_resvec(int M, int nsys, int mcols, const double* cs, const double* sn,
+                                const double* sv, const int64_t* done, double* z,
+                                cudaStream_t st) {
+  gmres_resvec_kernel<<<(nsys + 63) / 64, 64, 0, st>>>(M, nsys, mcols, cs, sn, sv, done, z);
+  count();
+  return cudaGetLastError();
+}
+
+// kx += r - rn - zid d: the operator applied to a refinement correction d,
+// taken from the inner solve's own right-hand side r and residual rn.
+template <int CPLX>
+__global__ void kx_update_kernel(double* __restrict__ kx, const double* __restrict__ r,
+                                 const double* __restrict__ rn, const double* __restrict__ d,
+                                 const double* __restrict__ zid, int64_t n, int nd, Segs sg) {
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int sy = sys_of(sg, e, nd);
+    const double zr = zid[2 * sy], zi = zid[2 * sy + 1];
+    if (CPLX) {
+      const double dr = d[2 * e], di = d[2 * e + 1];
+      kx[2 * e] += r[2 * e] - rn[2 * e] - (zr * dr - zi * di);
+      kx[2 * e + 1] += r[2 * e + 1] - rn[2 * e + 1] - (zr * di + zi * dr);
+    } else {
+      kx[e] += r[e] - rn[e] - zr * d[e];
+    }
+  }
+}
+
+cudaError_t launch_kx_update(double* kx, const double* r, const double* rn, const double* d,
+                             const double* zid, int64_t n, int nd, int cplx, const Segs& sg,
+                             cudaStream_t st) {
+  if (cplx)
+    kx_update_kernel<1><<<grid_for(n, 256), 256, 0, st>>>(kx, r, rn, d, zid, n, nd, sg);
+  else
+    kx_update_kernel<0><<<grid_for(n, 256), 256, 0, st>>>(kx, r, rn, d, zid, n, nd, sg);
+  count();
+  return cudaGetLastError();
 }
 
 cudaError_t launch_gmres_givens(int it, int M, int nsys, const double* h1, const double* h2,

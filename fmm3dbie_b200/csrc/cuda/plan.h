@@ -129,10 +129,11 @@ struct GmresWorkspace {
   DBuf<double> ls;
   DBuf<int64_t> done;
   DBuf<int> brk;
+  DBuf<double> zc;  // Krylov-basis coefficients of the residual vector
 };
 
 struct MixedWorkspace {
-  DBuf<double> r, d, partial, nrm, kx;
+  DBuf<double> r, d, partial, nrm, kx, rn;
 };
 
 // Per-precision stage totals (index 0 = f64 matvecs, 1 = f32 matvecs).
@@ -331,9 +332,12 @@ struct GmresOut {
 // the final relative residual rres uses `rres_precision` (-1 skips it).
 // d_x0 (optional) is an initial guess.
 // eps_sys (optional): a relative tolerance per system in place of eps_gmres.
+// d_res (optional): receives rhs - (zid I + K) soln under the inner
+// operator, formed from the Krylov basis and the rotations (no matvec).
 int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble* zid,
           const double* d_rhs, const double* d_x0, int64_t numit, double eps_gmres,
-          double* d_soln, GmresOut& out, cudaStream_t st, const double* eps_sys = nullptr);
+          double* d_soln, GmresOut& out, cudaStream_t st, const double* eps_sys = nullptr,
+          double* d_res = nullptr);
 
 // Mixed-precision solve: FP64 residuals and iterative refinement around
 // FP32-matvec GMRES inner solves.  Stops when the FP64 relative residual
@@ -345,14 +349,17 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
 // step whose correction d is small, kFp32OpErr ||d||_w / ||x||_w <=
 // eps_target / 4 for every active system, adds the FP32 operator's K d to
 // it instead (FP32 error on a correction of relative size ||d||/||x||); any
-// other step applies the FP64 operator to x again.
+// other step applies the FP64 operator to x again.  The FP32 K d needs no
+// matvec: the inner GMRES returns its own residual vector rn = r - A32 d
+// (from the Arnoldi relation A32 V_m = V_{m+1} H), so K d = r - rn - zid d.
 struct MixedOut {
   std::vector<int64_t> inner_iters;  // total inner GMRES iterations per system
   std::vector<double> rres;          // final FP64 relative residual per system
   std::vector<int64_t> outer;        // refinement steps per system
   std::vector<int64_t> x0_dropped;   // 1 where the initial guess was replaced by 0
   int fp64_matvecs = 0, fp32_matvecs = 0;
-  int incr_matvecs = 0;              // FP32 applications to corrections (in fp32_matvecs)
+  int incr_matvecs = 0;              // refinement steps whose K d came from the inner
+                                     // solve's Krylov basis (no matvec)
   double max_incr_ratio = 0.0;       // largest ||d||_w / ||x||_w of an increment step
   int status = kOk;
 };
@@ -364,7 +371,7 @@ constexpr double kFp32OpErr = 1e-6;
 int mixed_residual_mode();
 void set_mixed_residual_mode(int mode);
 // statistics of the calling thread's last mixed solve: fp64 and fp32
-// matvecs, increment matvecs, largest increment ratio
+// matvecs, increment steps, largest increment ratio
 const MixedOut& last_mixed_out();
 int solve_mixed(Operator& P, int nd, const cdouble* zid, const double* d_rhs, const double* d_x0,
                 int64_t numit, double eps_target, double inner_floor, int max_outer,

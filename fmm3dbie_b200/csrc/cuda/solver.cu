@@ -83,7 +83,8 @@ int Operator::init_segments(cudaStream_t st) {
 
 int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble* zid,
           const double* d_rhs, const double* d_x0, int64_t numit, double eps_gmres,
-          double* d_soln, GmresOut& out, cudaStream_t st, const double* eps_sys) {
+          double* d_soln, GmresOut& out, cudaStream_t st, const double* eps_sys,
+          double* d_res) {
   if (!P.square()) {
     set_last_error("GMRES needs an operator whose targets are its nodes");
     return kErrArg;
@@ -217,6 +218,15 @@ int gmres(Operator& P, int precision, int rres_precision, int nd, const cdouble*
   const int mused = int(std::max<int64_t>(it, 1));
   BIE_CUDA(dev::launch_gmres_backsolve(int(M), nsys, mused, d_H, d_sv, ws.done.p, ws.coef.p, st));
   BIE_CUDA(dev::launch_combo(V, ldv, mused, ws.coef.p, d_soln, n, nd, cplx, sg, st));
+  if (d_res) {
+    // r0 - A V y = V_{0..mused} z: the Krylov vectors V_0 .. V_done of each
+    // system (the last one normalised by the Givens step) and z from the
+    // rotations
+    BIE_CUDA(ws.zc.alloc(size_t(2) * (M + 1) * nsys));
+    BIE_CUDA(dev::launch_gmres_resvec(int(M), nsys, mused + 1, d_cs, d_sn, d_sv, ws.done.p,
+                                      ws.zc.p, st));
+    BIE_CUDA(dev::launch_combo(V, ldv, mused + 1, ws.zc.p, d_res, n, nd, cplx, sg, st));
+  }
   std::vector<int> brk(nsys);
   BIE_CUDA(cudaMemcpyAsync(out.errs.data(), d_errs, nE * sizeof(double), cudaMemcpyDeviceToHost, st));
   BIE_CUDA(cudaMemcpyAsync(brk.data(), ws.brk.p, nsys * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -306,6 +316,7 @@ static int solve_mixed_impl(Operator& P, int nd, const cdouble* zid, const doubl
   DBuf<double>& partial = P.mws.partial;
   DBuf<double>& nrm = P.mws.nrm;
   DBuf<double>& kx = P.mws.kx;  // K x in FP64 (see MixedOut)
+  DBuf<double>& rn = P.mws.rn;  // an inner solve's own residual vector
   BIE_CUDA(r.alloc(ldv));
   BIE_CUDA(d.alloc(ldv));
   BIE_CUDA(kx.alloc(ldv));
@@ -448,7 +459,10 @@ static int solve_mixed_impl(Operator& P, int nd, const cdouble* zid, const doubl
       }
     }
     GmresOut go;
-    ier = gmres(P, 1, -1, nd, zid, r.p, nullptr, numit, tol, d.p, go, st, tol_sys.data());
+    const bool want_rn = increments && kx_valid;
+    if (want_rn) BIE_CUDA(rn.alloc(ldv));
+    ier = gmres(P, 1, -1, nd, zid, r.p, nullptr, numit, tol, d.p, go, st, tol_sys.data(),
+                want_rn ? rn.p : nullptr);
     if (ier && ier != kNotConverged) return ier;
     int64_t maxit = 0;
     for (int q = 0; q < nsys; ++q) {
@@ -486,10 +500,9 @@ static int solve_mixed_impl(Operator& P, int nd, const cdouble* zid, const doubl
     }
     if ((ier = P.set_active(seg_mask(), st))) return ier;
     if (incr) {
-      ier = P.apply(1, nd, d.p, r.p, st);  // r = K32 d
-      if (ier) return ier;
-      BIE_CUDA(dev::launch_axpby(r.p, kx.p, 1.0, 0.0, 1.0, 0.0, n, cplx, st));
-      ++out.fp32_matvecs;
+      // K32 d = A32 d - zid d = (r - rn) - zid d, with rn = r - A32 d the
+      // inner solve's residual vector from its Krylov basis: no matvec
+      BIE_CUDA(dev::launch_kx_update(kx.p, r.p, rn.p, d.p, d_zid, n, nd, cplx, sg, st));
       ++out.incr_matvecs;
       out.max_incr_ratio = std::max(out.max_incr_ratio, ratio_max);
     } else {

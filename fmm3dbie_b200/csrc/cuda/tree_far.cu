@@ -286,10 +286,10 @@ __global__ void __launch_bounds__(kEvThreads)
   __shared__ R2 sg1[kEvTile];
   __shared__ R4 sst[kEvTile];
   __shared__ R2 sphi[PROXYT ? 1 : tree::kMaxProxies];
-  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kFarTrigN : 1];
   const double2* tab = nullptr;
   if constexpr (sizeof(R) == 8 && KIND == 1) {
-    fill_trig_table(stab);  // published by the first __syncthreads below
+    fill_far_trig_table(stab);  // published by the first __syncthreads below
     tab = stab;
   }
   const int tid = threadIdx.x, m = blockIdx.y;
@@ -481,10 +481,10 @@ __global__ void __launch_bounds__(kEvThreads)
   __shared__ __align__(16) unsigned char sbuf[kSstBytes > kPhiBytes ? kSstBytes : kPhiBytes];
   R(*sst)[MD][C] = reinterpret_cast<R(*)[MD][C]>(sbuf);
   R2* sphi = reinterpret_cast<R2*>(sbuf);
-  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kTrigN : 1];
+  __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kFarTrigN : 1];
   const double2* tab = nullptr;
   if constexpr (sizeof(R) == 8 && KIND == 1) {
-    fill_trig_table(stab);  // published by the first __syncthreads below
+    fill_far_trig_table(stab);  // published by the first __syncthreads below
     tab = stab;
   }
   const int tid = threadIdx.x;

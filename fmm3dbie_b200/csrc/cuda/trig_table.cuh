@@ -41,5 +41,41 @@ __device__ __forceinline__ void sincos_tab(double x, const double2* tab, double&
   c = fma(t.x, cp, -(t.y * sp));
 }
 
+// The far-field variant of the same method, for the direct and hierarchical
+// far-field kernels, whose phases stay below 100 and whose products only need
+// ~1e-14: the same 256-entry table and series, with j found by the
+// round-to-integer of adding 1.5 * 2^52 (no conversion instructions) and the
+// reduction x - j (2 pi / N) in one fused multiply-add with 2 pi / N rounded
+// to FP64: its error, j times the rounding of the step (at most 1.7e-18), is
+// below 1e-14 for x < 100.
+constexpr int kFarTrigN = kTrigN;
+constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
+
+__device__ __forceinline__ void fill_far_trig_table(double2* tab) { fill_trig_table(tab); }
+
+__device__ __forceinline__ void sincos_far(double x, const double2* tab, double& s, double& c) {
+  const double u = fma(x, kTrigInvStep, kRoundMagic);  // 1.5 2^52 + rint(x / step)
+  const int j = __double2loint(u) & (kFarTrigN - 1);
+  const double jd = u - kRoundMagic;
+  const double rho = fma(-jd, kTrigStep, x);
+  const double r2 = rho * rho;
+  const double sp = fma(rho * r2, fma(r2, 1.0 / 120.0, -1.0 / 6.0), rho);
+  const double cp = fma(r2, fma(r2, fma(r2, -1.0 / 720.0, 1.0 / 24.0), -0.5), 1.0);
+  const double2 t = tab[j];
+  s = fma(t.y, cp, t.x * sp);
+  c = fma(t.x, cp, -(t.y * sp));
+}
+
+// 1/sqrt(a) in FP64 for a > 0 in the FP32 normal range: the FP32 hardware
+// approximation y0 (relative error e0 ~ 2^-22) refined by one third-order
+// step of the binomial series of (1 - e)^(-1/2), e = 1 - a y0^2:
+//   y = y0 (1 + e/2 + 3 e^2 / 8),
+// whose truncation error 5 e^3 / 16 ~ 1e-20 is below the FP64 rounding.
+__device__ __forceinline__ double rsqrt_far(double a) {
+  const double y0 = double(rsqrtf(float(a)));
+  const double e = fma(-(a * y0), y0, 1.0);
+  return fma(y0 * e, fma(e, 0.375, 0.5), y0);
+}
+
 }  // namespace dev
 }  // namespace bie

@@ -353,12 +353,13 @@ int bie_plan_timing(void* plan, int64_t enable, double* times);
  * wide: 1 (default; BIE_MIXED_RESIDUAL=increment) keeps K x in FP64 from the
  * first refinement step's FP64 matvec and adds the FP32 operator's K d for a
  * later correction d whose FP32 error cannot reach the target
- * (1e-6 ||d||_w / ||x||_w <= eps_gmres / 4 for every active system), else
- * applies the FP64 operator to x again; 0 (BIE_MIXED_RESIDUAL=full) applies
- * the FP64 operator to x after every inner solve.  bie_last_mixed_stats:
- * the calling thread's last mixed solve: out[0] FP64 matvecs, out[1] FP32
- * matvecs (increments included), out[2] increment matvecs, out[3] largest
- * ||d||_w / ||x||_w of an increment.  No reference counterpart. */
+ * (1e-6 ||d||_w / ||x||_w <= eps_gmres / 4 for every active system), taken
+ * from the inner GMRES's residual vector without a matvec, else applies the
+ * FP64 operator to x again; 0 (BIE_MIXED_RESIDUAL=full) applies the FP64
+ * operator to x after every inner solve.  bie_last_mixed_stats: the calling
+ * thread's last mixed solve: out[0] FP64 matvecs, out[1] FP32 matvecs,
+ * out[2] increment steps, out[3] largest ||d||_w / ||x||_w of an increment.
+ * No reference counterpart. */
 int bie_set_mixed_residual(int64_t mode);
 int bie_get_mixed_residual(void);
 int bie_last_mixed_stats(double* out);
