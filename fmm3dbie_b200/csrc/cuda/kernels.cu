@@ -670,11 +670,17 @@ struct Vec2<double> {
 
 constexpr int kCombineThreads = 256;  // 8 warps = 8 consecutive target rows per block
 constexpr int kCombineUnroll = 4;     // W_eff entries per lane in flight
+// Blocks per SM the one-density form is compiled for (48 registers): 5 % faster
+// on the 35,840-node matvec than 4 blocks (64 registers); 6 and 8 blocks, and
+// 8 entries per lane in flight, measured slower.
+constexpr int kCombineMinBlocks = 5;
 
 
 // Rows 8*bx .. 8*bx+7 (one warp each) of the near correction plus the far
 // partial sums.
-template <int CPLX, typename W>
+// SINGLE: the one-density form (nd == 1), compiled apart from the
+// several-density form so that each has its own register budget.
+template <int CPLX, typename W, bool SINGLE>
 __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
                                              const W* __restrict__ weff,
                                              const double* __restrict__ sigma,
@@ -683,7 +689,7 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
   const int lane = threadIdx.x & 31;
   const int64_t i = (int64_t(bx) * blockDim.x + threadIdx.x) >> 5;
   const int64_t ntarg = g.ntarg;
-  if (nd == 1) {
+  if constexpr (SINGLE) {
     __shared__ double sred[32][8][2];
     // the row's range and its first 32 near pairs are loaded before the
     // partial-sum phase and its barrier, so their latency overlaps it
@@ -751,37 +757,40 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
         const int ne = nkc * np0;
         const float inv = 1.0f / float(np0);
         for (int eb = 0; eb < ne; eb += 32 * kU) {
-          double wr[kU], wi[kU], sr[kU], si[kU];
+          W wr[kU], wi[kU];  // W_eff stays in its storage precision until the FMA
+          double sr[kU], si[kU];
 #pragma unroll
           for (int u = 0; u < kU; ++u) {
             const int e = eb + 32 * u + lane;
             const bool ok = e < ne;
             const int kk = ok ? int((float(e) + 0.5f) * inv) : 0;
             const int psk = __shfl_sync(kFull, ps, kk);
-            wr[u] = wi[u] = sr[u] = si[u] = 0.0;
+            wr[u] = wi[u] = W(0);
+            sr[u] = si[u] = 0.0;
             if (ok) {
               const int node = psk + (e - kk * np0);
               if (CPLX) {
                 const typename Vec2<W>::T wv =
                     reinterpret_cast<const typename Vec2<W>::T*>(weff)[e0 + e];
                 const double2 sv = reinterpret_cast<const double2*>(sigma)[node];
-                wr[u] = double(wv.x);
-                wi[u] = double(wv.y);
+                wr[u] = wv.x;
+                wi[u] = wv.y;
                 sr[u] = sv.x;
                 si[u] = sv.y;
               } else {
-                wr[u] = double(weff[e0 + e]);
+                wr[u] = weff[e0 + e];
                 sr[u] = sigma[node];
               }
             }
           }
 #pragma unroll
           for (int u = 0; u < kU; ++u) {
+            const double a = double(wr[u]), b = double(wi[u]);
             if (CPLX) {
-              ar = fma(wr[u], sr[u], fma(-wi[u], si[u], ar));
-              ai = fma(wr[u], si[u], fma(wi[u], sr[u], ai));
+              ar = fma(a, sr[u], fma(-b, si[u], ar));
+              ai = fma(a, si[u], fma(b, sr[u], ai));
             } else {
-              ar = fma(wr[u], sr[u], ar);
+              ar = fma(a, sr[u], ar);
             }
           }
         }
@@ -819,7 +828,7 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
       }
     }
     return;
-  }
+  } else {
   // several densities per point: lanes run over densities
   if (i >= ntarg) return;
   const int64_t k0 = nr.row_ptr[i], k1 = nr.row_ptr[i + 1];
@@ -858,14 +867,15 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
       pot[o] = ar;
     }
   }
+  }
 }
 
-template <int CPLX, typename W>
-__global__ void __launch_bounds__(kCombineThreads)
+template <int CPLX, typename W, bool SINGLE>
+__global__ void __launch_bounds__(kCombineThreads, SINGLE ? kCombineMinBlocks : 1)
     combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
                    const double* __restrict__ sigma, const double* __restrict__ partial,
                    int nchunks, double* __restrict__ pot, int nd) {
-  combine_rows<CPLX, W>(g, nr, weff, sigma, partial, nchunks, pot, nd, blockIdx.x);
+  combine_rows<CPLX, W, SINGLE>(g, nr, weff, sigma, partial, nchunks, pot, nd, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1575,7 +1585,7 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
-template <int CPLX, typename W>
+template <int CPLX, typename W, bool SINGLE>
 __global__ void __launch_bounds__(kCombineThreads)
     batch_combine_kernel(const BatchSurf* __restrict__ bs, const int2* __restrict__ items,
                          int nitems, const double* const* __restrict__ xref,
@@ -1599,7 +1609,7 @@ __global__ void __launch_bounds__(kCombineThreads)
     }
     const Geometry g = S.g;
     const Near nr = S.nr;
-    combine_rows<CPLX, W>(g, nr, static_cast<const W*>(S.weff[prec]), x + S.vofs * nd * C,
+    combine_rows<CPLX, W, SINGLE>(g, nr, static_cast<const W*>(S.weff[prec]), x + S.vofs * nd * C,
                           partial + S.pofs[prec], S.nchunks[prec], y + S.vofs * nd * C, nd, it.y);
     __syncthreads();
   }
@@ -1717,20 +1727,25 @@ cudaError_t launch_batch_matvec(const BatchArgs& a, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   e = batch_far_any(a, st, nullptr);
   if (e != cudaSuccess) return e;
+  auto combine = [&](auto kern) {
+    kern<<<a.grid_row, kCombineThreads, 0, st>>>(a.surfs, a.row_items, a.nrow_items, a.xref,
+                                                 a.yref, a.partial, a.nd, a.precision);
+  };
+  const bool one = a.nd == 1;
   if (cplx) {
     if (a.precision == 1)
-      batch_combine_kernel<1, float><<<a.grid_row, kCombineThreads, 0, st>>>(
-          a.surfs, a.row_items, a.nrow_items, a.xref, a.yref, a.partial, a.nd, a.precision);
+      one ? combine(batch_combine_kernel<1, float, true>)
+          : combine(batch_combine_kernel<1, float, false>);
     else
-      batch_combine_kernel<1, double><<<a.grid_row, kCombineThreads, 0, st>>>(
-          a.surfs, a.row_items, a.nrow_items, a.xref, a.yref, a.partial, a.nd, a.precision);
+      one ? combine(batch_combine_kernel<1, double, true>)
+          : combine(batch_combine_kernel<1, double, false>);
   } else {
     if (a.precision == 1)
-      batch_combine_kernel<0, float><<<a.grid_row, kCombineThreads, 0, st>>>(
-          a.surfs, a.row_items, a.nrow_items, a.xref, a.yref, a.partial, a.nd, a.precision);
+      one ? combine(batch_combine_kernel<0, float, true>)
+          : combine(batch_combine_kernel<0, float, false>);
     else
-      batch_combine_kernel<0, double><<<a.grid_row, kCombineThreads, 0, st>>>(
-          a.surfs, a.row_items, a.nrow_items, a.xref, a.yref, a.partial, a.nd, a.precision);
+      one ? combine(batch_combine_kernel<0, double, true>)
+          : combine(batch_combine_kernel<0, double, false>);
   }
   count(3);
   return cudaGetLastError();
@@ -1845,16 +1860,27 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
   const int threads = kCombineThreads;
   const int64_t blocks = (g.ntarg * 32 + threads - 1) / threads;
   const dim3 grid(static_cast<unsigned>(blocks)), block(threads);
+  const bool one = a.nd == 1;
   if (kp.kind == 1) {
-    if (a.weff_f32)
-      combine_kernel<1, float><<<grid, block, 0, st>>>(g, nr, (const float*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-    else
-      combine_kernel<1, double><<<grid, block, 0, st>>>(g, nr, (const double*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+    if (a.weff_f32) {
+      const float* w = static_cast<const float*>(a.weff);
+      if (one) combine_kernel<1, float, true><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+      else combine_kernel<1, float, false><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+    } else {
+      const double* w = static_cast<const double*>(a.weff);
+      if (one) combine_kernel<1, double, true><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+      else combine_kernel<1, double, false><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+    }
   } else {
-    if (a.weff_f32)
-      combine_kernel<0, float><<<grid, block, 0, st>>>(g, nr, (const float*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-    else
-      combine_kernel<0, double><<<grid, block, 0, st>>>(g, nr, (const double*)a.weff, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+    if (a.weff_f32) {
+      const float* w = static_cast<const float*>(a.weff);
+      if (one) combine_kernel<0, float, true><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+      else combine_kernel<0, float, false><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+    } else {
+      const double* w = static_cast<const double*>(a.weff);
+      if (one) combine_kernel<0, double, true><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+      else combine_kernel<0, double, false><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+    }
   }
   count();
   return cudaGetLastError();
