@@ -421,6 +421,15 @@ __global__ void __launch_bounds__(NT, (kFarMinBlocks<R, NT>)) far_kernel(Geometr
 // ---------------------------------------------------------------------------
 constexpr int kMdCentre = 512;
 
+// FP32 Helmholtz blocks of up to 8 densities stage each density as
+// (re, im, im, re) for the packed complex multiply-add (4 densities: 4 %
+// faster than the scalar form on the 35,840-node matvec); with 16 densities
+// that layout and its registers measured 20 % slower, so those stay scalar.
+template <int KIND, typename R, int MD>
+constexpr bool kMdPacked = sizeof(R) == 4 && KIND == 1 && MD <= 8;
+template <int KIND, typename R, int MD>
+constexpr int kMdSigWords = kMdPacked<KIND, R, MD> ? 4 : (KIND == 1 ? 2 : 1);
+
 
 // One block's work of the multi-density far field: target block bx, source
 // chunk by, density group bz (MD densities).  Shared tiles and the FP64 trig
@@ -478,17 +487,58 @@ __device__ __forceinline__ void far_md_block(const Geometry& g, const KParams& k
     for (int q = threadIdx.x; q < TILE * MD; q += NT) {
       const int qs = q / MD, mm = q - qs * MD;
       const bool ok = qs < ns && m0 + mm < nd;
+      if constexpr (kMdPacked<KIND, R, MD>) {
+        // (re, im, im, re): the density and its swapped copy for the packed
+        // complex multiply-add
+        const R xr = ok ? sig[(size_t(sb + qs) * nd + m0 + mm) * 2] : R(0);
+        const R xi = ok ? sig[(size_t(sb + qs) * nd + m0 + mm) * 2 + 1] : R(0);
+        reinterpret_cast<float4*>(ssig)[q] = make_float4(xr, xi, xi, xr);
+      } else {
 #pragma unroll
-      for (int c = 0; c < C; ++c)
-        ssig[q * C + c] = ok ? sig[(size_t(sb + qs) * nd + m0 + mm) * C + c] : R(0);
+        for (int c = 0; c < C; ++c)
+          ssig[q * C + c] = ok ? sig[(size_t(sb + qs) * nd + m0 + mm) * C + c] : R(0);
+      }
     }
     __syncthreads();
-    if constexpr (sizeof(R) == 4 && KIND == 0) {
+    if constexpr (kMdPacked<KIND, R, MD>) {
+      // FP32 Helmholtz, up to 8 densities per block: each density's complex
+      // multiply-add as two packed lanes (re, im): acc += (K_r, K_r) (x_r, x_i)
+      // after (-K_i, K_i) (x_i, x_r), each lane rounded as the scalar form in
+      // the scalar form's order.
+      float2 tr2[TPT][MD];
+#pragma unroll
+      for (int t = 0; t < TPT; ++t)
+#pragma unroll
+        for (int m = 0; m < MD; ++m) tr2[t][m] = make_float2(0.f, 0.f);
+#pragma unroll 2
+      for (int j = 0; j < TILE; ++j) {
+        const R4 a = sg0[j];
+        const R2 b = sg1[j];
+        const R4 sv4 = reinterpret_cast<const R4*>(sab)[j];
+        const float4* sv = reinterpret_cast<const float4*>(ssig) + j * MD;
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+          float kr_ = 0.f, ki_ = 0.f;
+          pair_helm(tx[t], ty[t], tz[t], a, b, sv4, k, kim, thr2, CK, kr_, ki_, tab);
+          const float2 kk = make_float2(kr_, kr_), kn = make_float2(-ki_, ki_);
+#pragma unroll
+          for (int m = 0; m < MD; ++m) {
+            const float4 x = sv[m];
+            tr2[t][m] = __ffma2_rn(kk, make_float2(x.x, x.y),
+                                   __ffma2_rn(kn, make_float2(x.z, x.w), tr2[t][m]));
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < TPT; ++t)
+#pragma unroll
+        for (int m = 0; m < MD; ++m) {
+          acc[t][m][0] += double(tr2[t][m].x);
+          acc[t][m][C - 1] += double(tr2[t][m].y);
+        }
+    } else if constexpr (sizeof(R) == 4 && KIND == 0) {
       // FP32 Laplace: two densities per packed multiply-add (fma.rn.f32x2,
-      // each lane rounded as the scalar form).  (The Helmholtz densities stay
-      // scalar: a packed complex multiply-add needs the density twice in
-      // shared memory, (re, im) and (im, re), and with MD = 16 that layout
-      // and its registers measured 20 % slower.)
+      // each lane rounded as the scalar form).
       constexpr int NP = MD / 2;
       float2 tr2[TPT][NP];
 #pragma unroll
@@ -589,7 +639,7 @@ __global__ void __launch_bounds__(NT) far_md_kernel(Geometry g, KParams kp,
   __shared__ typename Vec<R>::T4 sg0[TILE];
   __shared__ typename Vec<R>::T2 sg1[TILE];
   __shared__ __align__(16) R sab[TILE * 2 * C];
-  __shared__ __align__(16) R ssig[TILE * MD * C];
+  __shared__ __align__(16) R ssig[TILE * MD * kMdSigWords<KIND, R, MD>];
   __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kFarTrigN : 1];
   const double2* tab = nullptr;
   if constexpr (sizeof(R) == 8 && KIND == 1) {
@@ -678,9 +728,200 @@ constexpr int kCombineMinBlocks = 5;
 
 // Rows 8*bx .. 8*bx+7 (one warp each) of the near correction plus the far
 // partial sums.
-// SINGLE: the one-density form (nd == 1), compiled apart from the
-// several-density form so that each has its own register budget.
-template <int CPLX, typename W, bool SINGLE>
+// Near correction of row i for several densities.  A lane takes D = min(nd,
+// KD) consecutive densities of one W_eff entry (the sigma values of a node's
+// densities are contiguous); the warp's lanes are (entry slot, density
+// group) pairs -- Q = the number of groups rounded up to a power of two (at
+// most 32) groups side by side, G = 32 / Q entries of the row at a time --
+// and the slots are summed by shuffles at the end.  Near pairs are taken 32
+// at a time (one lane-parallel load of their first nodes and entry
+// offsets).  With KD = 4, where all 32 have the same node count, the row's
+// entries run as one flat range, two entries per lane in flight; with KD =
+// 1 (few entry slots, where the flat range's per-entry shuffles cost more
+// than they save) the pairs run one after the other.  KD = 4 serves nd <= 8
+// (nd = 4: 0.26 ms on the 35,840-node matvec, against 0.94 ms with the lanes
+// over densities alone), KD = 1 serves 8 < nd <= 32 (nd = 16: 0.63 against
+// 0.90 ms).
+template <int CPLX, typename W, int kD>
+__device__ __forceinline__ void combine_row_md(const Geometry& g, const Near& nr,
+                                               const W* __restrict__ weff,
+                                               const double* __restrict__ sigma,
+                                               const double* __restrict__ partial, int nchunks,
+                                               double* __restrict__ pot, int nd, int64_t i,
+                                               int lane) {
+  const int64_t ntarg = g.ntarg;
+  const int64_t k0 = nr.row_ptr[i], k1 = nr.row_ptr[i + 1];
+  constexpr unsigned kFull = 0xffffffffu;
+  const int D = nd < kD ? nd : kD;
+  const int ngroups = (nd + D - 1) / D;
+  int Q = 1;
+  while (Q < ngroups && Q < 32) Q <<= 1;
+  const int G = 32 / Q, ql = lane & (Q - 1), slot = lane / Q;
+  for (int qb = 0; qb < ngroups; qb += Q) {
+    const int m0 = (qb + ql) * D;
+    const int dn = m0 < nd ? (nd - m0 < D ? nd - m0 : D) : 0;  // densities of this lane
+    double ar[kD], ai[kD];
+#pragma unroll
+    for (int d = 0; d < kD; ++d) ar[d] = ai[d] = 0.0;
+    // far-field partial sums, chunks spread over the entry slots
+    if (dn > 0)
+      for (int c = slot; c < nchunks; c += G) {
+        const size_t o = (size_t(c) * ntarg + i) * nd + m0;
+#pragma unroll
+        for (int d = 0; d < kD; ++d)
+          if (d < dn) {
+            if (CPLX) {
+              const double2 v = reinterpret_cast<const double2*>(partial)[o + d];
+              ar[d] += v.x;
+              ai[d] += v.y;
+            } else {
+              ar[d] += partial[o + d];
+            }
+          }
+      }
+    // one entry: weight w times the lane's densities of node
+    auto entry = [&](int64_t we, int node) {
+      const size_t so = size_t(node) * nd + m0;
+      if (CPLX) {
+        const typename Vec2<W>::T wv = reinterpret_cast<const typename Vec2<W>::T*>(weff)[we];
+        const double wr = double(wv.x), wi = double(wv.y);
+#pragma unroll
+        for (int d = 0; d < kD; ++d)
+          if (d < dn) {
+            const double2 sv = reinterpret_cast<const double2*>(sigma)[so + d];
+            ar[d] = fma(wr, sv.x, fma(-wi, sv.y, ar[d]));
+            ai[d] = fma(wr, sv.y, fma(wi, sv.x, ai[d]));
+          }
+      } else {
+        const double w = double(weff[we]);
+#pragma unroll
+        for (int d = 0; d < kD; ++d)
+          if (d < dn) ar[d] = fma(w, sigma[so + d], ar[d]);
+      }
+    };
+    for (int64_t kc = k0; kc < k1; kc += 32) {
+      const int nkc = int(k1 - kc < 32 ? k1 - kc : 32);
+      int psl = 0, npl = 0;
+      int64_t wbl = 0;
+      if (lane < nkc) {
+        psl = nr.nps[kc + lane];
+        wbl = nr.wofs[kc + lane];
+        npl = int(nr.wofs[kc + lane + 1] - wbl);
+      }
+      const int np0 = __shfl_sync(kFull, npl, 0);
+      const int64_t e0 = __shfl_sync(kFull, wbl, 0);
+      if (kD > 1 && __all_sync(kFull, lane >= nkc || npl == np0)) {
+        // entry e of the group belongs to pair e / np0 (exact in FP32, as
+        // in the one-density form)
+        const int ne = nkc * np0;
+        const float inv = 1.0f / float(np0);
+        // (the same trip count on every lane: the shuffles need the whole warp)
+        constexpr int U = 8 / kD;  // entries per lane in flight
+        for (int eb = 0; eb < ne; eb += U * G) {
+          int node[U], ee[U];
+          bool ok[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int e = eb + u * G + slot;
+            ee[u] = e;
+            ok[u] = e < ne && dn > 0;
+            const int kk = e < ne ? int((float(e) + 0.5f) * inv) : 0;
+            const int psk = __shfl_sync(kFull, psl, kk);
+            node[u] = psk + (e - kk * np0);
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (ok[u]) entry(e0 + ee[u], node[u]);
+        }
+      } else {
+        for (int j = 0; j < nkc; ++j) {
+          const int ps = __shfl_sync(kFull, psl, j), np = __shfl_sync(kFull, npl, j);
+          const int64_t wb = __shfl_sync(kFull, wbl, j);
+          if (dn == 0) continue;
+#pragma unroll(kD == 1 ? 4 : 1)
+          for (int mm = slot; mm < np; mm += G) entry(wb + mm, ps + mm);
+        }
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < kD; ++d)
+      for (int off = Q; off < 32; off <<= 1) {
+        ar[d] += __shfl_xor_sync(kFull, ar[d], off);
+        if (CPLX) ai[d] += __shfl_xor_sync(kFull, ai[d], off);
+      }
+    if (slot == 0)
+#pragma unroll
+      for (int d = 0; d < kD; ++d)
+        if (d < dn) {
+          const size_t o = size_t(i) * nd + m0 + d;
+          if (CPLX) {
+            pot[2 * o] = ar[d];
+            pot[2 * o + 1] = ai[d];
+          } else {
+            pot[o] = ar[d];
+          }
+        }
+  }
+}
+
+// More than 32 densities: the lanes run over densities, every lane over the
+// whole row (1.42 ms at nd = 64 on the 35,840-node matvec, where the slot
+// forms measured 1.6-2.3 ms).
+template <int CPLX, typename W>
+__device__ __forceinline__ void combine_row_wide(const Geometry& g, const Near& nr,
+                                                 const W* __restrict__ weff,
+                                                 const double* __restrict__ sigma,
+                                                 const double* __restrict__ partial,
+                                                 int nchunks, double* __restrict__ pot, int nd,
+                                                 int64_t i, int lane) {
+  const int64_t ntarg = g.ntarg;
+  const int64_t k0 = nr.row_ptr[i], k1 = nr.row_ptr[i + 1];
+  for (int m = lane; m < nd; m += 32) {
+    double ar = 0, ai = 0;
+    for (int c = 0; c < nchunks; ++c) {
+      const size_t o = (size_t(c) * ntarg + i) * nd + m;
+      if (CPLX) {
+        ar += partial[2 * o];
+        ai += partial[2 * o + 1];
+      } else {
+        ar += partial[o];
+      }
+    }
+    for (int64_t k = k0; k < k1; ++k) {
+      const int ps = nr.nps[k];
+      const int64_t wb = nr.wofs[k];
+      const int np = int(nr.wofs[k + 1] - wb);
+      for (int mm = 0; mm < np; ++mm) {
+        const size_t so = size_t(ps + mm) * nd + m;
+        if (CPLX) {
+          const double wr = double(weff[2 * (wb + mm)]), wi = double(weff[2 * (wb + mm) + 1]);
+          const double sr = sigma[2 * so], si = sigma[2 * so + 1];
+          ar = fma(wr, sr, fma(-wi, si, ar));
+          ai = fma(wr, si, fma(wi, sr, ai));
+        } else {
+          ar = fma(double(weff[wb + mm]), sigma[so], ar);
+        }
+      }
+    }
+    const size_t o = size_t(i) * nd + m;
+    if (CPLX) {
+      pot[2 * o] = ar;
+      pot[2 * o + 1] = ai;
+    } else {
+      pot[o] = ar;
+    }
+  }
+}
+
+// MODE: the form of the row's work, by density count -- kCombineOne (nd ==
+// 1), kCombineMd4 (nd <= 8), kCombineMd1 (nd <= 32), kCombineWide -- each
+// compiled as its own kernel so that each has its own register budget.
+constexpr int kCombineOne = 0, kCombineMd4 = 1, kCombineMd1 = 2, kCombineWide = 3;
+inline int combine_mode(int nd) {
+  return nd == 1 ? kCombineOne : nd <= 8 ? kCombineMd4 : nd <= 32 ? kCombineMd1 : kCombineWide;
+}
+
+template <int CPLX, typename W, int MODE>
 __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
                                              const W* __restrict__ weff,
                                              const double* __restrict__ sigma,
@@ -689,7 +930,7 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
   const int lane = threadIdx.x & 31;
   const int64_t i = (int64_t(bx) * blockDim.x + threadIdx.x) >> 5;
   const int64_t ntarg = g.ntarg;
-  if constexpr (SINGLE) {
+  if constexpr (MODE == kCombineOne) {
     __shared__ double sred[32][8][2];
     // the row's range and its first 32 near pairs are loaded before the
     // partial-sum phase and its barrier, so their latency overlaps it
@@ -829,53 +1070,22 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
     }
     return;
   } else {
-  // several densities per point: lanes run over densities
-  if (i >= ntarg) return;
-  const int64_t k0 = nr.row_ptr[i], k1 = nr.row_ptr[i + 1];
-  for (int m = lane; m < nd; m += 32) {
-    double ar = 0, ai = 0;
-    for (int c = 0; c < nchunks; ++c) {
-      const size_t o = (size_t(c) * ntarg + i) * nd + m;
-      if (CPLX) {
-        ar += partial[2 * o];
-        ai += partial[2 * o + 1];
-      } else {
-        ar += partial[o];
-      }
-    }
-    for (int64_t k = k0; k < k1; ++k) {
-      const int p = nr.col[k];
-      const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
-      const int64_t wb = nr.wofs[k];
-      for (int mm = 0; mm < np; ++mm) {
-        const size_t so = size_t(ps + mm) * nd + m;
-        if (CPLX) {
-          const double wr = double(weff[2 * (wb + mm)]), wi = double(weff[2 * (wb + mm) + 1]);
-          const double sr = sigma[2 * so], si = sigma[2 * so + 1];
-          ar = fma(wr, sr, fma(-wi, si, ar));
-          ai = fma(wr, si, fma(wi, sr, ai));
-        } else {
-          ar = fma(double(weff[wb + mm]), sigma[so], ar);
-        }
-      }
-    }
-    const size_t o = size_t(i) * nd + m;
-    if (CPLX) {
-      pot[2 * o] = ar;
-      pot[2 * o + 1] = ai;
-    } else {
-      pot[o] = ar;
-    }
-  }
+    if (i >= ntarg) return;
+    if constexpr (MODE == kCombineMd4)
+      combine_row_md<CPLX, W, 4>(g, nr, weff, sigma, partial, nchunks, pot, nd, i, lane);
+    else if constexpr (MODE == kCombineMd1)
+      combine_row_md<CPLX, W, 1>(g, nr, weff, sigma, partial, nchunks, pot, nd, i, lane);
+    else
+      combine_row_wide<CPLX, W>(g, nr, weff, sigma, partial, nchunks, pot, nd, i, lane);
   }
 }
 
-template <int CPLX, typename W, bool SINGLE>
-__global__ void __launch_bounds__(kCombineThreads, SINGLE ? kCombineMinBlocks : 1)
+template <int CPLX, typename W, int MODE>
+__global__ void __launch_bounds__(kCombineThreads, MODE == kCombineOne ? kCombineMinBlocks : 1)
     combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
                    const double* __restrict__ sigma, const double* __restrict__ partial,
                    int nchunks, double* __restrict__ pot, int nd) {
-  combine_rows<CPLX, W, SINGLE>(g, nr, weff, sigma, partial, nchunks, pot, nd, blockIdx.x);
+  combine_rows<CPLX, W, MODE>(g, nr, weff, sigma, partial, nchunks, pot, nd, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1561,7 +1771,7 @@ __global__ void __launch_bounds__(NT)
   __shared__ typename Vec<R>::T4 sg0[TILE];
   __shared__ typename Vec<R>::T2 sg1[TILE];
   __shared__ __align__(16) R sab[TILE * 2 * C];
-  __shared__ __align__(16) R ssig[TILE * MD * C];
+  __shared__ __align__(16) R ssig[TILE * MD * kMdSigWords<KIND, R, MD>];
   __shared__ double2 stab[sizeof(R) == 8 && KIND == 1 ? kFarTrigN : 1];
   const double2* tab = nullptr;
   if constexpr (sizeof(R) == 8 && KIND == 1) {
@@ -1585,7 +1795,7 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
-template <int CPLX, typename W, bool SINGLE>
+template <int CPLX, typename W, int MODE>
 __global__ void __launch_bounds__(kCombineThreads)
     batch_combine_kernel(const BatchSurf* __restrict__ bs, const int2* __restrict__ items,
                          int nitems, const double* const* __restrict__ xref,
@@ -1609,7 +1819,7 @@ __global__ void __launch_bounds__(kCombineThreads)
     }
     const Geometry g = S.g;
     const Near nr = S.nr;
-    combine_rows<CPLX, W, SINGLE>(g, nr, static_cast<const W*>(S.weff[prec]), x + S.vofs * nd * C,
+    combine_rows<CPLX, W, MODE>(g, nr, static_cast<const W*>(S.weff[prec]), x + S.vofs * nd * C,
                           partial + S.pofs[prec], S.nchunks[prec], y + S.vofs * nd * C, nd, it.y);
     __syncthreads();
   }
@@ -1731,21 +1941,28 @@ cudaError_t launch_batch_matvec(const BatchArgs& a, cudaStream_t st) {
     kern<<<a.grid_row, kCombineThreads, 0, st>>>(a.surfs, a.row_items, a.nrow_items, a.xref,
                                                  a.yref, a.partial, a.nd, a.precision);
   };
-  const bool one = a.nd == 1;
+  auto by_mode = [&](auto one, auto md4, auto md1, auto wide) {
+    switch (combine_mode(a.nd)) {
+      case kCombineOne: combine(one); break;
+      case kCombineMd4: combine(md4); break;
+      case kCombineMd1: combine(md1); break;
+      default: combine(wide); break;
+    }
+  };
   if (cplx) {
     if (a.precision == 1)
-      one ? combine(batch_combine_kernel<1, float, true>)
-          : combine(batch_combine_kernel<1, float, false>);
+      by_mode(batch_combine_kernel<1, float, 0>, batch_combine_kernel<1, float, 1>,
+              batch_combine_kernel<1, float, 2>, batch_combine_kernel<1, float, 3>);
     else
-      one ? combine(batch_combine_kernel<1, double, true>)
-          : combine(batch_combine_kernel<1, double, false>);
+      by_mode(batch_combine_kernel<1, double, 0>, batch_combine_kernel<1, double, 1>,
+              batch_combine_kernel<1, double, 2>, batch_combine_kernel<1, double, 3>);
   } else {
     if (a.precision == 1)
-      one ? combine(batch_combine_kernel<0, float, true>)
-          : combine(batch_combine_kernel<0, float, false>);
+      by_mode(batch_combine_kernel<0, float, 0>, batch_combine_kernel<0, float, 1>,
+              batch_combine_kernel<0, float, 2>, batch_combine_kernel<0, float, 3>);
     else
-      one ? combine(batch_combine_kernel<0, double, true>)
-          : combine(batch_combine_kernel<0, double, false>);
+      by_mode(batch_combine_kernel<0, double, 0>, batch_combine_kernel<0, double, 1>,
+              batch_combine_kernel<0, double, 2>, batch_combine_kernel<0, double, 3>);
   }
   count(3);
   return cudaGetLastError();
@@ -1860,27 +2077,33 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
   const int threads = kCombineThreads;
   const int64_t blocks = (g.ntarg * 32 + threads - 1) / threads;
   const dim3 grid(static_cast<unsigned>(blocks)), block(threads);
-  const bool one = a.nd == 1;
+  auto go = [&](auto kern, const auto* w) {
+    kern<<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
+  };
+  auto by_mode = [&](auto one, auto md4, auto md1, auto wide, const auto* w) {
+    switch (combine_mode(a.nd)) {
+      case kCombineOne: go(one, w); break;
+      case kCombineMd4: go(md4, w); break;
+      case kCombineMd1: go(md1, w); break;
+      default: go(wide, w); break;
+    }
+  };
+  const float* wf = static_cast<const float*>(a.weff);
+  const double* wd = static_cast<const double*>(a.weff);
   if (kp.kind == 1) {
-    if (a.weff_f32) {
-      const float* w = static_cast<const float*>(a.weff);
-      if (one) combine_kernel<1, float, true><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-      else combine_kernel<1, float, false><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-    } else {
-      const double* w = static_cast<const double*>(a.weff);
-      if (one) combine_kernel<1, double, true><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-      else combine_kernel<1, double, false><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-    }
+    if (a.weff_f32)
+      by_mode(combine_kernel<1, float, 0>, combine_kernel<1, float, 1>,
+              combine_kernel<1, float, 2>, combine_kernel<1, float, 3>, wf);
+    else
+      by_mode(combine_kernel<1, double, 0>, combine_kernel<1, double, 1>,
+              combine_kernel<1, double, 2>, combine_kernel<1, double, 3>, wd);
   } else {
-    if (a.weff_f32) {
-      const float* w = static_cast<const float*>(a.weff);
-      if (one) combine_kernel<0, float, true><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-      else combine_kernel<0, float, false><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-    } else {
-      const double* w = static_cast<const double*>(a.weff);
-      if (one) combine_kernel<0, double, true><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-      else combine_kernel<0, double, false><<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
-    }
+    if (a.weff_f32)
+      by_mode(combine_kernel<0, float, 0>, combine_kernel<0, float, 1>,
+              combine_kernel<0, float, 2>, combine_kernel<0, float, 3>, wf);
+    else
+      by_mode(combine_kernel<0, double, 0>, combine_kernel<0, double, 1>,
+              combine_kernel<0, double, 2>, combine_kernel<0, double, 3>, wd);
   }
   count();
   return cudaGetLastError();
