@@ -739,9 +739,9 @@ constexpr int kCombineMinBlocks = 5;
 // entries run as one flat range, two entries per lane in flight; with KD =
 // 1 (few entry slots, where the flat range's per-entry shuffles cost more
 // than they save) the pairs run one after the other.  KD = 4 serves nd <= 8
-// (nd = 4: 0.26 ms on the 35,840-node matvec, against 0.94 ms with the lanes
-// over densities alone), KD = 1 serves 8 < nd <= 32 (nd = 16: 0.63 against
-// 0.90 ms).
+// (nd = 4: 0.26 ms on the 35,840-node matvec, against 0.64 ms with the lanes
+// over densities alone), KD = 1 serves 8 < nd <= 32 (nd = 16: 0.72 against
+// 0.63-0.90 ms in runs of the lanes-over-densities form).
 template <int CPLX, typename W, int kD>
 __device__ __forceinline__ void combine_row_md(const Geometry& g, const Near& nr,
                                                const W* __restrict__ weff,
