@@ -728,20 +728,18 @@ constexpr int kCombineMinBlocks = 5;
 
 // Rows 8*bx .. 8*bx+7 (one warp each) of the near correction plus the far
 // partial sums.
-// Near correction of row i for several densities.  A lane takes D = min(nd,
+// Near correction of row i for 2..8 densities.  A lane takes D = min(nd,
 // KD) consecutive densities of one W_eff entry (the sigma values of a node's
 // densities are contiguous); the warp's lanes are (entry slot, density
-// group) pairs -- Q = the number of groups rounded up to a power of two (at
-// most 32) groups side by side, G = 32 / Q entries of the row at a time --
-// and the slots are summed by shuffles at the end.  Near pairs are taken 32
-// at a time (one lane-parallel load of their first nodes and entry
-// offsets).  With KD = 4, where all 32 have the same node count, the row's
-// entries run as one flat range, two entries per lane in flight; with KD =
-// 1 (few entry slots, where the flat range's per-entry shuffles cost more
-// than they save) the pairs run one after the other.  KD = 4 serves nd <= 8
-// (nd = 4: 0.26 ms on the 35,840-node matvec, against 0.64 ms with the lanes
-// over densities alone), KD = 1 serves 8 < nd <= 32 (nd = 16: 0.72 against
-// 0.63-0.90 ms in runs of the lanes-over-densities form).
+// group) pairs -- Q = the number of groups rounded up to a power of two
+// groups side by side, G = 32 / Q entries of the row at a time -- and the
+// slots are summed by shuffles at the end.  Near pairs are taken 32 at a
+// time (one lane-parallel load of their first nodes and entry offsets);
+// where all 32 have the same node count the row's entries run as one flat
+// range, two entries per lane in flight.  nd = 4: 0.20 ms on the 35,840-node
+// matvec against 0.63 ms with the lanes over densities (the wide form); at
+// nd = 16 the same scheme with one density per lane measured 0.72 against
+// 0.62 ms, so the wide form serves more than 8 densities.
 template <int CPLX, typename W, int kD>
 __device__ __forceinline__ void combine_row_md(const Geometry& g, const Near& nr,
                                                const W* __restrict__ weff,
@@ -810,13 +808,13 @@ __device__ __forceinline__ void combine_row_md(const Geometry& g, const Near& nr
       }
       const int np0 = __shfl_sync(kFull, npl, 0);
       const int64_t e0 = __shfl_sync(kFull, wbl, 0);
-      if (kD > 1 && __all_sync(kFull, lane >= nkc || npl == np0)) {
+      if (__all_sync(kFull, lane >= nkc || npl == np0)) {
         // entry e of the group belongs to pair e / np0 (exact in FP32, as
         // in the one-density form)
         const int ne = nkc * np0;
         const float inv = 1.0f / float(np0);
         // (the same trip count on every lane: the shuffles need the whole warp)
-        constexpr int U = 8 / kD;  // entries per lane in flight
+        constexpr int U = 2;  // entries per lane in flight
         for (int eb = 0; eb < ne; eb += U * G) {
           int node[U], ee[U];
           bool ok[U];
@@ -838,7 +836,6 @@ __device__ __forceinline__ void combine_row_md(const Geometry& g, const Near& nr
           const int ps = __shfl_sync(kFull, psl, j), np = __shfl_sync(kFull, npl, j);
           const int64_t wb = __shfl_sync(kFull, wbl, j);
           if (dn == 0) continue;
-#pragma unroll(kD == 1 ? 4 : 1)
           for (int mm = slot; mm < np; mm += G) entry(wb + mm, ps + mm);
         }
       }
@@ -864,8 +861,8 @@ __device__ __forceinline__ void combine_row_md(const Geometry& g, const Near& nr
   }
 }
 
-// More than 32 densities: the lanes run over densities, every lane over the
-// whole row (1.42 ms at nd = 64 on the 35,840-node matvec, where the slot
+// More than 8 densities: the lanes run over densities, every lane over the
+// whole row (1.43 ms at nd = 64 on the 35,840-node matvec, where the slot
 // forms measured 1.6-2.3 ms).
 template <int CPLX, typename W>
 __device__ __forceinline__ void combine_row_wide(const Geometry& g, const Near& nr,
@@ -888,9 +885,9 @@ __device__ __forceinline__ void combine_row_wide(const Geometry& g, const Near& 
       }
     }
     for (int64_t k = k0; k < k1; ++k) {
-      const int ps = nr.nps[k];
+      const int p = nr.col[k];
+      const int ps = g.pstart[p], np = g.pstart[p + 1] - ps;
       const int64_t wb = nr.wofs[k];
-      const int np = int(nr.wofs[k + 1] - wb);
       for (int mm = 0; mm < np; ++mm) {
         const size_t so = size_t(ps + mm) * nd + m;
         if (CPLX) {
@@ -914,11 +911,11 @@ __device__ __forceinline__ void combine_row_wide(const Geometry& g, const Near& 
 }
 
 // MODE: the form of the row's work, by density count -- kCombineOne (nd ==
-// 1), kCombineMd4 (nd <= 8), kCombineMd1 (nd <= 32), kCombineWide -- each
-// compiled as its own kernel so that each has its own register budget.
-constexpr int kCombineOne = 0, kCombineMd4 = 1, kCombineMd1 = 2, kCombineWide = 3;
+// 1), kCombineMd4 (nd <= 8), kCombineWide (more) -- each compiled as its own
+// kernel so that each has its own register budget.
+constexpr int kCombineOne = 0, kCombineMd4 = 1, kCombineWide = 2;
 inline int combine_mode(int nd) {
-  return nd == 1 ? kCombineOne : nd <= 8 ? kCombineMd4 : nd <= 32 ? kCombineMd1 : kCombineWide;
+  return nd == 1 ? kCombineOne : nd <= 8 ? kCombineMd4 : kCombineWide;
 }
 
 template <int CPLX, typename W, int MODE>
@@ -1073,15 +1070,21 @@ __device__ __forceinline__ void combine_rows(const Geometry& g, const Near& nr,
     if (i >= ntarg) return;
     if constexpr (MODE == kCombineMd4)
       combine_row_md<CPLX, W, 4>(g, nr, weff, sigma, partial, nchunks, pot, nd, i, lane);
-    else if constexpr (MODE == kCombineMd1)
-      combine_row_md<CPLX, W, 1>(g, nr, weff, sigma, partial, nchunks, pot, nd, i, lane);
     else
       combine_row_wide<CPLX, W>(g, nr, weff, sigma, partial, nchunks, pot, nd, i, lane);
   }
 }
 
+// Blocks per SM each form is compiled for.  The several-density forms at 4
+// (64 registers, no spills): unconstrained they took 96 (wide) and 127
+// registers and 2 blocks per SM, and measured 0.89 against 0.62 ms at
+// nd = 16, 1.73 against 1.42 ms at nd = 64, 0.25 against 0.20 ms at nd = 4
+// on the 35,840-node matvec.
+template <int MODE>
+constexpr int kCombineBlocks = MODE == kCombineOne ? kCombineMinBlocks : 4;
+
 template <int CPLX, typename W, int MODE>
-__global__ void __launch_bounds__(kCombineThreads, MODE == kCombineOne ? kCombineMinBlocks : 1)
+__global__ void __launch_bounds__(kCombineThreads, kCombineBlocks<MODE>)
     combine_kernel(Geometry g, Near nr, const W* __restrict__ weff,
                    const double* __restrict__ sigma, const double* __restrict__ partial,
                    int nchunks, double* __restrict__ pot, int nd) {
@@ -1796,7 +1799,7 @@ __global__ void __launch_bounds__(NT)
 }
 
 template <int CPLX, typename W, int MODE>
-__global__ void __launch_bounds__(kCombineThreads)
+__global__ void __launch_bounds__(kCombineThreads, kCombineBlocks<MODE>)
     batch_combine_kernel(const BatchSurf* __restrict__ bs, const int2* __restrict__ items,
                          int nitems, const double* const* __restrict__ xref,
                          double* const* __restrict__ yref, const double* __restrict__ partial,
@@ -1941,28 +1944,27 @@ cudaError_t launch_batch_matvec(const BatchArgs& a, cudaStream_t st) {
     kern<<<a.grid_row, kCombineThreads, 0, st>>>(a.surfs, a.row_items, a.nrow_items, a.xref,
                                                  a.yref, a.partial, a.nd, a.precision);
   };
-  auto by_mode = [&](auto one, auto md4, auto md1, auto wide) {
+  auto by_mode = [&](auto one, auto md4, auto wide) {
     switch (combine_mode(a.nd)) {
       case kCombineOne: combine(one); break;
       case kCombineMd4: combine(md4); break;
-      case kCombineMd1: combine(md1); break;
       default: combine(wide); break;
     }
   };
   if (cplx) {
     if (a.precision == 1)
       by_mode(batch_combine_kernel<1, float, 0>, batch_combine_kernel<1, float, 1>,
-              batch_combine_kernel<1, float, 2>, batch_combine_kernel<1, float, 3>);
+              batch_combine_kernel<1, float, 2>);
     else
       by_mode(batch_combine_kernel<1, double, 0>, batch_combine_kernel<1, double, 1>,
-              batch_combine_kernel<1, double, 2>, batch_combine_kernel<1, double, 3>);
+              batch_combine_kernel<1, double, 2>);
   } else {
     if (a.precision == 1)
       by_mode(batch_combine_kernel<0, float, 0>, batch_combine_kernel<0, float, 1>,
-              batch_combine_kernel<0, float, 2>, batch_combine_kernel<0, float, 3>);
+              batch_combine_kernel<0, float, 2>);
     else
       by_mode(batch_combine_kernel<0, double, 0>, batch_combine_kernel<0, double, 1>,
-              batch_combine_kernel<0, double, 2>, batch_combine_kernel<0, double, 3>);
+              batch_combine_kernel<0, double, 2>);
   }
   count(3);
   return cudaGetLastError();
@@ -2080,11 +2082,10 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
   auto go = [&](auto kern, const auto* w) {
     kern<<<grid, block, 0, st>>>(g, nr, w, a.sigma, a.partial, a.nchunks, a.pot, a.nd);
   };
-  auto by_mode = [&](auto one, auto md4, auto md1, auto wide, const auto* w) {
+  auto by_mode = [&](auto one, auto md4, auto wide, const auto* w) {
     switch (combine_mode(a.nd)) {
       case kCombineOne: go(one, w); break;
       case kCombineMd4: go(md4, w); break;
-      case kCombineMd1: go(md1, w); break;
       default: go(wide, w); break;
     }
   };
@@ -2093,17 +2094,17 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
   if (kp.kind == 1) {
     if (a.weff_f32)
       by_mode(combine_kernel<1, float, 0>, combine_kernel<1, float, 1>,
-              combine_kernel<1, float, 2>, combine_kernel<1, float, 3>, wf);
+              combine_kernel<1, float, 2>, wf);
     else
       by_mode(combine_kernel<1, double, 0>, combine_kernel<1, double, 1>,
-              combine_kernel<1, double, 2>, combine_kernel<1, double, 3>, wd);
+              combine_kernel<1, double, 2>, wd);
   } else {
     if (a.weff_f32)
       by_mode(combine_kernel<0, float, 0>, combine_kernel<0, float, 1>,
-              combine_kernel<0, float, 2>, combine_kernel<0, float, 3>, wf);
+              combine_kernel<0, float, 2>, wf);
     else
       by_mode(combine_kernel<0, double, 0>, combine_kernel<0, double, 1>,
-              combine_kernel<0, double, 2>, combine_kernel<0, double, 3>, wd);
+              combine_kernel<0, double, 2>, wd);
   }
   count();
   return cudaGetLastError();
