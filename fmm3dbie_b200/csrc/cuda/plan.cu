@@ -118,16 +118,22 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
     set_last_error("iquad(1) must be 1");
     return kErrArg;
   }
+  if (nquad < 0 || (nnz > 0 && s.iquad[nnz] - 1 != nquad)) {
+    set_last_error("nquad != iquad(nnz+1)-1");
+    return kErrArg;
+  }
+  // The near quadrature (the largest input: nquad entries) goes to the device
+  // first, so that its copy runs while the host checks the near list and
+  // builds the other arrays; the fold below follows it on the stream.
+  const size_t wlen = size_t(nquad) * (cplx ? 2 : 1);
+  BIE_CUDA(weff64_.alloc(std::max<size_t>(wlen, 1)));
+  if (wlen) BIE_CUDA(cudaMemcpyAsync(weff64_.p, s.wnear, wlen * sizeof(double), cudaMemcpyHostToDevice, st));
   for (int64_t k = 0; k < nnz; ++k) {
     const int64_t c = s.col_ind[k];
     if (c < 1 || c > npatches || s.iquad[k + 1] - s.iquad[k] != s.ixyzs[c] - s.ixyzs[c - 1]) {
       set_last_error("col_ind/iquad entry " + std::to_string(k + 1) + " invalid");
       return kErrArg;
     }
-  }
-  if (nnz > 0 && s.iquad[nnz] - 1 != nquad) {
-    set_last_error("nquad != iquad(nnz+1)-1");
-    return kErrArg;
   }
   // ---- host-side arrays ------------------------------------------------------
   std::vector<double> htx(ntarg), hty(ntarg), htz(ntarg);
@@ -289,9 +295,6 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   nr.nps = nps_.p;
   nr.wofs = wofs_.p;
   // ---- fold the smooth near part into W_eff (in place over wnear) -----------
-  const size_t wlen = size_t(nquad) * (cplx ? 2 : 1);
-  BIE_CUDA(weff64_.alloc(std::max<size_t>(wlen, 1)));
-  if (wlen) BIE_CUDA(cudaMemcpyAsync(weff64_.p, s.wnear, wlen * sizeof(double), cudaMemcpyHostToDevice, st));
   if (s.keep_f32) {
     // FP32 path: subtract the smooth part as the FP32 far kernel computes it
     BIE_CUDA(weff32_.alloc(std::max<size_t>(wlen, 1)));
