@@ -569,13 +569,25 @@ __device__ __forceinline__ void far_md_block(const Geometry& g, const KParams& k
           acc[t][2 * m + 1][0] += double(tr2[t][m].y);
         }
     } else {
-      R tr[TPT][MD][C];
+      // FP32: tile sums in FP32, added to the FP64 sums after each tile;
+      // FP64: straight into the FP64 sums (a second set of FP64 tile sums
+      // would only cost registers)
+      constexpr bool kTileSums = sizeof(R) == 4;
+      R tr[kTileSums ? TPT : 1][kTileSums ? MD : 1][C];
+      auto T = [&](int t, int m, int c) -> R& {
+        if constexpr (kTileSums)
+          return tr[t][m][c];
+        else
+          return reinterpret_cast<R&>(acc[t][m][c]);
+      };
+      if constexpr (kTileSums) {
 #pragma unroll
-      for (int t = 0; t < TPT; ++t)
+        for (int t = 0; t < TPT; ++t)
 #pragma unroll
-        for (int m = 0; m < MD; ++m)
+          for (int m = 0; m < MD; ++m)
 #pragma unroll
-          for (int c = 0; c < C; ++c) tr[t][m][c] = R(0);
+            for (int c = 0; c < C; ++c) tr[t][m][c] = R(0);
+      }
 #pragma unroll 2
       for (int j = 0; j < TILE; ++j) {
         const R4 a = sg0[j];
@@ -590,10 +602,10 @@ __device__ __forceinline__ void far_md_block(const Geometry& g, const KParams& k
 #pragma unroll
             for (int m2 = 0; m2 < MD / 2; ++m2) {
               const R4 x = sv[m2];  // densities 2*m2 and 2*m2+1
-              tr[t][2 * m2][0] = fma(kr_, x.x, fma(-ki_, x.y, tr[t][2 * m2][0]));
-              tr[t][2 * m2][1] = fma(kr_, x.y, fma(ki_, x.x, tr[t][2 * m2][1]));
-              tr[t][2 * m2 + 1][0] = fma(kr_, x.z, fma(-ki_, x.w, tr[t][2 * m2 + 1][0]));
-              tr[t][2 * m2 + 1][1] = fma(kr_, x.w, fma(ki_, x.z, tr[t][2 * m2 + 1][1]));
+              T(t, 2 * m2, 0) = fma(kr_, x.x, fma(-ki_, x.y, T(t, 2 * m2, 0)));
+              T(t, 2 * m2, 1) = fma(kr_, x.y, fma(ki_, x.x, T(t, 2 * m2, 1)));
+              T(t, 2 * m2 + 1, 0) = fma(kr_, x.z, fma(-ki_, x.w, T(t, 2 * m2 + 1, 0)));
+              T(t, 2 * m2 + 1, 1) = fma(kr_, x.w, fma(ki_, x.z, T(t, 2 * m2 + 1, 1)));
             }
           }
         } else {
@@ -604,16 +616,18 @@ __device__ __forceinline__ void far_md_block(const Geometry& g, const KParams& k
             pair_lap<R>(tx[t], ty[t], tz[t], a, b, s, thr2, kv);
             const R* sv = ssig + j * MD;
 #pragma unroll
-            for (int m = 0; m < MD; ++m) tr[t][m][0] = fma(kv, sv[m], tr[t][m][0]);
+            for (int m = 0; m < MD; ++m) T(t, m, 0) = fma(kv, sv[m], T(t, m, 0));
           }
         }
       }
+      if constexpr (kTileSums) {
 #pragma unroll
-      for (int t = 0; t < TPT; ++t)
+        for (int t = 0; t < TPT; ++t)
 #pragma unroll
-        for (int m = 0; m < MD; ++m)
+          for (int m = 0; m < MD; ++m)
 #pragma unroll
-          for (int c = 0; c < C; ++c) acc[t][m][c] += double(tr[t][m][c]);
+            for (int c = 0; c < C; ++c) acc[t][m][c] += double(tr[t][m][c]);
+      }
     }
   }
 #pragma unroll
