@@ -563,9 +563,20 @@ __global__ void __launch_bounds__(kEvThreads)
         }
         __syncthreads();
         if (!wact) continue;  // a warp without targets only helps load the tiles
-        R tr[MD], ti[MD];
+        // FP32: tile sums in FP32, added to the FP64 sums after the tile;
+        // FP64: straight into the FP64 sums
+        constexpr bool kTileSums = sizeof(R) == 4;
+        R trs[kTileSums ? MD : 1], tis[kTileSums ? MD : 1];
+        auto tr = [&](int mm) -> R& {
+          if constexpr (kTileSums) return trs[mm]; else return reinterpret_cast<R&>(accr[mm]);
+        };
+        auto ti = [&](int mm) -> R& {
+          if constexpr (kTileSums) return tis[mm]; else return reinterpret_cast<R&>(acci[mm]);
+        };
+        if constexpr (kTileSums) {
 #pragma unroll
-        for (int mm = 0; mm < MD; ++mm) tr[mm] = ti[mm] = R(0);
+          for (int mm = 0; mm < MD; ++mm) trs[mm] = tis[mm] = R(0);
+        }
         if (en.kind == 2) {
           for (int j = 0; j < ns; ++j) {
             R gr = R(0), gi = R(0);
@@ -575,10 +586,10 @@ __global__ void __launch_bounds__(kEvThreads)
               const R qr = sst[j][mm][0];
               if constexpr (KIND == 1) {
                 const R qi = sst[j][mm][1];
-                tr[mm] = fma(qr, gr, fma(-qi, gi, tr[mm]));
-                ti[mm] = fma(qr, gi, fma(qi, gr, ti[mm]));
+                tr(mm) = fma(qr, gr, fma(-qi, gi, tr(mm)));
+                ti(mm) = fma(qr, gi, fma(qi, gr, ti(mm)));
               } else {
-                tr[mm] = fma(qr, gr, tr[mm]);
+                tr(mm) = fma(qr, gr, tr(mm));
               }
             }
           }
@@ -598,8 +609,8 @@ __global__ void __launch_bounds__(kEvThreads)
 #pragma unroll
               for (int mm = 0; mm < MD; ++mm) {
                 const R2 sv = *reinterpret_cast<const R2*>(sst[j][mm]);
-                tr[mm] = fma(sv.x, kr_, fma(-sv.y, ki_, tr[mm]));
-                ti[mm] = fma(sv.x, ki_, fma(sv.y, kr_, ti[mm]));
+                tr(mm) = fma(sv.x, kr_, fma(-sv.y, ki_, tr(mm)));
+                ti(mm) = fma(sv.x, ki_, fma(sv.y, kr_, ti(mm)));
               }
             } else {
               R g, dd;
@@ -609,14 +620,16 @@ __global__ void __launch_bounds__(kEvThreads)
                 pair_lap_unit<R, false>(tx, ty, tz, sg0[j], sg1[j], thr2, g, dd);
               const R kv = fma(w.x, g, w.z * dd);
 #pragma unroll
-              for (int mm = 0; mm < MD; ++mm) tr[mm] = fma(sst[j][mm][0], kv, tr[mm]);
+              for (int mm = 0; mm < MD; ++mm) tr(mm) = fma(sst[j][mm][0], kv, tr(mm));
             }
           }
         }
+        if constexpr (kTileSums) {
 #pragma unroll
-        for (int mm = 0; mm < MD; ++mm) {
-          accr[mm] += double(tr[mm]);
-          acci[mm] += double(ti[mm]);
+          for (int mm = 0; mm < MD; ++mm) {
+            accr[mm] += double(trs[mm]);
+            acci[mm] += double(tis[mm]);
+          }
         }
       }
     }
