@@ -1303,7 +1303,7 @@ template <int CPLX>
 __global__ void mdot_partial_kernel(const double* __restrict__ V, int64_t ldv, int m,
                                     const double* __restrict__ w, const double* __restrict__ wts,
                                     int nd, Segs sg, double* __restrict__ partial) {
-  __shared__ double2 red[256];
+  __shared__ double2 red[512];  // 256 rows, or two halves of 8 warps x nd
   const int tid = threadIdx.x;
   const int rows = blockDim.x / nd;  // blockDim.x is a multiple of nd
   const int dd = tid % nd, r = tid / nd;
@@ -1323,19 +1323,43 @@ __global__ void mdot_partial_kernel(const double* __restrict__ V, int64_t ldv, i
         sr += wt * v[e] * w[e];
       }
     }
-    red[tid] = make_double2(sr, si);
-    __syncthreads();
-    if (tid < nd) {
-      double ar = 0, ai = 0;
-      for (int q = 0; q < rows; ++q) {
-        ar += red[q * nd + tid].x;
-        ai += red[q * nd + tid].y;
+    if (32 % nd == 0) {
+      // nd divides the warp: lane l holds density l % nd, so xor shuffles over
+      // offsets nd .. 16 sum each warp's rows; the warp sums of this k go to
+      // one half of red (halves alternate with k, one barrier per k)
+      for (int off = 16; off >= nd; off >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, off);
+        si += __shfl_xor_sync(0xffffffffu, si, off);
       }
-      const size_t o = (size_t(k) * nd + tid) * sg.nchunk + c;
-      partial[2 * o] = ar;
-      partial[2 * o + 1] = ai;
+      double2* half = red + (k & 1) * 256;
+      const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+      if (lane < nd) half[warp * nd + lane] = make_double2(sr, si);
+      __syncthreads();
+      if (tid < nd) {
+        double ar = 0, ai = 0;
+        for (int q = 0; q < nw; ++q) {
+          ar += half[q * nd + tid].x;
+          ai += half[q * nd + tid].y;
+        }
+        const size_t o = (size_t(k) * nd + tid) * sg.nchunk + c;
+        partial[2 * o] = ar;
+        partial[2 * o + 1] = ai;
+      }
+    } else {
+      red[tid] = make_double2(sr, si);
+      __syncthreads();
+      if (tid < nd) {
+        double ar = 0, ai = 0;
+        for (int q = 0; q < rows; ++q) {
+          ar += red[q * nd + tid].x;
+          ai += red[q * nd + tid].y;
+        }
+        const size_t o = (size_t(k) * nd + tid) * sg.nchunk + c;
+        partial[2 * o] = ar;
+        partial[2 * o + 1] = ai;
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 
