@@ -1303,12 +1303,45 @@ template <int CPLX>
 __global__ void mdot_partial_kernel(const double* __restrict__ V, int64_t ldv, int m,
                                     const double* __restrict__ w, const double* __restrict__ wts,
                                     int nd, Segs sg, double* __restrict__ partial) {
-  __shared__ double2 red[512];  // 256 rows, or two halves of 8 warps x nd
+  __shared__ double2 red[256];
   const int tid = threadIdx.x;
   const int rows = blockDim.x / nd;  // blockDim.x is a multiple of nd
   const int dd = tid % nd, r = tid / nd;
   const int c = blockIdx.x;
   const int64_t lo = sg.chunk_lo[c], hi = sg.chunk_hi[c];
+  if (32 % nd == 0) {
+    // nd divides the warp: each warp takes whole vectors k = warp, warp + nw,
+    // ... over the chunk (lane = row (lane / nd), density lane % nd), sums
+    // its rows with xor shuffles over offsets nd .. 16, and writes; no
+    // barriers
+    const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    const int wr = 32 / nd, ld = lane % nd, lr = lane / nd;
+    for (int k = warp; k < m; k += nw) {
+      const double* v = V + size_t(k) * ldv;
+      double sr = 0, si = 0;
+      for (int64_t pt = lo + lr; pt < hi; pt += wr) {
+        const int64_t e = pt * nd + ld;
+        const double wt = wts[pt];
+        if (CPLX) {
+          const double vr = v[2 * e], vi = v[2 * e + 1], xr = w[2 * e], xi = w[2 * e + 1];
+          sr += wt * (vr * xr + vi * xi);
+          si += wt * (vr * xi - vi * xr);
+        } else {
+          sr += wt * v[e] * w[e];
+        }
+      }
+      for (int off = 16; off >= nd; off >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, off);
+        si += __shfl_xor_sync(0xffffffffu, si, off);
+      }
+      if (lane < nd) {
+        const size_t o = (size_t(k) * nd + lane) * sg.nchunk + c;
+        partial[2 * o] = sr;
+        partial[2 * o + 1] = si;
+      }
+    }
+    return;
+  }
   for (int k = 0; k < m; ++k) {
     const double* v = V + size_t(k) * ldv;
     double sr = 0, si = 0;
@@ -1323,29 +1356,7 @@ __global__ void mdot_partial_kernel(const double* __restrict__ V, int64_t ldv, i
         sr += wt * v[e] * w[e];
       }
     }
-    if (32 % nd == 0) {
-      // nd divides the warp: lane l holds density l % nd, so xor shuffles over
-      // offsets nd .. 16 sum each warp's rows; the warp sums of this k go to
-      // one half of red (halves alternate with k, one barrier per k)
-      for (int off = 16; off >= nd; off >>= 1) {
-        sr += __shfl_xor_sync(0xffffffffu, sr, off);
-        si += __shfl_xor_sync(0xffffffffu, si, off);
-      }
-      double2* half = red + (k & 1) * 256;
-      const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-      if (lane < nd) half[warp * nd + lane] = make_double2(sr, si);
-      __syncthreads();
-      if (tid < nd) {
-        double ar = 0, ai = 0;
-        for (int q = 0; q < nw; ++q) {
-          ar += half[q * nd + tid].x;
-          ai += half[q * nd + tid].y;
-        }
-        const size_t o = (size_t(k) * nd + tid) * sg.nchunk + c;
-        partial[2 * o] = ar;
-        partial[2 * o + 1] = ai;
-      }
-    } else {
+    {
       red[tid] = make_double2(sr, si);
       __syncthreads();
       if (tid < nd) {
