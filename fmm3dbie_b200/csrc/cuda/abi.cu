@@ -229,7 +229,7 @@ int plan_from_arrays(bie::Plan& P, int kind, cdouble zk, cdouble alpha, cdouble 
                      const int64_t* iquad, int64_t nquad, const double* wnear,
                      const int64_t* novers, int64_t nptso, const int64_t* ixyzso,
                      const double* srcover, const double* whtsover, bool keep_f32,
-                     cudaStream_t st) {
+                     cudaStream_t st, bool async_weff = false) {
   int ier = ensure_tables();
   if (ier) return ier;
   ier = check_surf(npatches, norders, ixyzs, iptype, npts);
@@ -261,6 +261,7 @@ int plan_from_arrays(bie::Plan& P, int kind, cdouble zk, cdouble alpha, cdouble 
   sp.srcover = srcover;
   sp.whtsover = whtsover;
   sp.keep_f32 = keep_f32;
+  sp.async_weff = async_weff;
   return P.build(sp, st);
 }
 
@@ -324,10 +325,11 @@ int solve_on_gpu(int kind, cdouble zk, cdouble alpha, cdouble beta, int64_t npat
   Stage stg;
   bie::AllocStreamScope alloc_scope(stg.st);  // plan buffers return to the pool on stg.st
   bie::Plan P;
+  // the near quadrature's upload and folds overlap the start of the solve
   int ier = plan_from_arrays(P, kind, zk, alpha, beta, npatches, norders, ixyzs, iptype, npts,
                              srccoefs, srcvals, 12, npts, srcvals, nnz, row_ptr, col_ind, iquad,
                              nquad, wnear, novers, nptso, ixyzso, srcover, whtsover, iprec == 1,
-                             stg.st);
+                             stg.st, true);
   if (ier) return ier;
   P.targets_on_surface = true;
   const int c = kind == 1 ? 2 : 1;

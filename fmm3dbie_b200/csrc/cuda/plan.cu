@@ -69,6 +69,15 @@ Plan::Plan() = default;
 Plan::~Plan() {
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
+  if (wst_) cudaStreamSynchronize(wst_);  // W_eff work done before its buffers go
+  if (wev_in_) cudaEventDestroy(wev_in_);
+  if (wev_done_) cudaEventDestroy(wev_done_);
+  if (wst_) cudaStreamDestroy(wst_);
+}
+
+int Plan::wait_weff(cudaStream_t st) {
+  if (wev_done_) BIE_CUDA(cudaStreamWaitEvent(st, wev_done_, 0));
+  return kOk;
 }
 
 int Plan::build(const PlanSpec& s, cudaStream_t st) {
@@ -127,7 +136,16 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   // builds the other arrays; the fold below follows it on the stream.
   const size_t wlen = size_t(nquad) * (cplx ? 2 : 1);
   BIE_CUDA(weff64_.alloc(std::max<size_t>(wlen, 1)));
-  if (wlen) BIE_CUDA(cudaMemcpyAsync(weff64_.p, s.wnear, wlen * sizeof(double), cudaMemcpyHostToDevice, st));
+  cudaStream_t wst = st;  // the stream of the W_eff upload and folds
+  if (s.async_weff) {
+    BIE_CUDA(cudaStreamCreateWithFlags(&wst_, cudaStreamNonBlocking));
+    BIE_CUDA(cudaEventCreateWithFlags(&wev_in_, cudaEventDisableTiming));
+    BIE_CUDA(cudaEventCreateWithFlags(&wev_done_, cudaEventDisableTiming));
+    BIE_CUDA(cudaEventRecord(wev_in_, st));  // the allocation, ordered on st
+    BIE_CUDA(cudaStreamWaitEvent(wst_, wev_in_, 0));
+    wst = wst_;
+  }
+  if (wlen) BIE_CUDA(cudaMemcpyAsync(weff64_.p, s.wnear, wlen * sizeof(double), cudaMemcpyHostToDevice, wst));
   for (int64_t k = 0; k < nnz; ++k) {
     const int64_t c = s.col_ind[k];
     if (c < 1 || c > npatches || s.iquad[k + 1] - s.iquad[k] != s.ixyzs[c] - s.ixyzs[c - 1]) {
@@ -295,12 +313,16 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   nr.nps = nps_.p;
   nr.wofs = wofs_.p;
   // ---- fold the smooth near part into W_eff (in place over wnear) -----------
-  if (s.keep_f32) {
-    // FP32 path: subtract the smooth part as the FP32 far kernel computes it
-    BIE_CUDA(weff32_.alloc(std::max<size_t>(wlen, 1)));
-    BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff32_.p, 1, st));
+  if (s.keep_f32) BIE_CUDA(weff32_.alloc(std::max<size_t>(wlen, 1)));
+  if (wst_) {
+    // the folds read the geometry uploaded on st and the buffers allocated there
+    BIE_CUDA(cudaEventRecord(wev_in_, st));
+    BIE_CUDA(cudaStreamWaitEvent(wst_, wev_in_, 0));
   }
-  BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff64_.p, 0, st));
+  // FP32 path: subtract the smooth part as the FP32 far kernel computes it
+  if (s.keep_f32) BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff32_.p, 1, wst));
+  BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff64_.p, 0, wst));
+  if (wst_) BIE_CUDA(cudaEventRecord(wev_done_, wst_));
   // per-source constants alpha w/(4pi), beta w/(4pi) for the multi-density far kernel
   BIE_CUDA(ab64_.alloc(size_t(nptso) * (cplx ? 4 : 2)));
   BIE_CUDA(ab32_.alloc(size_t(nptso) * (cplx ? 4 : 2)));
@@ -368,6 +390,7 @@ const TreeStats* Plan::tree_stats(int precision) const {
 
 int Plan::refold32(const double* tcen, cudaStream_t st) {
   if (!weff32_.p) return kOk;
+  if (int e = wait_weff(st)) return e;
   dev::Geometry gg = g;
   gg.tcen = tcen;
   BIE_CUDA(dev::launch_fold(gg, nr, kp, weff64_.p, weff32_.p, 2, st));
@@ -592,6 +615,7 @@ int Plan::matvec(int precision, int nd, const double* d_sigma, double* d_pot, cu
   }
   BIE_CUDA(launch_far_stage(a, st));
   if (timing) BIE_CUDA(cudaEventRecord(ev_[2], st));
+  if (int e = wait_weff(st)) return e;
   BIE_CUDA(dev::launch_combine(g, nr, kp, a, st));
   if (timing) {
     BIE_CUDA(cudaEventRecord(ev_[3], st));
@@ -634,6 +658,7 @@ int Plan::matvec_tree(int precision, int nd, const double* d_sigma, double* d_po
   BIE_CUDA(T.run(precision, nd, kp, nd > 1 ? nullptr : str_.p, partial_.p, st,
                  nd > 1 ? str_.p : nullptr));
   if (timing) BIE_CUDA(cudaEventRecord(ev_[2], st));
+  if (int e = wait_weff(st)) return e;
   BIE_CUDA(dev::launch_combine(g, nr, kp, a, st));
   if (timing) {
     BIE_CUDA(cudaEventRecord(ev_[3], st));

@@ -120,6 +120,12 @@ struct PlanSpec {
   const double* srcover = nullptr;  // 12 x nptso
   const double* whtsover = nullptr;
   bool keep_f32 = true;  // also keep an f32 copy of W_eff
+  // Upload the near quadrature and fold W_eff on a second stream that the
+  // plan's matvecs wait on at their near correction (an event), so that a
+  // solve started right after the build runs its first far field while the
+  // near quadrature is still on its way.  Only for plans whose W_eff is read
+  // through Plan::matvec (not the batch engine).
+  bool async_weff = false;
 };
 
 struct GmresWorkspace {
@@ -221,6 +227,8 @@ class Plan : public Operator {
   // Nonzero once a tensor-core far-field launch timed out waiting for its MMAs.
   int tc_error() const;
   int* tc_err_ptr() { return tc_err_.p; }
+  // makes st wait for W_eff (a no-op unless the plan was built with async_weff)
+  int wait_weff(cudaStream_t st);
   // several-density oversampling of a matvec on the engine of
   // dev::oversample_engine() (a.tc_err is the plan's flag)
   cudaError_t oversample(const dev::MatvecArgs& a, cudaStream_t st);
@@ -269,6 +277,9 @@ class Plan : public Operator {
   DBuf<char> str_;
   DBuf<double> partial_;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+  // async_weff: the W_eff stream and the events that order it
+  cudaStream_t wst_ = nullptr;
+  cudaEvent_t wev_in_ = nullptr, wev_done_ = nullptr;
 };
 
 // A batch of surfaces solved together: one operator whose nodes are the
