@@ -324,6 +324,19 @@ int solve_on_gpu(int kind, cdouble zk, cdouble alpha, cdouble beta, int64_t npat
   }
   Stage stg;
   bie::AllocStreamScope alloc_scope(stg.st);  // plan buffers return to the pool on stg.st
+  // The right-hand sides go first: a copy issued while the near quadrature's
+  // chunks are in flight waits for them on the copy engine.
+  const int c = kind == 1 ? 2 : 1;
+  const size_t len = size_t(npts) * nrhs * c;
+  bie::DBuf<double> dr, dx;
+  if (dr.alloc(len) || dx.alloc(len)) {
+    bie::set_last_error("device allocation failed");
+    return BIE_ERR_NOMEM;
+  }
+  if (cudaMemcpyAsync(dr.p, rhs, sizeof(double) * len, cudaMemcpyHostToDevice, stg.st) != cudaSuccess) {
+    bie::set_last_error("right-hand side upload failed");
+    return BIE_ERR_CUDA;
+  }
   bie::Plan P;
   // the near quadrature's upload and folds overlap the start of the solve
   int ier = plan_from_arrays(P, kind, zk, alpha, beta, npatches, norders, ixyzs, iptype, npts,
@@ -332,14 +345,6 @@ int solve_on_gpu(int kind, cdouble zk, cdouble alpha, cdouble beta, int64_t npat
                              stg.st, true);
   if (ier) return ier;
   P.targets_on_surface = true;
-  const int c = kind == 1 ? 2 : 1;
-  const size_t len = size_t(npts) * nrhs * c;
-  bie::DBuf<double> dr, dx;
-  if (dr.alloc(len) || dx.alloc(len)) {
-    bie::set_last_error("device allocation failed");
-    return BIE_ERR_NOMEM;
-  }
-  cudaMemcpyAsync(dr.p, rhs, sizeof(double) * len, cudaMemcpyHostToDevice, stg.st);
   // zid = -(-1)^ifinout beta/2 (helm_comb_dir.f:2215, lap_comb_dir.f90:1619)
   const double sgn = (ifinout % 2 == 0) ? -1.0 : 1.0;
   const std::vector<cdouble> zid(size_t(nrhs), sgn * beta / 2.0);  // one per system

@@ -103,8 +103,10 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
 // (same centring and pair functions), weff is float*.
 // match32 = 2: wnear is the FP64 W_eff; weff (float*) = wnear + exact part -
 // FP32-matched part (an FP32 W_eff for another far-field centring).
+// Near pairs k0 .. k1 - 1 only (k1 < 0: to the last pair).
 cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp,
-                        const double* wnear, void* weff, int match32, cudaStream_t st);
+                        const double* wnear, void* weff, int match32, cudaStream_t st,
+                        int64_t k0 = 0, int64_t k1 = -1);
 cudaError_t launch_to_f32(const double* in, float* out, int64_t n, cudaStream_t st);
 // Caller strengths (charge, dipole strength per source; complex interleaved
 // when kind == 1) -> far-kernel layout in the far precision, times 1/(4 pi).

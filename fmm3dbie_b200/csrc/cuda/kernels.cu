@@ -1125,13 +1125,13 @@ constexpr int kFarBlockTargetsF32 = 512;  // kFarThreads * kTptF32 (checked belo
 
 template <int CPLX, int MATCH32, typename OUT>
 __global__ void fold_kernel(Geometry g, Near nr, KParams kp, const double* __restrict__ wnear,
-                            OUT* __restrict__ weff) {
+                            OUT* __restrict__ weff, int64_t k0, int64_t k1) {
   extern __shared__ double sh[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double* a = sh + size_t(warp) * g.max_nf * 2;
-  // find the row of pair k by binary search over row_ptr
-  const int64_t k = int64_t(blockIdx.x) * (blockDim.x >> 5) + warp;
-  if (k >= nr.nnz) return;
+  // find the row of pair k (near pairs k0 .. k1 - 1) by binary search over row_ptr
+  const int64_t k = k0 + int64_t(blockIdx.x) * (blockDim.x >> 5) + warp;
+  if (k >= k1) return;
   int64_t lo = 0, hi = g.ntarg;  // row_ptr[lo] <= k < row_ptr[hi]
   while (hi - lo > 1) {
     const int64_t mid = (lo + hi) >> 1;
@@ -2161,26 +2161,27 @@ cudaError_t launch_combine(const Geometry& g, const Near& nr, const KParams& kp,
 }
 
 cudaError_t launch_fold(const Geometry& g, const Near& nr, const KParams& kp, const double* wnear,
-                        void* weff, int match32, cudaStream_t st) {
-  if (nr.nnz == 0) return cudaSuccess;
+                        void* weff, int match32, cudaStream_t st, int64_t k0, int64_t k1) {
+  if (k1 < 0) k1 = nr.nnz;
+  if (k1 <= k0) return cudaSuccess;
   const int warps = 4;
   const size_t sh = size_t(warps) * g.max_nf * 2 * sizeof(double);
   if (sh > 48 * 1024) return cudaErrorInvalidValue;  // max_nf <= 289 keeps this <= 18.5 KB
-  const dim3 grid(static_cast<unsigned>((nr.nnz + warps - 1) / warps)), block(32 * warps);
+  const dim3 grid(static_cast<unsigned>((k1 - k0 + warps - 1) / warps)), block(32 * warps);
   if (kp.kind == 1) {
     if (match32 == 2)
-      fold_kernel<1, 2, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
+      fold_kernel<1, 2, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff, k0, k1);
     else if (match32)
-      fold_kernel<1, 1, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
+      fold_kernel<1, 1, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff, k0, k1);
     else
-      fold_kernel<1, 0, double><<<grid, block, sh, st>>>(g, nr, kp, wnear, (double*)weff);
+      fold_kernel<1, 0, double><<<grid, block, sh, st>>>(g, nr, kp, wnear, (double*)weff, k0, k1);
   } else {
     if (match32 == 2)
-      fold_kernel<0, 2, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
+      fold_kernel<0, 2, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff, k0, k1);
     else if (match32)
-      fold_kernel<0, 1, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff);
+      fold_kernel<0, 1, float><<<grid, block, sh, st>>>(g, nr, kp, wnear, (float*)weff, k0, k1);
     else
-      fold_kernel<0, 0, double><<<grid, block, sh, st>>>(g, nr, kp, wnear, (double*)weff);
+      fold_kernel<0, 0, double><<<grid, block, sh, st>>>(g, nr, kp, wnear, (double*)weff, k0, k1);
   }
   count();
   return cudaGetLastError();

@@ -7,7 +7,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
+#include <stdexcept>
 #include <tuple>
 
 #include "../host/basis.h"
@@ -35,6 +37,109 @@ cudaError_t upload(DBuf<T>& b, const std::vector<T>& h, cudaStream_t st) {
   if (h.empty()) return cudaSuccess;
   return cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
 }
+template <class T>
+cudaError_t upload(DBuf<T>& b, const T* h, size_t n, cudaStream_t st) {
+  cudaError_t e = b.alloc(std::max<size_t>(n, 1));
+  if (e != cudaSuccess || n == 0) return e;
+  return cudaMemcpyAsync(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+// near-pair chunks of the near quadrature's upload in an async_weff build,
+// and how many of them are issued before the host builds the other arrays
+// (about the 2 ms that building takes at the PCIe bandwidth, for the
+// 287 MB of a 35,840-node Helmholtz surface)
+constexpr int kWeffChunks = 8, kWeffEarlyChunks = 3;
+
+// Interpolation matrices by (patch type, order, oversampled order): functions
+// of the key alone, computed once per process and shared by every plan.
+int cached_interp_matrix(int ip, int no, int nf, const std::vector<double>*& m) {
+  static std::mutex mu;
+  static auto* cache = new std::map<std::tuple<int, int, int>, std::vector<double>>;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_tuple(ip, no, nf);
+  auto it = cache->find(key);
+  if (it == cache->end()) {
+    std::vector<double> v;
+    if (const int ier = interp_matrix(ip, no, nf, v)) return ier;
+    it = cache->emplace(key, std::move(v)).first;
+  }
+  m = &it->second;
+  return 0;
+}
+
+// Pinned staging for the arrays a plan build assembles on the host, shared by
+// the builds of the process one at a time.  It is allocated (its pages
+// faulted in) once and grown when a larger plan comes, so the uploads out of
+// it are asynchronous and a build pays no page faults.  A build that finds it
+// in use by another thread, or needs more than kMaxPinned bytes, stages in
+// pageable memory instead.  The destructor waits for the copies out of it.
+class HostStaging {
+ public:
+  static constexpr size_t kMaxPinned = size_t(256) << 20;
+  template <class T>
+  static size_t bytes(size_t n) {
+    return (n * sizeof(T) + 63) / 64 * 64;
+  }
+  explicit HostStaging(size_t n) : cap_(n) {
+    Pool& pl = pool();
+    if (n <= kMaxPinned && pl.mu.try_lock()) {
+      locked_ = true;
+      if (pl.cap < n) {
+        if (pl.p) cudaFreeHost(pl.p);
+        pl.p = nullptr;
+        pl.cap = 0;
+        const size_t want = std::min(kMaxPinned, std::max(n + n / 4, size_t(8) << 20));
+        void* q = nullptr;
+        if (cudaHostAlloc(&q, want, cudaHostAllocPortable) == cudaSuccess) {
+          pl.p = static_cast<char*>(q);
+          pl.cap = want;
+        } else {
+          cudaGetLastError();  // pageable staging below
+        }
+      }
+      base_ = pl.p;
+    }
+    if (!base_) {
+      heap_.reset(new char[n + 64]);
+      base_ = heap_.get() + (64 - reinterpret_cast<uintptr_t>(heap_.get()) % 64) % 64;
+    }
+  }
+  ~HostStaging() {
+    if (st_set_) cudaStreamSynchronize(st_);
+    if (locked_) pool().mu.unlock();
+  }
+  HostStaging(const HostStaging&) = delete;
+  HostStaging& operator=(const HostStaging&) = delete;
+  // the stream that the uploads out of the buffer are issued on
+  void copies_on(cudaStream_t st) {
+    st_ = st;
+    st_set_ = true;
+  }
+  template <class T>
+  T* take(size_t n) {
+    const size_t b = bytes<T>(n);
+    if (off_ + b > cap_) throw std::logic_error("plan staging buffer too small");
+    T* r = reinterpret_cast<T*>(base_ + off_);
+    off_ += b;
+    return r;
+  }
+
+ private:
+  struct Pool {
+    std::mutex mu;
+    char* p = nullptr;
+    size_t cap = 0;
+  };
+  static Pool& pool() {
+    static Pool* p = new Pool;  // never destroyed: builds may run during exit
+    return *p;
+  }
+  char* base_ = nullptr;
+  size_t cap_ = 0, off_ = 0;
+  bool locked_ = false, st_set_ = false;
+  cudaStream_t st_ = nullptr;
+  std::unique_ptr<char[]> heap_;
+};
 }  // namespace
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
@@ -69,10 +174,15 @@ Plan::Plan() = default;
 Plan::~Plan() {
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
-  if (wst_) cudaStreamSynchronize(wst_);  // W_eff work done before its buffers go
+  // W_eff copies and folds done before their buffers go
+  if (wst_) cudaStreamSynchronize(wst_);
+  if (fst_) cudaStreamSynchronize(fst_);
   if (wev_in_) cudaEventDestroy(wev_in_);
   if (wev_done_) cudaEventDestroy(wev_done_);
+  for (auto e : wev_copy_)
+    if (e) cudaEventDestroy(e);
   if (wst_) cudaStreamDestroy(wst_);
+  if (fst_) cudaStreamDestroy(fst_);
 }
 
 int Plan::wait_weff(cudaStream_t st) {
@@ -132,82 +242,159 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
     return kErrArg;
   }
   // The near quadrature (the largest input: nquad entries) goes to the device
-  // first, so that its copy runs while the host checks the near list and
-  // builds the other arrays; the fold below follows it on the stream.
-  const size_t wlen = size_t(nquad) * (cplx ? 2 : 1);
+  // in near-pair chunks.  The first chunks' copies run while the host checks
+  // the near list and builds the other arrays; the uploads of those follow,
+  // and the other chunks wait for them, so that the geometry lands early
+  // (copy engines take the copies of different streams in turns, not in the
+  // order they were issued).  With async_weff each chunk's folds start on
+  // their own stream as soon as the chunk has landed, beside the solve's
+  // first far field.
+  const int cw = cplx ? 2 : 1;
+  const size_t wlen = size_t(nquad) * cw;
   BIE_CUDA(weff64_.alloc(std::max<size_t>(wlen, 1)));
-  cudaStream_t wst = st;  // the stream of the W_eff upload and folds
+  const int nwc = (s.async_weff && nnz >= int64_t(kWeffChunks) * 1024) ? kWeffChunks : 1;
+  std::vector<int64_t> kc(nwc + 1, 0), qc(nwc + 1, 0);
+  for (int c = 1; c <= nwc; ++c) {
+    kc[c] = nnz * c / nwc;
+    // clamped into order: an iquad that is not monotone is rejected below,
+    // before any fold reads W_eff
+    qc[c] = c == nwc ? nquad : std::min(nquad, std::max(qc[c - 1], s.iquad[kc[c]] - 1));
+  }
+  cudaStream_t wst = st, fst = st;  // streams of the W_eff chunk copies and of the folds
   if (s.async_weff) {
     BIE_CUDA(cudaStreamCreateWithFlags(&wst_, cudaStreamNonBlocking));
+    BIE_CUDA(cudaStreamCreateWithFlags(&fst_, cudaStreamNonBlocking));
     BIE_CUDA(cudaEventCreateWithFlags(&wev_in_, cudaEventDisableTiming));
     BIE_CUDA(cudaEventCreateWithFlags(&wev_done_, cudaEventDisableTiming));
+    wev_copy_.assign(size_t(nwc), nullptr);
+    for (auto& e : wev_copy_) BIE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     BIE_CUDA(cudaEventRecord(wev_in_, st));  // the allocation, ordered on st
     BIE_CUDA(cudaStreamWaitEvent(wst_, wev_in_, 0));
     wst = wst_;
+    fst = fst_;
   }
-  if (wlen) BIE_CUDA(cudaMemcpyAsync(weff64_.p, s.wnear, wlen * sizeof(double), cudaMemcpyHostToDevice, wst));
+  // an input rejected below returns while chunk copies may still read the
+  // caller's near quadrature: they finish first
+  struct CopyGuard {
+    cudaStream_t s;
+    bool done = false;
+    ~CopyGuard() {
+      if (!done) cudaStreamSynchronize(s);
+    }
+  } copy_guard{wst};
+  auto copy_chunk = [&](int c) -> int {
+    if (qc[c + 1] > qc[c])
+      BIE_CUDA(cudaMemcpyAsync(weff64_.p + qc[c] * cw, s.wnear + qc[c] * cw,
+                               size_t(qc[c + 1] - qc[c]) * cw * sizeof(double),
+                               cudaMemcpyHostToDevice, wst));
+    if (!wev_copy_.empty()) BIE_CUDA(cudaEventRecord(wev_copy_[size_t(c)], wst));
+    return kOk;
+  };
+  const int early = nwc > 1 ? std::min(nwc - 1, kWeffEarlyChunks) : 1;
+  for (int c = 0; c < early; ++c)
+    if (int e = copy_chunk(c)) return e;
+  // ---- interpolation classes -------------------------------------------------
+  std::vector<int32_t> cls_of(npatches);
+  std::vector<const std::vector<double>*> cls_mat;
+  {
+    std::map<std::tuple<int, int, int>, int> cls;
+    for (int64_t p = 0; p < npatches; ++p) {
+      auto key = std::make_tuple(int(s.iptype[p]), int(s.norders[p]), int(s.novers[p]));
+      auto it = cls.find(key);
+      if (it == cls.end()) {
+        const std::vector<double>* m = nullptr;
+        const int ier = cached_interp_matrix(std::get<0>(key), std::get<1>(key), std::get<2>(key), m);
+        if (ier) {
+          set_last_error("interpolation matrix: basis tables unavailable or singular");
+          return ier == 6 ? kErrTables : kErrSingular;
+        }
+        it = cls.emplace(key, int(cls_mat.size())).first;
+        cls_mat.push_back(m);
+      }
+      cls_of[p] = it->second;
+    }
+  }
+  size_t nim = 0;
+  for (const auto* m : cls_mat) nim += m->size();
+  // ---- host-side arrays, in the pinned staging buffer --------------------------
+  const int64_t nbt = (ntarg + dev::kFarBlockTargets32 - 1) / dev::kFarBlockTargets32;
+  const int64_t nbs = (nptso + dev::kFarTileSources - 1) / dev::kFarTileSources;
+  const size_t nbt6 = size_t(6) * std::max<int64_t>(nbt, 1), nbs6 = size_t(6) * std::max<int64_t>(nbs, 1);
+  using HS = HostStaging;
+  const size_t stage_bytes =
+      3 * HS::bytes<double>(ntarg) + 7 * HS::bytes<double>(nptso) +
+      2 * HS::bytes<int32_t>(npatches + 1) + HS::bytes<int32_t>(npatches) +
+      HS::bytes<int64_t>(cls_mat.size()) + HS::bytes<double>(nim) + HS::bytes<int64_t>(ntarg + 1) +
+      HS::bytes<int64_t>(nnz + 1) + 2 * HS::bytes<int32_t>(nnz) + HS::bytes<double>(npts) +
+      HS::bytes<double>(nbt6) + HS::bytes<double>(nbs6);
+  HostStaging stage(stage_bytes);
+  double* htx = stage.take<double>(ntarg);
+  double* hty = stage.take<double>(ntarg);
+  double* htz = stage.take<double>(ntarg);
+  double* hsrc[7];
+  for (auto& h : hsrc) h = stage.take<double>(nptso);
+  int32_t* hps = stage.take<int32_t>(npatches + 1);
+  int32_t* hos = stage.take<int32_t>(npatches + 1);
+  int32_t* hpc = stage.take<int32_t>(npatches);
+  int64_t* hcm = stage.take<int64_t>(cls_mat.size());
+  double* him = stage.take<double>(nim);
+  int64_t* hrp = stage.take<int64_t>(ntarg + 1);
+  int64_t* hwo = stage.take<int64_t>(nnz + 1);
+  int32_t* hcol = stage.take<int32_t>(nnz);
+  int32_t* hnps = stage.take<int32_t>(nnz);
+  double* hqw = stage.take<double>(npts);
+  double* htb = stage.take<double>(nbt6);
+  double* hsb = stage.take<double>(nbs6);
+  // the near list, checked and converted in one pass
+  int64_t bad = nnz;
+#pragma omp parallel for schedule(static) reduction(min : bad) if (nnz >= 65536)
   for (int64_t k = 0; k < nnz; ++k) {
     const int64_t c = s.col_ind[k];
     if (c < 1 || c > npatches || s.iquad[k + 1] - s.iquad[k] != s.ixyzs[c] - s.ixyzs[c - 1]) {
-      set_last_error("col_ind/iquad entry " + std::to_string(k + 1) + " invalid");
-      return kErrArg;
+      bad = std::min(bad, k);
+      continue;
     }
+    hcol[k] = int32_t(c - 1);
+    hnps[k] = int32_t(s.ixyzs[c - 1] - 1);
+    hwo[k] = s.iquad[k] - 1;
   }
-  // ---- host-side arrays ------------------------------------------------------
-  std::vector<double> htx(ntarg), hty(ntarg), htz(ntarg);
+  if (bad < nnz) {
+    set_last_error("col_ind/iquad entry " + std::to_string(bad + 1) + " invalid");
+    return kErrArg;
+  }
+  hwo[nnz] = nquad;
+  for (int64_t i = 0; i <= ntarg; ++i) hrp[i] = s.row_ptr[i] - 1;
+#pragma omp parallel for schedule(static) if (ntarg >= 65536)
   for (int64_t i = 0; i < ntarg; ++i) {
     htx[i] = s.targs[size_t(s.ndtarg) * i];
     hty[i] = s.targs[size_t(s.ndtarg) * i + 1];
     htz[i] = s.targs[size_t(s.ndtarg) * i + 2];
   }
-  std::vector<double> hsx(nptso), hsy(nptso), hsz(nptso), hnx(nptso), hny(nptso), hnz(nptso),
-      hw(nptso);
+#pragma omp parallel for schedule(static) if (nptso >= 65536)
   for (int64_t j = 0; j < nptso; ++j) {
     const double* o = s.srcover + 12 * j;
-    hsx[j] = o[0];
-    hsy[j] = o[1];
-    hsz[j] = o[2];
-    hnx[j] = o[9];
-    hny[j] = o[10];
-    hnz[j] = o[11];
-    hw[j] = s.whtsover[j];
+    hsrc[0][j] = o[0];
+    hsrc[1][j] = o[1];
+    hsrc[2][j] = o[2];
+    hsrc[3][j] = o[9];
+    hsrc[4][j] = o[10];
+    hsrc[5][j] = o[11];
+    hsrc[6][j] = s.whtsover[j];
   }
-  std::vector<int32_t> hps(npatches + 1), hos(npatches + 1), hpc(npatches);
-  std::map<std::tuple<int, int, int>, int> cls;
-  std::vector<int64_t> hcm;
-  std::vector<double> him;
   for (int64_t p = 0; p <= npatches; ++p) {
     hps[p] = int32_t(s.ixyzs[p] - 1);
     hos[p] = int32_t(s.ixyzso[p] - 1);
   }
-  for (int64_t p = 0; p < npatches; ++p) {
-    auto key = std::make_tuple(int(s.iptype[p]), int(s.norders[p]), int(s.novers[p]));
-    auto it = cls.find(key);
-    if (it == cls.end()) {
-      std::vector<double> m;
-      const int ier = interp_matrix(std::get<0>(key), std::get<1>(key), std::get<2>(key), m);
-      if (ier) {
-        set_last_error("interpolation matrix: basis tables unavailable or singular");
-        return ier == 6 ? kErrTables : kErrSingular;
-      }
-      const int id = int(hcm.size());
-      hcm.push_back(int64_t(him.size()));
-      him.insert(him.end(), m.begin(), m.end());
-      it = cls.emplace(key, id).first;
+  for (int64_t p = 0; p < npatches; ++p) hpc[p] = cls_of[p];
+  {
+    size_t o = 0;
+    for (size_t c = 0; c < cls_mat.size(); ++c) {
+      hcm[c] = int64_t(o);
+      std::copy(cls_mat[c]->begin(), cls_mat[c]->end(), him + o);
+      o += cls_mat[c]->size();
     }
-    hpc[p] = it->second;
   }
-  std::vector<int64_t> hrp(ntarg + 1), hwo(nnz + 1);
-  std::vector<int32_t> hcol(nnz), hnps(nnz);
-  for (int64_t i = 0; i <= ntarg; ++i) hrp[i] = s.row_ptr[i] - 1;
-  for (int64_t k = 0; k < nnz; ++k) {
-    hcol[k] = int32_t(s.col_ind[k] - 1);
-    hnps[k] = hps[hcol[k]];
-    hwo[k] = s.iquad[k] - 1;
-  }
-  hwo[nnz] = nquad;
   // smooth quadrature weights at the nodes (needed by the GMRES inner product)
-  std::vector<double> hqw(npts);
   {
     Surf sf;
     sf.npatches = npatches;
@@ -217,7 +404,7 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
     sf.iptype = s.iptype;
     sf.srccoefs = s.srccoefs;
     sf.srcvals = s.srcvals;
-    qwts(sf, hqw.data());
+    qwts(sf, hqw);
   }
   kp.kind = kind;
   kp.ar = s.alpha.real();
@@ -231,10 +418,11 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   // bounding boxes of the FP32 far kernel's target blocks and source tiles;
   // margin: the threshold plus 2^-12 of the extent, far above the FP32
   // rounding of the centred coordinates
-  auto boxes = [](const std::vector<double>& x, const std::vector<double>& y,
-                  const std::vector<double>& z, int64_t per, std::vector<double>& out) {
-    const int64_t n = int64_t(x.size()), nb = (n + per - 1) / per;
-    out.assign(size_t(6) * std::max<int64_t>(nb, 1), 0.0);
+  auto boxes = [](const double* x, const double* y, const double* z, int64_t n, int64_t per,
+                  double* out) {
+    const int64_t nb = (n + per - 1) / per;
+    if (nb == 0) std::fill(out, out + 6, 0.0);
+#pragma omp parallel for schedule(static) if (nb >= 256)
     for (int64_t b = 0; b < nb; ++b) {
       double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
       for (int64_t j = b * per; j < std::min(n, (b + 1) * per); ++j) {
@@ -250,38 +438,44 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
       }
     }
   };
-  std::vector<double> htb, hsb;
-  boxes(htx, hty, htz, dev::kFarBlockTargets32, htb);
-  boxes(hsx, hsy, hsz, dev::kFarTileSources, hsb);
+  boxes(htx, hty, htz, ntarg, dev::kFarBlockTargets32, htb);
+  boxes(hsrc[0], hsrc[1], hsrc[2], nptso, dev::kFarTileSources, hsb);
   double ext = 0.0;
-  for (size_t b = 0; b + 5 < htb.size(); b += 6)
-    for (int c = 0; c < 3; ++c) ext = std::max(ext, std::fabs(htb[b + c]) + std::fabs(htb[b + 3 + c]));
-  for (size_t b = 0; b + 5 < hsb.size(); b += 6)
-    for (int c = 0; c < 3; ++c) ext = std::max(ext, std::fabs(hsb[b + c]) + std::fabs(hsb[b + 3 + c]));
+  for (int64_t b = 0; b < nbt; ++b)
+    for (int c = 0; c < 3; ++c) ext = std::max(ext, std::fabs(htb[6 * b + c]) + std::fabs(htb[6 * b + 3 + c]));
+  for (int64_t b = 0; b < nbs; ++b)
+    for (int c = 0; c < 3; ++c) ext = std::max(ext, std::fabs(hsb[6 * b + c]) + std::fabs(hsb[6 * b + 3 + c]));
   const double margin = kp.thresh + std::ldexp(ext, -12);
   // ---- upload ----------------------------------------------------------------
-  BIE_CUDA(upload(tx_, htx, st));
-  BIE_CUDA(upload(ty_, hty, st));
-  BIE_CUDA(upload(tz_, htz, st));
-  BIE_CUDA(upload(sx_, hsx, st));
-  BIE_CUDA(upload(sy_, hsy, st));
-  BIE_CUDA(upload(sz_, hsz, st));
-  BIE_CUDA(upload(snx_, hnx, st));
-  BIE_CUDA(upload(sny_, hny, st));
-  BIE_CUDA(upload(snz_, hnz, st));
-  BIE_CUDA(upload(sw_, hw, st));
-  BIE_CUDA(upload(pstart_, hps, st));
-  BIE_CUDA(upload(ostart_, hos, st));
-  BIE_CUDA(upload(pclass_, hpc, st));
-  BIE_CUDA(upload(cmoff_, hcm, st));
-  BIE_CUDA(upload(imat_, him, st));
-  BIE_CUDA(upload(row_ptr_, hrp, st));
-  BIE_CUDA(upload(col_, hcol, st));
-  BIE_CUDA(upload(nps_, hnps, st));
-  BIE_CUDA(upload(wofs_, hwo, st));
-  BIE_CUDA(upload(wts_, hqw, st));
-  BIE_CUDA(upload(tbox_, htb, st));
-  BIE_CUDA(upload(sbox_, hsb, st));
+  stage.copies_on(st);
+  BIE_CUDA(upload(tx_, htx, ntarg, st));
+  BIE_CUDA(upload(ty_, hty, ntarg, st));
+  BIE_CUDA(upload(tz_, htz, ntarg, st));
+  BIE_CUDA(upload(sx_, hsrc[0], nptso, st));
+  BIE_CUDA(upload(sy_, hsrc[1], nptso, st));
+  BIE_CUDA(upload(sz_, hsrc[2], nptso, st));
+  BIE_CUDA(upload(snx_, hsrc[3], nptso, st));
+  BIE_CUDA(upload(sny_, hsrc[4], nptso, st));
+  BIE_CUDA(upload(snz_, hsrc[5], nptso, st));
+  BIE_CUDA(upload(sw_, hsrc[6], nptso, st));
+  BIE_CUDA(upload(pstart_, hps, npatches + 1, st));
+  BIE_CUDA(upload(ostart_, hos, npatches + 1, st));
+  BIE_CUDA(upload(pclass_, hpc, npatches, st));
+  BIE_CUDA(upload(cmoff_, hcm, cls_mat.size(), st));
+  BIE_CUDA(upload(imat_, him, nim, st));
+  BIE_CUDA(upload(row_ptr_, hrp, ntarg + 1, st));
+  BIE_CUDA(upload(col_, hcol, nnz, st));
+  BIE_CUDA(upload(nps_, hnps, nnz, st));
+  BIE_CUDA(upload(wofs_, hwo, nnz + 1, st));
+  BIE_CUDA(upload(wts_, hqw, npts, st));
+  BIE_CUDA(upload(tbox_, htb, nbt6, st));
+  BIE_CUDA(upload(sbox_, hsb, nbs6, st));
+  if (early < nwc) {
+    BIE_CUDA(cudaEventRecord(wev_in_, st));  // the uploads above
+    BIE_CUDA(cudaStreamWaitEvent(wst_, wev_in_, 0));
+  }
+  for (int c = early; c < nwc; ++c)
+    if (int e = copy_chunk(c)) return e;
   g.ntarg = ntarg;
   g.nptso = nptso;
   g.npatches = npatches;
@@ -314,15 +508,19 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   nr.wofs = wofs_.p;
   // ---- fold the smooth near part into W_eff (in place over wnear) -----------
   if (s.keep_f32) BIE_CUDA(weff32_.alloc(std::max<size_t>(wlen, 1)));
-  if (wst_) {
+  if (fst_) {
     // the folds read the geometry uploaded on st and the buffers allocated there
     BIE_CUDA(cudaEventRecord(wev_in_, st));
-    BIE_CUDA(cudaStreamWaitEvent(wst_, wev_in_, 0));
+    BIE_CUDA(cudaStreamWaitEvent(fst_, wev_in_, 0));
   }
-  // FP32 path: subtract the smooth part as the FP32 far kernel computes it
-  if (s.keep_f32) BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff32_.p, 1, wst));
-  BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff64_.p, 0, wst));
-  if (wst_) BIE_CUDA(cudaEventRecord(wev_done_, wst_));
+  for (int c = 0; c < nwc; ++c) {
+    if (fst_) BIE_CUDA(cudaStreamWaitEvent(fst_, wev_copy_[size_t(c)], 0));
+    // FP32 path: subtract the smooth part as the FP32 far kernel computes it
+    if (s.keep_f32)
+      BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff32_.p, 1, fst, kc[c], kc[c + 1]));
+    BIE_CUDA(dev::launch_fold(g, nr, kp, weff64_.p, weff64_.p, 0, fst, kc[c], kc[c + 1]));
+  }
+  if (fst_) BIE_CUDA(cudaEventRecord(wev_done_, fst_));
   // per-source constants alpha w/(4pi), beta w/(4pi) for the multi-density far kernel
   BIE_CUDA(ab64_.alloc(size_t(nptso) * (cplx ? 4 : 2)));
   BIE_CUDA(ab32_.alloc(size_t(nptso) * (cplx ? 4 : 2)));
@@ -331,7 +529,7 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   BIE_CUDA(tc_err_.alloc(1));
   BIE_CUDA(cudaMemsetAsync(tc_err_.p, 0, sizeof(int), st));
   for (auto& e : ev_) BIE_CUDA(cudaEventCreate(&e));
-  // host vectors above are consumed by async copies: wait before they go
+  // the staged host arrays are consumed by async copies: wait before they go
   BIE_CUDA(cudaStreamSynchronize(st));
   // far-field method by problem size
   {
@@ -354,6 +552,7 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   nodes = npts;
   d_node_wts = wts_.p;
   seg_start = {0, npts};
+  copy_guard.done = true;
   return init_segments(st);
 }
 

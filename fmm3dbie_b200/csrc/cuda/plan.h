@@ -277,9 +277,11 @@ class Plan : public Operator {
   DBuf<char> str_;
   DBuf<double> partial_;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
-  // async_weff: the W_eff stream and the events that order it
-  cudaStream_t wst_ = nullptr;
+  // async_weff: the streams of the near quadrature's chunk copies (wst_) and
+  // of the folds (fst_), and the events that order them
+  cudaStream_t wst_ = nullptr, fst_ = nullptr;
   cudaEvent_t wev_in_ = nullptr, wev_done_ = nullptr;
+  std::vector<cudaEvent_t> wev_copy_;  // one per chunk copy
 };
 
 // A batch of surfaces solved together: one operator whose nodes are the
