@@ -118,3 +118,64 @@ def test_batched_systems_match_individual(torch, ellipsoid_small, ellipsoid_helm
                                                                   st.over, 1e-10, iprec=1)
     assert stt == 0 and np.all(rres <= 1e-10)
     assert np.max(np.abs(soln - X)) < 1e-8 * np.max(np.abs(X))
+
+
+def test_host_buffer_solve_matches_device_plan(torch, ellipsoid_small, ellipsoid_helm_setup):
+    """The host-buffer solver uploads the near quadrature in near-pair chunks
+    whose folds run on their own stream beside the solve's first far field;
+    from pinned buffers that overlap is real.  Its solution must be the
+    device-resident plan's (same kernels, same W_eff)."""
+    s, st = ellipsoid_small, ellipsoid_helm_setup
+    zp = (2.0, -2.0j, 1.0)
+    assert st.near.row_ptr[-1] - 1 >= 8 * 1024  # enough near pairs for the chunked upload
+    rhs = _ps(2.0, np.array([0.1, -0.2, 0.3]), s.xyz)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    near_p = S.NearField(pin(st.near.row_ptr), pin(st.near.col_ind), pin(st.near.iquad),
+                         pin(st.near.wnear))
+    P = Plan(1, zp, s, st.near, st.over)
+    xd, info = P.solve(torch.tensor(rhs, device="cuda"), 0.5, mode=1, numit=100,
+                       eps_gmres=1e-10)
+    xd = xd.cpu().numpy()
+    w = s.qwts()
+    for _ in range(2):  # the second call reuses the pinned staging of the first
+        niter, rres, soln, status = layer.helm_comb_dir_solver_guru_ext(
+            s, 1e-7, zp, 100, 1, pin(rhs[:, None]), near_p, st.over, 1e-10, iprec=1)
+        assert status == 0 and rres[0] <= 1e-10
+        assert niter[0] == info["niter"][0]
+        assert wnorm(w, soln[:, 0] - xd) / wnorm(w, xd) < 1e-12
+
+
+def test_concurrent_plan_builds(torch, ellipsoid_small, ellipsoid_helm_setup):
+    """Plan builds in two threads at once: one stages its host arrays in the
+    library's pinned buffer, the other in pageable memory; both operators
+    equal a plan built alone."""
+    import threading
+    s, st = ellipsoid_small, ellipsoid_helm_setup
+    zp = (2.0, -2.0j, 1.0)
+    rng = np.random.default_rng(11)
+    sig = rng.normal(size=s.npts) + 1j * rng.normal(size=s.npts)
+    ref_plan = Plan(1, zp, s, st.near, st.over)
+    x = torch.tensor(sig, device="cuda")
+    ref = {p: ref_plan.matvec(x, p).cpu().numpy() for p in (0, 1)}
+    out, errs = {}, []
+    barrier = threading.Barrier(2)
+
+    def work(i):
+        try:
+            barrier.wait()
+            P = Plan(1, zp, s, st.near, st.over)
+            out[i] = {p: P.matvec(x, p).cpu().numpy() for p in (0, 1)}
+            P.close()
+        except Exception as e:  # reported below, in the test's own thread
+            errs.append(e)
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs, errs
+    for i in range(2):
+        for p in (0, 1):
+            d = np.linalg.norm(out[i][p] - ref[p]) / np.linalg.norm(ref[p])
+            assert d < 1e-13, (i, p, d)
