@@ -325,7 +325,7 @@ int solve_on_gpu(int kind, cdouble zk, cdouble alpha, cdouble beta, int64_t npat
   Stage stg;
   bie::AllocStreamScope alloc_scope(stg.st);  // plan buffers return to the pool on stg.st
   // The right-hand sides go first: a copy issued while the near quadrature's
-  // chunks are in flight waits for them on the copy engine.
+  // chunk copies are queued lands after all of them (measured).
   const int c = kind == 1 ? 2 : 1;
   const size_t len = size_t(npts) * nrhs * c;
   bie::DBuf<double> dr, dx;

@@ -245,8 +245,8 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   // in near-pair chunks.  The first chunks' copies run while the host checks
   // the near list and builds the other arrays; the uploads of those follow,
   // and the other chunks wait for them, so that the geometry lands early
-  // (copy engines take the copies of different streams in turns, not in the
-  // order they were issued).  With async_weff each chunk's folds start on
+  // (measured: a copy issued on st while chunk copies are queued on their
+  // stream lands after all of them).  With async_weff each chunk's folds start on
   // their own stream as soon as the chunk has landed, beside the solve's
   // first far field.
   const int cw = cplx ? 2 : 1;
