@@ -174,6 +174,10 @@ Plan::Plan() = default;
 Plan::~Plan() {
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
+  release_weff_streams();
+}
+
+void Plan::release_weff_streams() {
   // W_eff copies and folds done before their buffers go
   if (wst_) cudaStreamSynchronize(wst_);
   if (fst_) cudaStreamSynchronize(fst_);
@@ -183,6 +187,9 @@ Plan::~Plan() {
     if (e) cudaEventDestroy(e);
   if (wst_) cudaStreamDestroy(wst_);
   if (fst_) cudaStreamDestroy(fst_);
+  wst_ = fst_ = nullptr;
+  wev_in_ = wev_done_ = nullptr;
+  wev_copy_.clear();
 }
 
 int Plan::wait_weff(cudaStream_t st) {
@@ -246,13 +253,14 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   // the near list and builds the other arrays; the uploads of those follow,
   // and the other chunks wait for them, so that the geometry lands early
   // (measured: a copy issued on st while chunk copies are queued on their
-  // stream lands after all of them).  With async_weff each chunk's folds start on
-  // their own stream as soon as the chunk has landed, beside the solve's
-  // first far field.
+  // stream lands after all of them).  Each chunk's folds start on their own
+  // stream as soon as the chunk has landed.  With async_weff the build
+  // returns before they finish and the solve's first far field runs beside
+  // them; otherwise the build waits for them.
   const int cw = cplx ? 2 : 1;
   const size_t wlen = size_t(nquad) * cw;
   BIE_CUDA(weff64_.alloc(std::max<size_t>(wlen, 1)));
-  const int nwc = (s.async_weff && nnz >= int64_t(kWeffChunks) * 1024) ? kWeffChunks : 1;
+  const int nwc = nnz >= int64_t(kWeffChunks) * 1024 ? kWeffChunks : 1;
   std::vector<int64_t> kc(nwc + 1, 0), qc(nwc + 1, 0);
   for (int c = 1; c <= nwc; ++c) {
     kc[c] = nnz * c / nwc;
@@ -261,7 +269,7 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
     qc[c] = c == nwc ? nquad : std::min(nquad, std::max(qc[c - 1], s.iquad[kc[c]] - 1));
   }
   cudaStream_t wst = st, fst = st;  // streams of the W_eff chunk copies and of the folds
-  if (s.async_weff) {
+  if (s.async_weff || nwc > 1) {
     BIE_CUDA(cudaStreamCreateWithFlags(&wst_, cudaStreamNonBlocking));
     BIE_CUDA(cudaStreamCreateWithFlags(&fst_, cudaStreamNonBlocking));
     BIE_CUDA(cudaEventCreateWithFlags(&wev_in_, cudaEventDisableTiming));
@@ -414,7 +422,6 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   kp.kr = s.zk.real();
   kp.ki = s.zk.imag();
   if (kind == 0) kp.ai = kp.bi = kp.kr = kp.ki = 0.0;
-  kp.thresh = fmm_thresh(nptso, s.srcover, 12, ntarg, s.targs, s.ndtarg);
   // bounding boxes of the FP32 far kernel's target blocks and source tiles;
   // margin: the threshold plus 2^-12 of the extent, far above the FP32
   // rounding of the centred coordinates
@@ -440,6 +447,21 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   };
   boxes(htx, hty, htz, ntarg, dev::kFarBlockTargets32, htb);
   boxes(hsrc[0], hsrc[1], hsrc[2], nptso, dev::kFarTileSources, hsb);
+  // get_fmm_thresh (get_fmm_thresh.f:81) from the union of the boxes: the
+  // same bounding box of all sources and targets, the extrema being exact
+  {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    auto add = [&](const double* bx, int64_t nb) {
+      for (int64_t b = 0; b < nb; ++b)
+        for (int c = 0; c < 3; ++c) {
+          lo[c] = std::min(lo[c], bx[6 * b + c]);
+          hi[c] = std::max(hi[c], bx[6 * b + 3 + c]);
+        }
+    };
+    add(htb, nbt);
+    add(hsb, nbs);
+    kp.thresh = std::ldexp(std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]}), -51);
+  }
   double ext = 0.0;
   for (int64_t b = 0; b < nbt; ++b)
     for (int c = 0; c < 3; ++c) ext = std::max(ext, std::fabs(htb[6 * b + c]) + std::fabs(htb[6 * b + 3 + c]));
@@ -529,8 +551,12 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   BIE_CUDA(tc_err_.alloc(1));
   BIE_CUDA(cudaMemsetAsync(tc_err_.p, 0, sizeof(int), st));
   for (auto& e : ev_) BIE_CUDA(cudaEventCreate(&e));
+  // without async_weff the build returns with W_eff complete
+  if (!s.async_weff && wev_done_) BIE_CUDA(cudaStreamWaitEvent(st, wev_done_, 0));
   // the staged host arrays are consumed by async copies: wait before they go
   BIE_CUDA(cudaStreamSynchronize(st));
+  copy_guard.done = true;  // from here the destructor waits for any copy still in flight
+  if (!s.async_weff) release_weff_streams();
   // far-field method by problem size
   {
     const char* fm = std::getenv("BIE_FAR_METHOD");
@@ -552,7 +578,6 @@ int Plan::build(const PlanSpec& s, cudaStream_t st) {
   nodes = npts;
   d_node_wts = wts_.p;
   seg_start = {0, npts};
-  copy_guard.done = true;
   return init_segments(st);
 }
 

@@ -277,8 +277,10 @@ class Plan : public Operator {
   DBuf<char> str_;
   DBuf<double> partial_;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
-  // async_weff: the streams of the near quadrature's chunk copies (wst_) and
-  // of the folds (fst_), and the events that order them
+  // the streams of the near quadrature's chunk copies (wst_) and of the
+  // folds (fst_), and the events that order them; a build without
+  // async_weff releases them once W_eff is complete
+  void release_weff_streams();
   cudaStream_t wst_ = nullptr, fst_ = nullptr;
   cudaEvent_t wev_in_ = nullptr, wev_done_ = nullptr;
   std::vector<cudaEvent_t> wev_copy_;  // one per chunk copy
